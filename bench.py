@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark of the 2D-Gaussian-surfel training step on B200.
+
+One step = forward over every view (projection, binning, tile raster), fused
+L1+SSIM loss, backward raster, projection backward and Adam over all surfel
+parameters, on a resident seeded synthetic scene (default: 1,000,000 surfels
+and 8 ring views from 640x480 to 1920x1080, 9.0 Mpx). The headline `value` is
+the batched mixed-precision form ("chosen"); the plain FP32 one-view-at-a-time
+form is timed on the same inputs in the same run.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one process per GPU under torchrun; the
+path has no exchange step at this scope), timed as the max over ranks.
+`--impl reference` times the reference algorithm's CPU implementation (the
+C++ restatement of the reference's CPU renderer; the reference itself is Rust
++ WGSL on wgpu/Vulkan and cannot be built or run on this machine).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd+Adam steps/s, 1M surfels 1080p: chosen vs plain form; HBM roofline frac"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", default="ring8_1m")
+    p.add_argument("--precision", default="f16", choices=["f32", "f16", "bf16"])
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU-baseline sample time")
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.lines = device, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------ CPU (oracle) timing
+def cpu_step_estimate(wl, seconds_target: float, threads: int = 0, view_ids=None):
+    """Seconds per full training step of the C++ restatement of the
+    reference's CPU renderer (crates/gs-cpu-ref) on this workload, measured on
+    a bounded sample: every view's projection, tile lists, L1+SSIM and
+    parameter chain in full, the per-pixel forward and backward walks on every
+    `stride`-th tile only, scaled by `stride`; Adam over all parameters once."""
+    import oracle
+    s = wl.surfels
+    scene = oracle.Scene(s.positions.astype(np.float64), s.scales.astype(np.float64), s.quats.astype(np.float64),
+                         s.opacities.astype(np.float64), s.sh48().astype(np.float64), s.sh_degree)
+    views = range(len(wl.cameras)) if view_ids is None else view_ids
+    total, detail = 0.0, []
+    stride = 64
+    adam = 0.0
+    for v in views:
+        c = wl.cameras[v]
+        cam = oracle.Camera(np.array(c.center), np.array(c.quat), c.focal, c.width, c.height)
+        tgt = np.zeros((c.width * c.height, 4))
+        t = oracle.cpu_step_timed(scene, cam, tgt, tile_stride=stride, threads=threads)
+        per_view = t[0] + (t[1] + t[3]) * stride + t[2] + t[4]
+        adam = t[5]
+        total += per_view
+        detail.append([round(x, 4) for x in t])
+    scale = len(wl.cameras) / len(list(views))
+    step = total * scale + adam
+    return step, stride, detail
+
+
+# ---------------------------------------------------------------- our arm
+def algorithmic_bytes(stage: str, n: int, views, E: int, P: int) -> float:
+    """Algorithmic HBM bytes of a stage per step (FP32 plain form)."""
+    nv = len(views)
+    if stage == "raster_fwd":
+        return E * (4 + 72) + 40 * P
+    if stage == "raster_bwd":
+        return E * (4 + 68) + 40 * P + 64 * n * nv
+    if stage == "project":
+        return 332.0 * n * nv
+    if stage == "project_bwd_adam":
+        return 600.0 * n * nv + 58 * 32.0 * n
+    if stage == "l1_ssim":
+        return 36.0 * P
+    if stage in ("tile_sort",):
+        return 2 * 2 * 8.0 * E
+    if stage == "expand":
+        return 8.0 * E
+    if stage == "ranges":
+        return 4.0 * E
+    if stage == "depth_sort_scan":
+        return 4 * 2 * 8.0 * n * nv
+    return 0.0
+
+
+def launches_per_step(n_tiles: int, nv: int, form: str) -> int:
+    bits = max(1, math.ceil(math.log2(max(n_tiles, 2))))
+    tile_passes = math.ceil(bits / 8)
+    fwd = 1 + 4 * 3 + 3 + 1 + 1 + tile_passes * 3 + 1 + 1
+    if form == "chosen":
+        return fwd + 2 + 1 + 1
+    return nv * (fwd + 2 + 1 + 1) + 5
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    from splattar_b200 import Rasterizer, StepSettings
+    from splattar_b200.rasterizer import AdamSettings
+    from splattar_b200.synthetic import workload
+
+    wl = workload(args.workload)
+    cams = wl.cameras
+    n, nv, P = wl.surfels.n, len(cams), wl.pixels
+    max_entries = int(min(4.2e9, 96 * n * nv))
+    rast = Rasterizer(n, 0, 0, max_entries, max_views=nv, max_pixels=P, precision=args.precision, color_only=True)
+    # Target images: the seed-1 scene rendered through the same cameras.
+    rast.upload_scene(wl.target_surfels.scene_input())
+    rast.forward(cams, n)
+    rast.check()
+    target = rast.read("out_color", 4 * P)
+    rast.write("target", target)
+    rast.upload_scene(wl.surfels.scene_input())
+    rast.optimizer_init(n)
+    adam = AdamSettings(eps=1e-15)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    chosen = StepSettings(0.8, 0.2, adam, "chosen")
+    plain = StepSettings(0.8, 0.2, adam, "plain")
+
+    def timed(step_cfg, steps, warmup):
+        for _ in range(warmup):
+            rast.train_step(cams, n, step_cfg, sp)
+        rast.check(sp)
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            rast.train_step(cams, n, step_cfg, sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rast.check(sp)
+        ms = e0.elapsed_time(e1) / steps
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_chosen = timed(chosen, args.steps, args.warmup)
+    clk = clocks.stop()
+    E = rast.entry_count()
+    ms_plain = None if args.no_plain else timed(plain, max(2, args.steps // 2), args.warmup)
+
+    # End to end through the public API: pinned host targets in, loss out.
+    tgt_host = torch.from_numpy(target.view(np.float32)).pin_memory()
+    loss_host = torch.zeros(2 * nv, dtype=torch.float64).pin_memory()
+    for _ in range(args.warmup):
+        rast.write_async("target", tgt_host.data_ptr(), tgt_host.numel() * 4, 0, sp)
+        rast.train_step(cams, n, chosen, sp)
+        rast.read_async("loss", loss_host.data_ptr(), loss_host.numel() * 8, 0, sp)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rast.write_async("target", tgt_host.data_ptr(), tgt_host.numel() * 4, 0, sp)
+        rast.train_step(cams, n, chosen, sp)
+        rast.read_async("loss", loss_host.data_ptr(), loss_host.numel() * 8, 0, sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms_e2e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    loss_vals = loss_host.numpy().copy()
+
+    # Stage timing (CUDA events between stages on the launch stream).
+    prof = [rast.train_step_profiled(cams, n, chosen, sp) for _ in range(3)]
+    stages = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
+    n_tiles = sum(((c.width + 15) // 16) * ((c.height + 15) // 16) for c in cams)
+    rast.check(sp)
+    result = dict(wl=wl, n=n, nv=nv, P=P, E=E, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
+                  stages=stages, n_tiles=n_tiles, loss=loss_vals, h2d=tgt_host.numel() * 4,
+                  d2h=loss_host.numel() * 8)
+    rast.close()
+    return result
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return main_reference(args, ws, rank)
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    r = run_ours(args, ws, rank, local)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    n, nv, P, E = r["n"], r["nv"], r["P"], r["E"]
+    steps_s = 1000.0 / r["ms_chosen"]
+    peak, peak_kind = measured_hbm_peak()
+    stages = r["stages"]
+    dom = max(stages, key=stages.get)
+    alg = algorithmic_bytes(dom, n, r["wl"].cameras, E, P)
+    achieved = alg / (stages[dom] * 1e-3) / 1e9 if stages[dom] > 0 else 0.0
+    line = {
+        "metric": METRIC,
+        "value": round(steps_s * ws, 4),
+        "unit": "steps/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(r["ms_chosen"], 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": args.workload,
+            "surfels": n,
+            "views": nv,
+            "resolutions": [f"{c.width}x{c.height}" for c in r["wl"].cameras],
+            "pixels_per_step": P,
+            "tile_entries_per_step": E,
+            "form": "chosen: views batched per pass, persistent raster kernels, projection backward fused with Adam, "
+                    f"{args.precision} storage of SH and projected colour/normal, CUDA-graph replay",
+            "loss": "0.8*L1 + 0.2*(1-SSIM), 11x11 Gaussian sigma 1.5",
+            "adam": "lr pos 1.6e-4 scales 5e-3 quat 1e-3 opacity 5e-2 sh 2.5e-3, betas 0.9/0.999, eps 1e-15",
+            "l2": "inputs larger than L2 (params+optimizer state ~1.5 GB, tile entries ~%.1f GB)" % (E * 16 / 1e9),
+            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+        },
+        "mpix_per_s": round(steps_s * P / 1e6 * ws, 2),
+        "plain": None if r["ms_plain"] is None else {
+            "steps_per_s": round(1000.0 / r["ms_plain"] * ws, 4), "ms_per_step": round(r["ms_plain"], 4),
+            "form": "views one at a time, FP32 records and SH, separate projection backward and Adam kernels"},
+        "chosen_over_plain": None if r["ms_plain"] is None else round(r["ms_plain"] / r["ms_chosen"], 3),
+        "e2e": {"value": round(1000.0 / r["ms_e2e"] * ws, 4), "unit": "steps/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"], "ms_per_step": round(r["ms_e2e"], 4),
+                "path": "Rasterizer.write_async(target, pinned) + gs_train_step + read_async(loss, pinned)"},
+        "gpu_launches": launches_per_step(r["n_tiles"], nv, "chosen") * args.steps,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s",
+                     "algorithmic_bytes": alg, "kernel_ms": round(stages[dom], 4)},
+        "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+        "clocks": r["clk"],
+        "loss": [float(x) for x in r["loss"][:4]],
+    }
+    if not args.no_cpu_baseline:
+        import oracle
+        cores = oracle.max_threads()
+        t0 = time.time()
+        step_s, stride, detail = cpu_step_estimate(r["wl"], args.cpu_seconds, threads=cores)
+        line["cpu_baseline"] = {"value": round(1.0 / step_s, 6), "unit": "steps/s", "cores": cores, "kind": "port",
+                                "sample": f"all {nv} views; projection, tile lists, L1+SSIM, parameter chain and Adam "
+                                          f"in full; per-pixel forward/backward on every {stride}th tile, scaled by "
+                                          f"{stride} ({time.time() - t0:.1f} s of CPU time)",
+                                "seconds_per_step": round(step_s, 3)}
+    print(json.dumps(line))
+
+
+def main_reference(args, ws, rank):
+    """Reference arm: the reference's CPU algorithm (C++ restatement of
+    crates/gs-cpu-ref) on this workload, all host threads, rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+    from splattar_b200.synthetic import workload
+    wl = workload(args.workload)
+    cores = oracle.max_threads()
+    nv = len(wl.cameras)
+    times = []
+    for k in range(args.warmup + args.steps):
+        v = k % nv
+        step_s, stride, _ = cpu_step_estimate(wl, 0, threads=cores, view_ids=[v])
+        if k >= args.warmup:
+            times.append(step_s)
+    step_s = statistics.mean(times)
+    val = 1.0 / step_s
+    line = {"metric": METRIC, "value": round(val, 6), "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(step_s * 1000, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "surfels": wl.surfels.n, "views": nv, "pixels_per_step": wl.pixels},
+            "cpu_baseline": {"value": round(val, 6), "unit": "steps/s", "cores": cores, "kind": "port",
+                             "sample": f"each step one view (rotating) of {nv}: projection, tile lists, L1+SSIM, "
+                                       f"parameter chain in full, per-pixel walks on every {stride}th tile scaled by "
+                                       f"{stride}, extrapolated to all {nv} views; Adam over all parameters"},
+            "e2e": {"value": round(val, 6), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference (Rust + WGSL on wgpu/Vulkan) cannot be built or run here; this is its CPU "
+                    "renderer's algorithm restated in C++"}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

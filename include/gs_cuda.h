@@ -1,0 +1,275 @@
+/*
+ * gs_cuda — B200 (sm_100a) implementation of splattar's differentiable
+ * 2D-Gaussian-surfel training step behind a plain C ABI.
+ *
+ * The reference exposes this path as concrete Rust structs holding public GPU
+ * buffers that callers bind directly (no trait exists):
+ *   gs_kernels::Rasterizer   crates/gs-kernels/src/rasterizer.rs:56-98
+ *   gs_kernels::TileBinner   crates/gs-kernels/src/binning.rs:22-43
+ *   gs_wgpu::RadixSorter     crates/gs-wgpu/src/sort.rs:17-327
+ *   gs_wgpu::PrefixSum       crates/gs-wgpu/src/prefix_sum.rs:19-165
+ *   gs_train::SsimLoss       first_attempt/crates/gs-train/src/ssim.rs:26-299
+ *   gs_train::Optimizer      first_attempt/crates/gs-train/src/optim.rs:50-242
+ *   gs_train::Trainer::step  first_attempt/crates/gs-train/src/trainer.rs:1139-1332
+ * Each entry point below names the reference item it replaces. Every call
+ * returns a gs_status. Work is stream-ordered on the caller's cudaStream_t
+ * (passed as void*; NULL = legacy default stream). Handles are not
+ * thread-safe; several handles may coexist. Device buffers are owned by the
+ * handle unless a function takes caller pointers.
+ *
+ * Device errors that cannot be returned synchronously (entry-capacity
+ * overflow, a bounded wait that expired) set a sticky error word on the
+ * device; gs_rasterizer_check() synchronises and reports it.
+ */
+#ifndef GS_CUDA_H
+#define GS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  GS_OK = 0,
+  GS_ERR_INVALID_ARG = 1,
+  GS_ERR_CAPACITY = 2,       /* surfels, views, pixels or tile entries exceed the config */
+  GS_ERR_CUDA = 3,           /* a CUDA runtime call failed */
+  GS_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait expired */
+  GS_ERR_NONFINITE = 5,
+  GS_ERR_STATE = 6           /* call out of order (e.g. backward before forward) */
+} gs_status;
+
+/* Storage precision of the renderer-facing copies (projected records, SH). */
+typedef enum { GS_PREC_F32 = 0, GS_PREC_F16 = 1, GS_PREC_BF16 = 2 } gs_precision;
+
+enum {
+  GS_FLAG_DETERMINISTIC = 1u << 0, /* ordered per-entry gradient reduction, no float atomics */
+  GS_FLAG_PERSISTENT = 1u << 1,    /* persistent raster kernels over a global tile queue */
+  GS_FLAG_COLOR_ONLY = 1u << 2     /* backward ignores dl_dcolor.w, dl_dnormal and lambda_dist */
+};
+
+/* Rasterizer::new(ctx, capacity, width, height, max_entries)
+ * (crates/gs-kernels/src/rasterizer.rs:108). Adds a view count and pixel
+ * budget for the batched multi-view form. Zero fields take defaults:
+ * max_views 1, max_pixels width*height*max_views, max_entries
+ * 64*capacity*max_views (the reference trainer's entries_per_surfel,
+ * first_attempt/crates/gs-train/src/trainer.rs:474), tile 16. */
+typedef struct {
+  uint32_t capacity;
+  uint32_t width;
+  uint32_t height;
+  uint32_t max_views;
+  uint64_t max_pixels;
+  uint64_t max_entries;
+  uint32_t tile;        /* 16 only in this build */
+  uint32_t batch;       /* shared-memory staging depth of the raster kernels: 64, 128 or 256 (0 = 128) */
+  uint32_t precision;   /* gs_precision */
+  uint32_t flags;       /* GS_FLAG_* */
+} gs_raster_config;
+
+/* RasterCamera (crates/gs-kernels/src/rasterizer.rs:34-41) plus the image
+ * size, which the reference fixes per Rasterizer. quat is camera-to-world
+ * xyzw, normalised on upload; principal point is the image centre; fx = fy. */
+typedef struct {
+  float quat[4];
+  float center[3];
+  float focal;
+  uint32_t width;
+  uint32_t height;
+  uint32_t sh_degree;
+} gs_camera;
+
+/* SceneInput (crates/gs-kernels/src/rasterizer.rs:44-54): host SoA arrays of
+ * ACTIVATED parameters. sh is coefficient-major rgb, sh_coeffs*3 floats per
+ * surfel, padded to 48 on upload. */
+typedef struct {
+  const float* positions; /* n*3 */
+  const float* scales;    /* n*2 */
+  const float* quats;     /* n*4 xyzw */
+  const float* opacities; /* n */
+  const float* sh;        /* n*sh_coeffs*3 */
+  uint32_t sh_coeffs;
+  uint32_t n;
+} gs_scene_input;
+
+/* Public buffers of Rasterizer (rasterizer.rs:66-93), TileBinner and SsimLoss.
+ * Per-pixel buffers hold all views back to back (gs_rasterizer_view_offset). */
+typedef enum {
+  GS_BUF_POSITIONS = 0,   /* float4 per surfel (w = 1) */
+  GS_BUF_SCALES = 1,      /* float2 */
+  GS_BUF_QUATS = 2,       /* float4 */
+  GS_BUF_OPACITIES = 3,   /* float */
+  GS_BUF_SH = 4,          /* 48 floats */
+  GS_BUF_OUT_COLOR = 5,   /* float4: rgb + accumulated alpha */
+  GS_BUF_OUT_AUX = 6,     /* float4: final T, alpha-weighted depth, 0, 0 */
+  GS_BUF_OUT_NORMAL = 7,  /* float4 */
+  GS_BUF_OUT_NCONTRIB = 8,/* u32: tile-list position just past the last contributor */
+  GS_BUF_DL_DCOLOR = 9,   /* float4: rgb loss gradient + depth-loss gradient in w */
+  GS_BUF_DL_DNORMAL = 10, /* float4 */
+  GS_BUF_GRAD_POS = 11,   /* float4 */
+  GS_BUF_GRAD_SCALES = 12,/* float2 */
+  GS_BUF_GRAD_QUAT = 13,  /* float4 */
+  GS_BUF_GRAD_OPACITY = 14,/* float */
+  GS_BUF_GRAD_SH = 15,    /* 48 floats */
+  GS_BUF_GRAD_CAM = 16,   /* 16 floats per view: dL/dR (column-major 9), dL/dC 3, dL/dfocal, pad 3 */
+  GS_BUF_TARGET = 17,     /* float4 loss target per pixel (SsimLoss::target) */
+  GS_BUF_RANGES = 18,     /* uint2 per tile (all views' tiles back to back): [start, end) */
+  GS_BUF_SORTED_ITEMS = 19,/* u32 per entry: item view*num_surfels + surfel, tile-major, depth-ascending */
+  GS_BUF_ENTRY_COUNT = 20,/* u64: total tile entries of the last forward */
+  GS_BUF_LOSS = 21,       /* double per view x2: sum |x-y| over rgb, sum SSIM over rgb */
+  GS_BUF_RAW_POS = 22,    /* optimizer raw parameters (Optimizer ParamClass::raw) */
+  GS_BUF_RAW_SCALES = 23,
+  GS_BUF_RAW_QUAT = 24,
+  GS_BUF_RAW_OPACITY = 25,
+  GS_BUF_RAW_SH = 26,
+  GS_BUF_RECTS = 27,      /* uint4 tile rect per item (x0,y0,x1,y1 inclusive; culled or off-screen = 1,1,0,0) */
+  GS_BUF_DEPTH_KEYS = 28, /* u32 per item after the depth sort: f32 bits of the centre depth, ascending */
+  GS_BUF_DEPTH_ORDER = 29 /* u32 per item after the depth sort: item index (stable, ties by index) */
+} gs_buffer_id;
+
+typedef struct gs_rasterizer gs_rasterizer;
+
+/* Rasterizer::new */
+gs_status gs_rasterizer_create(const gs_raster_config* cfg, gs_rasterizer** out);
+gs_status gs_rasterizer_destroy(gs_rasterizer* r);
+/* Rasterizer::upload_scene (rasterizer.rs:359-386). Blocking copy. */
+gs_status gs_rasterizer_upload_scene(gs_rasterizer* r, const gs_scene_input* scene, void* stream);
+/* Rasterizer::lambda_dist (rasterizer.rs:60) */
+gs_status gs_rasterizer_set_lambda_dist(gs_rasterizer* r, float lambda_dist);
+/* Rasterizer::forward (rasterizer.rs:389-448): projection, binning, forward
+ * raster for n_views cameras (1 = the reference's single-view call). */
+gs_status gs_rasterizer_forward(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
+                                void* stream);
+/* Rasterizer::backward (rasterizer.rs:320-356): clears the gradient buffers,
+ * then backward raster and projection backward, summing over the views of the
+ * last forward. Reads dl_dcolor (+ w depth gradient) and dl_dnormal. */
+gs_status gs_rasterizer_backward(gs_rasterizer* r, uint32_t num_surfels, void* stream);
+/* Buffer address and size in bytes. */
+gs_status gs_rasterizer_buffer(gs_rasterizer* r, gs_buffer_id id, void** dptr, size_t* bytes);
+/* First pixel (in per-pixel buffers) and first tile of a view of the last forward. */
+gs_status gs_rasterizer_view_offset(gs_rasterizer* r, uint32_t view, uint64_t* pixel_offset, uint32_t* tile_offset);
+/* Stream-ordered copies between host memory and a handle buffer; blocking. */
+gs_status gs_rasterizer_read(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_offset, void* host, size_t bytes,
+                             void* stream);
+gs_status gs_rasterizer_write(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_offset, const void* host, size_t bytes,
+                              void* stream);
+/* Asynchronous variants: host memory must be pinned and stay valid until the
+ * stream reaches the copy. */
+gs_status gs_rasterizer_read_async(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_offset, void* host, size_t bytes,
+                                   void* stream);
+gs_status gs_rasterizer_write_async(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_offset, const void* host,
+                                    size_t bytes, void* stream);
+/* Synchronises the stream and reports (and clears) the sticky device error word. */
+gs_status gs_rasterizer_check(gs_rasterizer* r, void* stream);
+/* Text of the last error on this handle (or of the last failed create when r is NULL). */
+gs_status gs_last_error(gs_rasterizer* r, char* msg, size_t cap);
+
+/* SsimLoss::encode (first_attempt/crates/gs-train/src/ssim.rs:236-280):
+ * L = w_l1*mean|x-y| + w_ssim*mean(1-SSIM) per view, rgb channels, 11-tap
+ * sigma 1.5 Gaussian window with zero padding. Reads OUT_COLOR and TARGET,
+ * writes DL_DCOLOR (w = 0) and the per-view sums into GS_BUF_LOSS. The
+ * reference's own form (1-lambda)*L1 + lambda*(1-SSIM)/2 is w_l1 = 1-lambda,
+ * w_ssim = lambda/2. */
+gs_status gs_loss_l1_ssim(gs_rasterizer* r, float w_l1, float w_ssim, void* stream);
+
+/* Optimizer (first_attempt/crates/gs-train/src/optim.rs:50-242) over the five
+ * classes the trainer registers (trainer.rs:757-761): pos (identity, 4 per
+ * surfel incl. pad lane), scales (exp), quat (identity), opacity (sigmoid),
+ * sh (identity, 48). */
+typedef struct {
+  float lr[5];      /* pos, scales, quat, opacity, sh */
+  float reg[5];     /* constant added to dL/d(activated) (optim.rs:37) */
+  float beta1;
+  float beta2;
+  float eps;        /* the reference uses 1e-8 (optim.rs:187) */
+} gs_adam_config;
+
+/* Trainer::new raw upload (trainer.rs:763-791): raw = inverse activation of
+ * the current activated buffers (log scales, logit opacity); zero moments, t = 0. */
+gs_status gs_optimizer_init(gs_rasterizer* r, uint32_t num_surfels, void* stream);
+/* Optimizer::encode_step (optim.rs:205-227): t += 1, Adam on every class,
+ * then refresh the activated buffers. */
+gs_status gs_optimizer_step(gs_rasterizer* r, const gs_adam_config* cfg, uint32_t num_surfels, void* stream);
+
+/* One Adam step on caller device arrays (adam.wgsl:45-74): activation 0
+ * identity, 1 exp, 2 sigmoid; t is the 1-based step for bias correction.
+ * act may be NULL. */
+gs_status gs_adam_flat(float* raw, const float* grad_act, float* m, float* v, float* act, uint64_t n,
+                       uint32_t activation, float lr, float beta1, float beta2, float eps, float reg, uint32_t t,
+                       void* stream);
+
+/* One training iteration (Trainer::step, trainer.rs:1139-1332, without the
+ * out-of-scope appearance, pose and noise stages): forward over n_views
+ * cameras, L1+SSIM against TARGET, backward summing over views, Adam.
+ * form 0 = plain: views one at a time, FP32, separate kernels per stage.
+ * form 1 = chosen: all views batched in one pass per stage, persistent raster
+ *          kernels, projection backward fused with Adam, storage precision
+ *          from the config, the whole step replayed as one CUDA graph. */
+typedef struct {
+  float w_l1;
+  float w_ssim;
+  gs_adam_config adam;
+  uint32_t form;
+} gs_step_config;
+gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
+                        const gs_step_config* cfg, void* stream);
+
+/* The same step with CUDA events recorded on the stream between its stages
+ * (not graph-replayed); blocking. stage_ms receives milliseconds per stage,
+ * summed over views: 0 projection, 1 depth sort + entry scan, 2 tile-entry
+ * expansion, 3 tile sort, 4 tile ranges, 5 forward raster, 6 L1+SSIM,
+ * 7 backward raster, 8 projection backward + Adam. */
+gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
+                                 const gs_step_config* cfg, void* stream, float stage_ms[9], uint32_t* n_stages);
+
+/* Densify/prune compaction (no reference counterpart; the reference only
+ * relocates at fixed budget, trainer.rs:1558-1689): surfels whose mean
+ * accumulated position-gradient norm exceeds grad_threshold are cloned
+ * (copy with zeroed moments, appended while capacity allows), surfels whose
+ * activated opacity is below opacity_threshold are removed, and survivors are
+ * compacted in index order. Resets the gradient accumulators. */
+typedef struct {
+  float grad_threshold;     /* 2e-4 in the 6M-surfel workload */
+  float opacity_threshold;  /* 0.005 */
+} gs_densify_config;
+gs_status gs_densify_prune(gs_rasterizer* r, const gs_densify_config* cfg, uint32_t num_surfels,
+                           uint32_t* num_out, void* stream);
+
+/* ---- TileBinner (crates/gs-kernels/src/binning.rs:22-238) ---------------
+ * Items are tile-space AABBs (uint4 min_x, min_y, max_x, max_y inclusive;
+ * max < min = culled) with u32 depth keys. After encode, sorted_entries holds
+ * entry indices in the reference's expansion order (item-major, row-major
+ * within the rect) grouped by tile and depth-ascending, ties by entry index;
+ * entry_items maps entry -> item; ranges holds [start, end) per tile. */
+typedef struct gs_binner gs_binner;
+gs_status gs_binner_create(uint32_t max_items, uint64_t max_entries, uint32_t num_tiles, gs_binner** out);
+gs_status gs_binner_destroy(gs_binner* b);
+gs_status gs_binner_encode(gs_binner* b, const uint32_t* rects_dev, const uint32_t* depths_dev, uint32_t num_items,
+                           uint32_t tiles_x, void* stream);
+/* which: 0 sorted_entries (u32), 1 entry_items (u32), 2 ranges (uint2), 3 entry count (u64) */
+gs_status gs_binner_buffer(gs_binner* b, uint32_t which, void** dptr, size_t* bytes);
+
+/* ---- RadixSorter / PrefixSum (crates/gs-wgpu/src/{sort,prefix_sum}.rs) ----
+ * Stable LSD sort of n (key, value) u32 pairs on bits [0, key_bits), in
+ * place; and an exclusive u32 scan with the total written to *total_dev.
+ * Both take caller device pointers and allocate their scratch on first use
+ * per size class (held until gs_shutdown). */
+gs_status gs_radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint64_t n, uint32_t key_bits, void* stream);
+gs_status gs_exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total_dev, void* stream);
+
+/* Camera-to-world rotation (column-major 3x3) exactly as the forward computes
+ * it from gs_camera.quat (glam Mat3::from_quat of the normalised quaternion,
+ * rasterizer.rs:410). Host-only, no GPU needed. */
+gs_status gs_camera_rotation(const gs_camera* cam, float rot9[9]);
+
+/* Library version string and build flags; host-only. */
+const char* gs_version(void);
+/* Frees the library's global scratch (sort/scan) on the current device. */
+gs_status gs_shutdown(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GS_CUDA_H */

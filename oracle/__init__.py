@@ -1,0 +1,250 @@
+"""Correctness oracle for the surfel training step — TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this package, and only as the checker or the timed CPU
+baseline. The shipped library never calls it.
+
+PARITY STATUS: unpinned against golden vectors. The reference ships no
+known-answer files for this path and its own oracle (crates/gs-cpu-ref, Rust)
+cannot be built here. ``gs_oracle.hpp`` restates it line by line in C++ and the
+restatement is certified by central finite differences (the reference's own
+gate, crates/gs-cpu-ref/tests/gradcheck.rs) and analytic known answers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile (g++, OpenMP)."""
+    src = [os.path.join(_HERE, f) for f in ("gs_oracle.cpp", "gs_oracle.hpp", "Makefile")]
+    stale = not os.path.exists(_LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(_LIB_PATH) for s in src)
+    if force or stale:
+        env = dict(os.environ)
+        env.pop("CXX", None)
+        subprocess.run(["make", "-C", _HERE, "-s", "liboracle.so"], check=True, env=env)
+    return _LIB_PATH
+
+
+class _Scene(C.Structure):
+    _fields_ = [("n", C.c_int), ("sh_degree", C.c_int), ("pos", C.c_void_p), ("scales", C.c_void_p),
+                ("quat", C.c_void_p), ("opacity", C.c_void_p), ("sh", C.c_void_p)]
+
+
+class _Camera(C.Structure):
+    _fields_ = [("center", C.c_double * 3), ("quat", C.c_double * 4), ("focal", C.c_double),
+                ("width", C.c_int), ("height", C.c_int)]
+
+
+class _Grads(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in
+                ("pos", "scales", "quat", "opacity", "sh", "cam_center", "cam_quat", "focal", "dl_dr_cam")]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        vp, i32, f64 = C.c_void_p, C.c_int, C.c_double
+        L.orc_project.argtypes = [vp, vp, i32, vp, vp, vp, vp]
+        L.orc_project.restype = i32
+        L.orc_render.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_render.restype = i32
+        L.orc_gradients.argtypes = [vp, vp, i32, vp, vp, vp, f64, i32, vp]
+        L.orc_gradients.restype = i32
+        L.orc_distortion_loss.argtypes = [vp, vp, i32]
+        L.orc_distortion_loss.restype = f64
+        L.orc_project_f32.argtypes = [i32, vp, vp, vp, vp, vp, C.c_float, i32, i32, i32, vp, vp, vp]
+        L.orc_project_f32.restype = i32
+        L.orc_camera_rotation_f32.argtypes = [vp, vp]
+        L.orc_camera_rotation_f32.restype = None
+        L.orc_gauss_weights.argtypes = [vp]
+        L.orc_gauss_weights.restype = None
+        L.orc_l1_ssim.argtypes = [vp, vp, i32, i32, f64, f64, vp, vp, vp]
+        L.orc_l1_ssim.restype = f64
+        L.orc_adam.argtypes = [i32, vp, vp, vp, vp, vp, i32, f64, f64, f64, f64, f64, i32]
+        L.orc_adam.restype = None
+        L.orc_cpu_step_timed.argtypes = [vp, vp, i32, i32, i32, vp, vp]
+        L.orc_cpu_step_timed.restype = i32
+        L.orc_max_threads.argtypes = []
+        L.orc_max_threads.restype = i32
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class Scene:
+    """Activated surfel parameters in float64 (the oracle's precision)."""
+    pos: np.ndarray      # (n,3)
+    scales: np.ndarray   # (n,2) activated
+    quat: np.ndarray     # (n,4) xyzw, unnormalised
+    opacity: np.ndarray  # (n,)
+    sh: np.ndarray       # (n,48) coefficient-major rgb, padded to 16 coefficients
+    sh_degree: int
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+    def c(self):
+        self.pos = np.ascontiguousarray(self.pos, np.float64)
+        self.scales = np.ascontiguousarray(self.scales, np.float64)
+        self.quat = np.ascontiguousarray(self.quat, np.float64)
+        self.opacity = np.ascontiguousarray(self.opacity, np.float64)
+        self.sh = np.ascontiguousarray(self.sh, np.float64)
+        s = _Scene(self.n, self.sh_degree, _p(self.pos), _p(self.scales), _p(self.quat), _p(self.opacity),
+                   _p(self.sh))
+        return s
+
+    def copy(self):
+        return Scene(self.pos.copy(), self.scales.copy(), self.quat.copy(), self.opacity.copy(), self.sh.copy(),
+                     self.sh_degree)
+
+
+@dataclass
+class Camera:
+    center: np.ndarray  # (3,)
+    quat: np.ndarray    # (4,) camera-to-world xyzw
+    focal: float
+    width: int
+    height: int
+
+    def c(self):
+        cam = _Camera()
+        for k in range(3):
+            cam.center[k] = float(self.center[k])
+        for k in range(4):
+            cam.quat[k] = float(self.quat[k])
+        cam.focal = float(self.focal)
+        cam.width = int(self.width)
+        cam.height = int(self.height)
+        return cam
+
+    def copy(self):
+        return Camera(np.array(self.center, np.float64), np.array(self.quat, np.float64), float(self.focal),
+                      self.width, self.height)
+
+
+def project(scene: Scene, cam: Camera, tile: int = 16):
+    n = scene.n
+    rects = np.zeros((n, 4), np.int32)
+    keys = np.zeros(n, np.uint32)
+    marg = np.zeros(n, np.uint8)
+    pos = np.zeros(n, np.int32)
+    s, c = scene.c(), cam.c()
+    lib().orc_project(C.byref(s), C.byref(c), tile, _p(rects), _p(keys), _p(marg), _p(pos))
+    return rects, keys, marg.astype(bool), pos
+
+
+def render(scene: Scene, cam: Camera, tile: int = 16, literal: bool = False, threads: int = 0):
+    P = cam.width * cam.height
+    out = dict(color=np.zeros((P, 3)), alpha=np.zeros(P), depth=np.zeros(P), normal=np.zeros((P, 3)),
+               trans=np.zeros(P), ncontrib=np.zeros(P, np.int32), marginal=np.zeros(P, np.uint8))
+    s, c = scene.c(), cam.c()
+    lib().orc_render(C.byref(s), C.byref(c), tile, int(literal), threads, _p(out["color"]), _p(out["alpha"]),
+                     _p(out["depth"]), _p(out["normal"]), _p(out["trans"]), _p(out["ncontrib"]),
+                     _p(out["marginal"]))
+    out["marginal"] = out["marginal"].astype(bool)
+    return out
+
+
+def gradients(scene: Scene, cam: Camera, dl_dcolor, dl_ddepth=None, dl_dnormal=None, lambda_dist: float = 0.0,
+              tile: int = 16, threads: int = 0):
+    n = scene.n
+    g = dict(pos=np.zeros((n, 3)), scales=np.zeros((n, 2)), quat=np.zeros((n, 4)), opacity=np.zeros(n),
+             sh=np.zeros((n, 48)), cam_center=np.zeros(3), cam_quat=np.zeros(4), focal=np.zeros(1),
+             dl_dr_cam=np.zeros(9))
+    gs = _Grads(*[_p(g[k]) for k in ("pos", "scales", "quat", "opacity", "sh", "cam_center", "cam_quat", "focal",
+                                      "dl_dr_cam")])
+    dlc = np.ascontiguousarray(dl_dcolor, np.float64).reshape(-1, 3)
+    dld = None if dl_ddepth is None else np.ascontiguousarray(dl_ddepth, np.float64).reshape(-1)
+    dln = None if dl_dnormal is None else np.ascontiguousarray(dl_dnormal, np.float64).reshape(-1, 3)
+    s, c = scene.c(), cam.c()
+    lib().orc_gradients(C.byref(s), C.byref(c), tile, _p(dlc), _p(dld), _p(dln), float(lambda_dist), threads,
+                        C.byref(gs))
+    g["focal"] = float(g["focal"][0])
+    return g
+
+
+def distortion_loss(scene: Scene, cam: Camera, tile: int = 16) -> float:
+    s, c = scene.c(), cam.c()
+    return lib().orc_distortion_loss(C.byref(s), C.byref(c), tile)
+
+
+def camera_rotation_f32(quat) -> np.ndarray:
+    q = np.ascontiguousarray(quat, np.float32)
+    r = np.zeros(9, np.float32)
+    lib().orc_camera_rotation_f32(_p(q), _p(r))
+    return r
+
+
+def project_f32(pos4, scales2, quats4, rot9, center3, focal, width, height, tile=16):
+    """f32 mirror of the projection: (rects (n,4) u32, keys (n,) u32, cam (n,12) f32)."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    scales2 = np.ascontiguousarray(scales2, np.float32)
+    quats4 = np.ascontiguousarray(quats4, np.float32)
+    rot9 = np.ascontiguousarray(rot9, np.float32)
+    center3 = np.ascontiguousarray(center3, np.float32)
+    n = pos4.shape[0]
+    rects = np.zeros((n, 4), np.uint32)
+    keys = np.zeros(n, np.uint32)
+    camo = np.zeros((n, 12), np.float32)
+    lib().orc_project_f32(n, _p(pos4), _p(scales2), _p(quats4), _p(rot9), _p(center3), float(focal), width, height,
+                          tile, _p(rects), _p(keys), _p(camo))
+    return rects, keys, camo
+
+
+def gauss_weights() -> np.ndarray:
+    w = np.zeros(6)
+    lib().orc_gauss_weights(_p(w))
+    return w
+
+
+def l1_ssim(img_rgba, ref_rgba, width, height, w_l1=0.8, w_ssim=0.2):
+    """(loss, dL/dimg rgba, l1 channel sum, ssim channel sum) in float64."""
+    img = np.ascontiguousarray(img_rgba, np.float64).reshape(-1, 4)
+    ref = np.ascontiguousarray(ref_rgba, np.float64).reshape(-1, 4)
+    dl = np.zeros_like(img)
+    l1 = C.c_double()
+    ss = C.c_double()
+    loss = lib().orc_l1_ssim(_p(img), _p(ref), width, height, w_l1, w_ssim, _p(dl), C.byref(l1), C.byref(ss))
+    return loss, dl, l1.value, ss.value
+
+
+def adam(raw, grad_act, m, v, activation, lr, beta1=0.9, beta2=0.999, eps=1e-8, reg=0.0, t=1):
+    """One Adam step in float64 (in place on raw/m/v); returns the activated values."""
+    raw = np.ascontiguousarray(raw, np.float64)
+    g = np.ascontiguousarray(grad_act, np.float64)
+    m = np.ascontiguousarray(m, np.float64)
+    v = np.ascontiguousarray(v, np.float64)
+    act = np.zeros_like(raw)
+    lib().orc_adam(raw.size, _p(raw), _p(g), _p(m), _p(v), _p(act), activation, lr, beta1, beta2, eps, reg, t)
+    return raw, m, v, act
+
+
+def max_threads() -> int:
+    return lib().orc_max_threads()
+
+
+def cpu_step_timed(scene: Scene, cam: Camera, target_rgba, tile=16, tile_stride=1, threads=0):
+    """Seconds per phase (prep+bin, fwd, loss, bwd, chain, adam) of one CPU step."""
+    times = np.zeros(6)
+    tgt = np.ascontiguousarray(target_rgba, np.float64).reshape(-1, 4)
+    s, c = scene.c(), cam.c()
+    lib().orc_cpu_step_timed(C.byref(s), C.byref(c), tile, tile_stride, threads, _p(tgt), _p(times))
+    return times

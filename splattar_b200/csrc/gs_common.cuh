@@ -1,0 +1,181 @@
+// Shared device-side definitions of the surfel training step.
+//
+// Conventions follow the reference renderer (crates/gs-cpu-ref/src/scene.rs:4-13
+// and crates/gs-kernels/src/shaders/raster_common.wgsl:5-95): right-handed
+// camera looking down its local -z, x_cam = Rᵀ(p − C) with R camera-to-world,
+// pixel ray d = ((x+.5−cx)/f, −(y+.5−cy)/f, −1) with the principal point at
+// the image centre, surfel tangent axes τu = Rᵀ R_q e0 s_u, τv = Rᵀ R_q e1 s_v.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace gs {
+
+// raster_common.wgsl:34-39 / scene.rs:17-21
+constexpr float LOWPASS_SIGMA2 = 0.5f;
+constexpr float ALPHA_SKIP = 0.0039215686f;  // 1/255
+constexpr float ALPHA_CLAMP = 0.995f;
+constexpr float T_TERMINATE = 1e-4f;
+constexpr float NEAR_DEPTH = 0.05f;
+constexpr int TILE = 16;
+constexpr int SH_FLOATS = 48;
+
+// Sticky device error word bits.
+constexpr uint32_t ERR_ENTRY_CAPACITY = 1u << 0;
+constexpr uint32_t ERR_TIMEOUT = 1u << 1;
+
+// Per-view camera and image layout, one entry per view of a step.
+struct ViewInfo {
+  float rot[9];       // camera-to-world R, column-major: rot[3*k + j] = R[j][k]
+  float center[3];
+  float focal;
+  float cx, cy;       // width/2, height/2
+  int width, height;
+  int tiles_x, tiles_y;
+  int tile_base;      // first global tile id of this view
+  int sh_degree;
+  long long pix_base; // first pixel of this view in per-pixel buffers
+};
+
+// Projected surfel record ("SurfelCam"), one per (view, surfel). The ray–splat
+// intersection of crates/gs-cpu-ref/src/forward.rs:136-169 solves
+// [τu τv −d](u,v,t)ᵀ = −c by Cramer's rule; with s = −d every triple product
+// is linear in s:  det = s·M,  u·det = s·Bu,  v·det = s·Bv,  t·det = tn, where
+// M = τu×τv, Bu = τv×c, Bv = c×τu, tn = −c·M. Storing M, Bu, Bv, tn makes the
+// per-pixel intersection three 3-term dot products.
+//   r0 = (M, tn)  r1 = (Bu, px)  r2 = (Bv, py)
+//   r3 = (colour rgb, opacity)  r4 = (normal xyz, centre depth)
+struct RecF32 {
+  float4 r0, r1, r2, r3, r4;
+};
+// Mixed-precision record: geometry stays FP32 (it feeds a ratio of nearly
+// cancelling dot products), colour/opacity/normal/depth are stored as 16-bit.
+template <typename H>
+struct RecH {
+  float4 r0, r1, r2;
+  H a[8];  // r,g,b,opacity,nx,ny,nz,depth
+};
+
+template <typename H> __device__ __forceinline__ float h2f(H x);
+template <> __device__ __forceinline__ float h2f<__half>(__half x) { return __half2float(x); }
+template <> __device__ __forceinline__ float h2f<__nv_bfloat16>(__nv_bfloat16 x) { return __bfloat162float(x); }
+template <typename H> __device__ __forceinline__ H f2h(float x);
+template <> __device__ __forceinline__ __half f2h<__half>(float x) { return __float2half_rn(x); }
+template <> __device__ __forceinline__ __nv_bfloat16 f2h<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+
+// Loads record `idx` as five float4 (converting 16-bit fields).
+template <int PREC>
+__device__ __forceinline__ void load_record(const void* recs, uint32_t idx, float4& r0, float4& r1, float4& r2,
+                                            float4& r3, float4& r4) {
+  if constexpr (PREC == 0) {
+    const float4* p = reinterpret_cast<const float4*>(recs) + (size_t)idx * 5;
+    r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2); r3 = __ldg(p + 3); r4 = __ldg(p + 4);
+  } else {
+    using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
+    const float4* p = reinterpret_cast<const float4*>(recs) + (size_t)idx * 4;
+    r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2);
+    float4 raw = __ldg(p + 3);
+    const H* h = reinterpret_cast<const H*>(&raw);
+    r3 = make_float4(h2f<H>(h[0]), h2f<H>(h[1]), h2f<H>(h[2]), h2f<H>(h[3]));
+    r4 = make_float4(h2f<H>(h[4]), h2f<H>(h[5]), h2f<H>(h[6]), h2f<H>(h[7]));
+  }
+}
+
+template <int PREC>
+__device__ __forceinline__ void store_record(void* recs, uint32_t idx, float4 r0, float4 r1, float4 r2, float4 r3,
+                                             float4 r4) {
+  if constexpr (PREC == 0) {
+    float4* p = reinterpret_cast<float4*>(recs) + (size_t)idx * 5;
+    p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4;
+  } else {
+    using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
+    float4* p = reinterpret_cast<float4*>(recs) + (size_t)idx * 4;
+    p[0] = r0; p[1] = r1; p[2] = r2;
+    float4 raw;
+    H* h = reinterpret_cast<H*>(&raw);
+    h[0] = f2h<H>(r3.x); h[1] = f2h<H>(r3.y); h[2] = f2h<H>(r3.z); h[3] = f2h<H>(r3.w);
+    h[4] = f2h<H>(r4.x); h[5] = f2h<H>(r4.y); h[6] = f2h<H>(r4.z); h[7] = f2h<H>(r4.w);
+    p[3] = raw;
+  }
+}
+
+inline size_t record_bytes(int prec) { return prec == 0 ? 80 : 64; }
+
+// Per-surfel camera-space gradient layout written by the backward raster and
+// consumed by the projection backward ("grad_geom"). The backward raster
+// reduces gradients with respect to the record fields, not (c, τu, τv): the
+// chain through M, Bu, Bv, tn is linear, so it is applied once per surfel.
+//   0-2 dL/dM   3-5 dL/dBu   6-8 dL/dBv   9 dL/dpx   10 dL/dpy
+//   11-13 dL/dcolour   14 dL/dopacity   15 dL/dtn
+//   16 dL/ddepth (screen-branch t)   17-19 dL/dnormal   (aux losses only)
+constexpr int GG_STRIDE = 20;
+
+__device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Warp "transpose" reduction of 16 per-lane values: after it, lanes 2c and
+// 2c+1 hold the warp-wide sum of value c. 16 shuffles instead of the 80 of
+// sixteen independent butterflies.
+__device__ __forceinline__ float warp_reduce16(float (&v)[16]) {
+  const unsigned FULL = 0xffffffffu;
+  int lane = threadIdx.x & 31;
+  float a[8];
+  bool hi = lane & 16;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    float send = hi ? v[k] : v[k + 8];
+    float keep = hi ? v[k + 8] : v[k];
+    a[k] = keep + __shfl_xor_sync(FULL, send, 16);
+  }
+  float b[4];
+  hi = lane & 8;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float send = hi ? a[k] : a[k + 4];
+    float keep = hi ? a[k + 4] : a[k];
+    b[k] = keep + __shfl_xor_sync(FULL, send, 8);
+  }
+  float c[2];
+  hi = lane & 4;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    float send = hi ? b[k] : b[k + 2];
+    float keep = hi ? b[k + 2] : b[k];
+    c[k] = keep + __shfl_xor_sync(FULL, send, 4);
+  }
+  hi = lane & 2;
+  float d = (hi ? c[1] : c[0]) + __shfl_xor_sync(FULL, hi ? c[0] : c[1], 2);
+  return d + __shfl_xor_sync(FULL, d, 1);
+}
+// Component held by this lane after warp_reduce16: bits 4..1 of the lane id.
+__device__ __forceinline__ int reduce16_component(int lane) {
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace gs
+
+#define GS_CUDA_TRY(expr)                                   \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) return ::gs::cuda_fail(_e, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+namespace gs {
+int cuda_fail(cudaError_t e, const char* expr, const char* file, int line);
+}

@@ -1,0 +1,185 @@
+// Internal launch interface between the host orchestration (gs_api.cu) and
+// the kernel translation units. Launchers return a cudaError_t value (0 = ok).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gs_common.cuh"
+
+namespace gs {
+
+struct ProjectArgs {
+  const ViewInfo* views;
+  uint32_t n;             // surfels of this step; item = view*n + surfel
+  const float4* pos;
+  const float2* scales;
+  const float4* quats;
+  const float* opac;
+  const void* sh;         // 48 per surfel, f32 or 16-bit by precision
+  void* records;
+  uint4* rects;
+  uint32_t* keys;
+  uint32_t* vals;
+  uint32_t* counts;
+};
+
+struct ProjectBwdArgs {
+  const ViewInfo* views;
+  uint32_t n;
+  int n_views;
+  int view;               // plain form: the view of this launch
+  const float4* pos;
+  const float2* scales;
+  const float4* quats;
+  const void* sh;
+  const float* grad_geom;     // atomic mode: [item][GG_STRIDE]
+  const float* partials;      // deterministic mode: [entry][GG_STRIDE], or null
+  const uint32_t* entry_offset;  // deterministic mode: first entry of each item
+  const unsigned long long* entry_total;  // deterministic mode: entries of the last forward
+  const uint32_t* counts;
+  float4* grad_pos;
+  float2* grad_scales;
+  float4* grad_quat;
+  float* grad_opacity;
+  float* grad_sh;
+  float* grad_cam;        // 16 per view, or null
+};
+
+struct AdamClass {
+  float* raw;
+  float* m;
+  float* v;
+  float* act;
+  float lr;
+  float reg;
+};
+
+struct AdamFusedArgs {
+  AdamClass cls[5];
+  float beta1, beta2, eps, bc1_inv, bc2_inv;
+  const float* dyn;       // optional device copy of {lr[5], reg[5], bc1_inv, bc2_inv} (graph replay)
+  void* sh_half;          // 16-bit activated SH copy for mixed precision, or null
+  int sh_half_is_bf16;
+  float* accum_grad_norm; // per-surfel running sum of |dL/dpos| (densify), or null
+};
+
+struct RasterArgs {
+  const ViewInfo* views;
+  int n_views;
+  int total_tiles;
+  const uint2* ranges;
+  const uint32_t* sorted_vals;  // item id (atomic mode) or expansion index (deterministic mode)
+  const uint32_t* exp_item;     // expansion index -> item (deterministic mode)
+  const void* records;
+  float4* out_color;
+  float4* out_aux;
+  float4* out_normal;
+  uint32_t* out_nc;
+  const float4* dl_dcolor;
+  const float4* dl_dnormal;
+  float* grad_geom;
+  float* partials;
+  float lambda_dist;
+  uint32_t* tile_counter;       // persistent kernels: zeroed before each launch
+};
+// Blocks per SM the raster kernels sustain (for persistent grids).
+int raster_fwd_occupancy(int prec, int batch, bool det);
+int raster_bwd_occupancy(int prec, bool aux, bool det);
+
+int launch_project(const ProjectArgs& a, int prec, uint32_t n_views, cudaStream_t st);
+int launch_project_bwd(const ProjectBwdArgs& a, int prec, bool aux, cudaStream_t st);
+int launch_project_bwd_adam(const ProjectBwdArgs& a, const AdamFusedArgs& opt, int prec, bool aux, cudaStream_t st);
+int launch_raster_fwd(const RasterArgs& a, int prec, int batch, bool det, bool persistent, int grid, cudaStream_t st);
+int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, bool det, bool persistent, int grid, cudaStream_t st);
+
+// ---- sort / scan / binning (gs_sort.cu) ----
+// Scratch for the scan and the radix sort; sized by the caller through
+// scan_scratch_bytes / sort_scratch_bytes.
+constexpr int SCAN_GRID = 512;    // blocks of the chunked scan
+constexpr int SORT_GRID = 296;    // blocks of the chunked radix passes (2 per SM)
+size_t scan_scratch_bytes();
+size_t sort_scratch_bytes();
+
+// Exclusive scan of n u32 values read as in[perm ? perm[i] : i] (n from
+// n_dev when non-null, else n_host). Writes out[i], and the total to
+// total_u32 (saturated) / total_u64 when non-null.
+int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_t n_host, const uint32_t* n_dev,
+                uint32_t* total_u32, unsigned long long* total_u64, void* scratch, cudaStream_t st);
+// Stable LSD radix sort of (key, val) over bits [0, key_bits). Ping-pongs
+// between (k0,v0) and (k1,v1); returns in *result_in_1 where the output is.
+int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n_host, const uint32_t* n_dev,
+                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st);
+
+struct ExpandArgs {
+  const uint32_t* perm;        // depth-sorted item order
+  const uint32_t* counts;      // per item
+  const uint32_t* offsets;     // exclusive scan of counts in sorted order
+  const uint4* rects;          // per item
+  const ViewInfo* views;       // null for the standalone binner
+  uint32_t items_per_view;     // item / items_per_view = view (when views != null)
+  uint32_t tiles_x;            // standalone binner grid width
+  const uint32_t* n_items_dev; // null: n_items_host
+  uint32_t n_items_host;
+  const unsigned long long* total;  // entries
+  uint64_t capacity;
+  uint32_t* keys;              // tile id (relative to the launch's first view) per entry
+  uint32_t* vals;              // per val_mode: 0 item, 1 expansion index, 2 reference entry index
+  int val_mode;
+  uint32_t* exp_item;          // val_mode 1: expansion index -> item
+  uint32_t* entry_offset;      // item -> first expansion index, or null
+  const uint32_t* ref_offsets; // val_mode 2: exclusive scan of counts in item order
+  uint32_t* entry_items;       // val_mode 2: reference entry index -> item
+  uint32_t* error_word;
+};
+int launch_expand(const ExpandArgs& a, cudaStream_t st);
+// ranges[t] = [start, end) of tile t in the sorted key stream (ranges zeroed by the callee).
+int launch_ranges(const uint32_t* sorted_keys, const unsigned long long* total, uint64_t capacity, uint2* ranges,
+                  uint32_t num_tiles, cudaStream_t st);
+// After the entry scan: on overflow flag the error and zero the entry counts.
+int launch_entry_guard(unsigned long long* total, uint32_t* count, uint64_t capacity, uint32_t* error_word,
+                       cudaStream_t st);
+// Number of key bits needed for num_tiles tile ids.
+int tile_key_bits(uint32_t num_tiles);
+// dst[i] = src[idx[i]] for i < n (device n).
+int launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, const unsigned long long* n,
+                      uint64_t capacity, cudaStream_t st);
+
+// ---- loss, optimizer, densify ----
+struct SsimArgs {
+  const ViewInfo* views;
+  int n_views;
+  int total_tiles16;          // 16x16 tiles over all views
+  const float4* img;
+  const float4* target;
+  float* coef;                // 9 floats per pixel scratch
+  float4* dl_dcolor;
+  double* loss_sums;          // 2 per view
+  float w_l1, w_ssim;
+  float w[6];                 // Gaussian window taps 0..5 (set by the launcher)
+};
+int launch_ssim(const SsimArgs& a, cudaStream_t st);
+
+int launch_adam_grad(const AdamClass& c, const float* grad, uint64_t n, int activation, float beta1, float beta2,
+                     float eps, float bc1_inv, float bc2_inv, cudaStream_t st);
+int launch_activate_init(const AdamClass& c, uint64_t n, int activation, cudaStream_t st);
+int launch_to_half(const float* src, void* dst, uint64_t n, bool bf16, cudaStream_t st);
+
+struct DensifyArgs {
+  uint32_t n, capacity;
+  float grad_threshold, opacity_threshold;
+  float inv_steps;                 // 1 / steps accumulated
+  const float* accum;              // per-surfel Σ|dL/dpos|
+  const float* opacity_act;
+  uint32_t* flags;                 // per surfel: keep (bit0), clone (bit1)
+  uint32_t* slots;                 // scan scratch
+  // parameter classes to compact: raw, m, v, act, floats per surfel
+  float* arrays[20];
+  int widths[20];
+  int n_arrays;
+  float* tmp;                      // capacity * max width staging
+  uint32_t* n_out_dev;
+};
+int launch_densify(DensifyArgs& a, void* scan_scratch, cudaStream_t st);
+
+}  // namespace gs

@@ -1,0 +1,445 @@
+// Prefix scan, stable LSD radix sort and tile binning.
+//
+// The reference bins with count → scan → expand (item-major) → stable 32-bit
+// sort by depth → gather tile keys → stable 32-bit sort by tile → ranges
+// (crates/gs-kernels/src/binning.rs:171-238, tile_binning.wgsl:30-103,
+// crates/gs-wgpu/src/shaders/radix_sort.wgsl): sixteen 4-bit passes over the
+// entries, equivalent to one sort by (tile, depth, entry index).
+//
+// Here the depth order is established on the ITEMS (one per surfel and view,
+// 4 passes of 8 bits over N·V keys), items are expanded in that order, and
+// the entries are stably sorted by tile id alone (⌈log2 tiles / 8⌉ passes,
+// usually 2). Within one tile each item owns at most one entry and entry
+// indices grow with item index, so the result is exactly the reference's
+// (tile, depth, entry) order.
+//
+// All passes read element counts from device memory, so a step needs no host
+// synchronisation and can be captured in a CUDA graph. Every block of a
+// chunked pass handles a fixed contiguous share of the input; nothing waits
+// on another block.
+#include <cub/block/block_reduce.cuh>
+#include <cub/block/block_scan.cuh>
+
+#include "gs_common.cuh"
+#include "gs_kernels.h"
+
+namespace gs {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint64_t read_n(uint64_t n_host, const uint32_t* n_dev) {
+  if (n_dev == nullptr) return n_host;
+  uint64_t d = *n_dev;
+  return d < n_host ? d : n_host;
+}
+
+// ------------------------------------------------------------------ scan
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ uint32_t scan_in(const uint32_t* in, const uint32_t* perm, uint64_t i) {
+  return perm ? in[perm[i]] : in[i];
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t* in, const uint32_t* perm, uint64_t n_host,
+                                                              const uint32_t* n_dev, unsigned long long* bsum) {
+  const uint64_t n = read_n(n_host, n_dev);
+  const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
+  unsigned long long s = 0;
+  for (uint64_t i = beg + threadIdx.x; i < end; i += SCAN_THREADS) s += scan_in(in, perm, i);
+  using BR = cub::BlockReduce<unsigned long long, SCAN_THREADS>;
+  __shared__ typename BR::TempStorage tmp;
+  s = BR(tmp).Sum(s);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(SCAN_GRID) k_scan_blocks(unsigned long long* bsum, uint32_t* total_u32,
+                                                           unsigned long long* total_u64) {
+  using BS = cub::BlockScan<unsigned long long, SCAN_GRID>;
+  __shared__ typename BS::TempStorage tmp;
+  unsigned long long v = bsum[threadIdx.x], excl, agg;
+  BS(tmp).ExclusiveSum(v, excl, agg);
+  bsum[threadIdx.x] = excl;
+  if (threadIdx.x == 0) {
+    if (total_u32) *total_u32 = agg > 0xffffffffull ? 0xffffffffu : (uint32_t)agg;
+    if (total_u64) *total_u64 = agg;
+  }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t* in, const uint32_t* perm, uint32_t* out,
+                                                            uint64_t n_host, const uint32_t* n_dev,
+                                                            const unsigned long long* boff) {
+  const uint64_t n = read_n(n_host, n_dev);
+  const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
+  using BS = cub::BlockScan<uint32_t, SCAN_THREADS>;
+  __shared__ typename BS::TempStorage tmp;
+  uint32_t running = (uint32_t)boff[blockIdx.x];
+  for (uint64_t t0 = beg; t0 < end; t0 += SCAN_TILE) {
+    uint32_t v[SCAN_ITEMS];
+    uint32_t loc = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      const uint64_t i = t0 + (uint64_t)threadIdx.x * SCAN_ITEMS + k;
+      v[k] = i < end ? scan_in(in, perm, i) : 0u;
+      loc += v[k];
+    }
+    uint32_t excl, agg;
+    BS(tmp).ExclusiveSum(loc, excl, agg);
+    uint32_t r = running + excl;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      const uint64_t i = t0 + (uint64_t)threadIdx.x * SCAN_ITEMS + k;
+      if (i < end) out[i] = r;
+      r += v[k];
+    }
+    running += agg;
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------ radix sort
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ROUNDS = 16;                       // keys per thread per tile
+constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;     // 4096
+constexpr int RS_BINS = 256;
+
+// Lanes of the warp whose digit equals this lane's (multi-split by ballots).
+__device__ __forceinline__ uint32_t match_digit(uint32_t d, int nbits, uint32_t active) {
+  uint32_t peers = active;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    if (b < nbits) {
+      const uint32_t bit = (d >> b) & 1u;
+      const uint32_t bal = __ballot_sync(FULL, bit);
+      peers &= bit ? bal : ~bal;
+    }
+  }
+  return peers;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* keys, uint64_t n_host, const uint32_t* n_dev,
+                                                           int shift, int nbits, uint32_t* hist) {
+  __shared__ uint32_t s_hist[RS_WARPS][RS_BINS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_hist[0][0])[k] = 0;
+  __syncthreads();
+  const uint64_t n = read_n(n_host, n_dev);
+  const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
+  const uint32_t mask = (1u << nbits) - 1u;
+  for (uint64_t base = beg + (uint64_t)warp * 32; base < end; base += RS_THREADS) {
+    const uint64_t i = base + lane;
+    const bool valid = i < end;
+    const uint32_t d = valid ? (keys[i] >> shift) & mask : 0u;
+    const uint32_t act = __ballot_sync(FULL, valid);
+    const uint32_t peers = match_digit(d, nbits, act);
+    if (valid && (peers & lanemask_lt()) == 0) s_hist[warp][d] += __popc(peers);
+  }
+  __syncthreads();
+  for (int d = tid; d < RS_BINS; d += RS_THREADS) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) s += s_hist[w][d];
+    hist[(size_t)d * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// Single-block exclusive scan of m u32 values in place.
+__global__ void __launch_bounds__(1024) k_scan_small(uint32_t* a, int m) {
+  using BS = cub::BlockScan<uint32_t, 1024>;
+  __shared__ typename BS::TempStorage tmp;
+  const int per = (m + 1023) / 1024;
+  const int beg = threadIdx.x * per;
+  uint32_t s = 0;
+  for (int k = 0; k < per; ++k)
+    if (beg + k < m) s += a[beg + k];
+  uint32_t excl;
+  BS(tmp).ExclusiveSum(s, excl);
+  for (int k = 0; k < per; ++k)
+    if (beg + k < m) {
+      const uint32_t v = a[beg + k];
+      a[beg + k] = excl;
+      excl += v;
+    }
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __restrict__ kin,
+                                                             const uint32_t* __restrict__ vin,
+                                                             uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                             uint64_t n_host, const uint32_t* n_dev, int shift,
+                                                             int nbits, const uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_k[RS_TILE];
+  __shared__ uint32_t s_v[RS_TILE];
+  __shared__ uint32_t s_wh[RS_WARPS][RS_BINS];
+  __shared__ uint32_t s_start[RS_BINS], s_cnt[RS_BINS], s_run[RS_BINS], s_base[RS_BINS];
+  using BS = cub::BlockScan<uint32_t, RS_THREADS>;
+  __shared__ typename BS::TempStorage tmp;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t n = read_n(n_host, n_dev);
+  const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
+  if (beg >= end) return;
+  const uint32_t mask = (1u << nbits) - 1u;
+  for (int d = tid; d < RS_BINS; d += RS_THREADS) {
+    s_run[d] = 0;
+    s_base[d] = hist[(size_t)d * gridDim.x + blockIdx.x];
+  }
+  for (uint64_t t0 = beg; t0 < end; t0 += RS_TILE) {
+    const int tn = (int)min((uint64_t)RS_TILE, end - t0);
+    for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_wh[0][0])[k] = 0;
+    __syncthreads();
+    uint32_t key[RS_ROUNDS], val[RS_ROUNDS], pre[RS_ROUNDS];
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
+      const bool valid = idx < tn;
+      key[r] = valid ? kin[t0 + idx] : 0u;
+      val[r] = valid ? vin[t0 + idx] : 0u;
+      const uint32_t d = (key[r] >> shift) & mask;
+      const uint32_t act = __ballot_sync(FULL, valid);
+      const uint32_t peers = match_digit(d, nbits, act);
+      uint32_t basev = 0;
+      if (valid) basev = s_wh[warp][d];
+      __syncwarp();
+      if (valid && (peers & lanemask_lt()) == 0) s_wh[warp][d] = basev + __popc(peers);
+      __syncwarp();
+      pre[r] = basev + __popc(peers & lanemask_lt());
+    }
+    __syncthreads();
+    {
+      const int d = tid;  // RS_THREADS == RS_BINS
+      uint32_t s = 0;
+#pragma unroll
+      for (int w = 0; w < RS_WARPS; ++w) {
+        const uint32_t c = s_wh[w][d];
+        s_wh[w][d] = s;
+        s += c;
+      }
+      s_cnt[d] = s;
+      uint32_t excl;
+      BS(tmp).ExclusiveSum(s, excl);
+      s_start[d] = excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
+      if (idx < tn) {
+        const uint32_t d = (key[r] >> shift) & mask;
+        const uint32_t pos = s_start[d] + s_wh[warp][d] + pre[r];
+        s_k[pos] = key[r];
+        s_v[pos] = val[r];
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < tn; i += RS_THREADS) {
+      const uint32_t k = s_k[i];
+      const uint32_t d = (k >> shift) & mask;
+      const size_t g = (size_t)s_base[d] + s_run[d] + (uint32_t)(i - (int)s_start[d]);
+      kout[g] = k;
+      vout[g] = s_v[i];
+    }
+    __syncthreads();
+    s_run[tid] += s_cnt[tid];
+    __syncthreads();
+  }
+}
+
+// --------------------------------------------------------------- binning
+__global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
+  const uint64_t n = read_n(a.n_items_host, a.n_items_dev);
+  const uint64_t tot = *a.total;  // zeroed by the entry guard on overflow
+  if (tot == 0 || tot > a.capacity) return;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps_total = (uint64_t)gridDim.x * (blockDim.x / 32);
+  for (uint64_t w = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); w * 32 < n; w += warps_total) {
+    const uint64_t k0 = w * 32, k = k0 + lane;
+    const bool valid = k < n;
+    uint32_t item = 0, cnt = 0, x0 = 0, y0 = 0, wd = 1, tb = 0, tx = a.tiles_x;
+    if (valid) {
+      item = a.perm[k];
+      cnt = a.counts[item];
+      if (cnt) {
+        const uint4 r = a.rects[item];
+        x0 = r.x; y0 = r.y; wd = r.z - r.x + 1u;
+      }
+      if (a.views) {
+        const ViewInfo* V = a.views + item / a.items_per_view;
+        tb = (uint32_t)__ldg(&V->tile_base);
+        tx = (uint32_t)__ldg(&V->tiles_x);
+      }
+    }
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t excl = incl - cnt;
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    const uint32_t off0 = a.offsets[k0];
+    if ((uint64_t)off0 + total > a.capacity) {
+      if (lane == 0 && total) atomicOr(a.error_word, ERR_ENTRY_CAPACITY);
+      continue;
+    }
+    if (valid && a.entry_offset) a.entry_offset[item] = off0 + excl;
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t j = base + lane;
+      int owner = 0;
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) {
+        const int c = owner + s;
+        const uint32_t ec = __shfl_sync(FULL, excl, c < 32 ? c : 31);
+        if (c < 32 && ec <= j) owner = c;
+      }
+      const uint32_t o_excl = __shfl_sync(FULL, excl, owner);
+      const uint32_t o_wd = __shfl_sync(FULL, wd, owner);
+      const uint32_t o_x0 = __shfl_sync(FULL, x0, owner);
+      const uint32_t o_y0 = __shfl_sync(FULL, y0, owner);
+      const uint32_t o_item = __shfl_sync(FULL, item, owner);
+      const uint32_t o_tb = __shfl_sync(FULL, tb, owner);
+      const uint32_t o_tx = __shfl_sync(FULL, tx, owner);
+      if (j < total) {
+        const uint32_t local = j - o_excl;
+        const uint32_t ly = local / o_wd, lx = local - ly * o_wd;
+        const uint32_t pos = off0 + j;
+        a.keys[pos] = o_tb + (o_y0 + ly) * o_tx + (o_x0 + lx);
+        if (a.val_mode == 1) {
+          a.vals[pos] = pos;
+          a.exp_item[pos] = o_item;
+        } else if (a.val_mode == 2) {
+          const uint32_t e = a.ref_offsets[o_item] + local;
+          a.vals[pos] = e;
+          if (e < tot) a.entry_items[e] = o_item;
+        } else {
+          a.vals[pos] = o_item;
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ranges(const uint32_t* keys, const unsigned long long* total,
+                                                uint64_t capacity, uint2* ranges, uint32_t num_tiles) {
+  const uint64_t n = min((uint64_t)*total, capacity);
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = keys[p];
+    if (t >= num_tiles) continue;
+    if (p == 0 || keys[p - 1] != t) ranges[t].x = (uint32_t)p;
+    if (p == n - 1 || keys[p + 1] != t) ranges[t].y = (uint32_t)(p + 1);
+  }
+}
+
+// Entry-capacity guard, run right after the entry scan: when the scene needs
+// more entries than were allocated, flag GS_ERR_CAPACITY and set the entry
+// count to zero so no later pass reads an entry that was never written.
+__global__ void k_entry_guard(unsigned long long* total, uint32_t* count, uint64_t capacity, uint32_t* error_word) {
+  if (*total > capacity) {
+    atomicOr(error_word, ERR_ENTRY_CAPACITY);
+    *total = 0;
+    *count = 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_gather(const uint32_t* src, const uint32_t* idx, uint32_t* dst,
+                                                const unsigned long long* total, uint64_t capacity) {
+  const uint64_t n = min((uint64_t)*total, capacity);
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x)
+    dst[p] = src[idx[p]];
+}
+
+// Standalone binner: tiles per rect (tile_binning.wgsl:30-43), depth keys and
+// the identity permutation for the item sort.
+__global__ void __launch_bounds__(256) k_rect_counts(const uint4* rects, const uint32_t* depths, uint32_t n,
+                                                     uint32_t* counts, uint32_t* keys, uint32_t* vals) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint4 r = rects[i];
+    counts[i] = (r.z >= r.x && r.w >= r.y) ? (r.z - r.x + 1u) * (r.w - r.y + 1u) : 0u;
+    keys[i] = depths[i];
+    vals[i] = i;
+  }
+}
+
+int grid_for(uint64_t n_max, int per_block, int cap_blocks) {
+  uint64_t g = (n_max + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > (uint64_t)cap_blocks) g = cap_blocks;
+  return (int)g;
+}
+
+}  // namespace
+
+size_t scan_scratch_bytes() { return sizeof(unsigned long long) * SCAN_GRID; }
+size_t sort_scratch_bytes() { return sizeof(uint32_t) * RS_BINS * SORT_GRID; }
+
+int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_t n_host, const uint32_t* n_dev,
+                uint32_t* total_u32, unsigned long long* total_u64, void* scratch, cudaStream_t st) {
+  auto* bsum = reinterpret_cast<unsigned long long*>(scratch);
+  k_scan_reduce<<<SCAN_GRID, SCAN_THREADS, 0, st>>>(in, perm, n_host, n_dev, bsum);
+  k_scan_blocks<<<1, SCAN_GRID, 0, st>>>(bsum, total_u32, total_u64);
+  k_scan_down<<<SCAN_GRID, SCAN_THREADS, 0, st>>>(in, perm, out, n_host, n_dev, bsum);
+  return (int)cudaGetLastError();
+}
+
+int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n_host, const uint32_t* n_dev,
+                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st) {
+  auto* hist = reinterpret_cast<uint32_t*>(scratch);
+  uint32_t *ki = k0, *vi = v0, *ko = k1, *vo = v1;
+  int in1 = 0;
+  for (int shift = 0; shift < key_bits; shift += 8) {
+    const int nbits = key_bits - shift < 8 ? key_bits - shift : 8;
+    k_rs_upsweep<<<SORT_GRID, RS_THREADS, 0, st>>>(ki, n_host, n_dev, shift, nbits, hist);
+    k_scan_small<<<1, 1024, 0, st>>>(hist, RS_BINS * SORT_GRID);
+    k_rs_downsweep<<<SORT_GRID, RS_THREADS, 0, st>>>(ki, vi, ko, vo, n_host, n_dev, shift, nbits, hist);
+    uint32_t* t = ki; ki = ko; ko = t;
+    t = vi; vi = vo; vo = t;
+    in1 ^= 1;
+  }
+  *result_in_1 = in1;
+  return (int)cudaGetLastError();
+}
+
+int launch_expand(const ExpandArgs& a, cudaStream_t st) {
+  const int grid = grid_for((uint64_t)a.n_items_host, 256, 148 * 16);
+  k_expand<<<grid, 256, 0, st>>>(a);
+  return (int)cudaGetLastError();
+}
+
+int launch_ranges(const uint32_t* sorted_keys, const unsigned long long* total, uint64_t capacity, uint2* ranges,
+                  uint32_t num_tiles, cudaStream_t st) {
+  cudaMemsetAsync(ranges, 0, sizeof(uint2) * (size_t)num_tiles, st);
+  k_ranges<<<148 * 8, 256, 0, st>>>(sorted_keys, total, capacity, ranges, num_tiles);
+  return (int)cudaGetLastError();
+}
+
+int launch_entry_guard(unsigned long long* total, uint32_t* count, uint64_t capacity, uint32_t* error_word,
+                       cudaStream_t st) {
+  k_entry_guard<<<1, 1, 0, st>>>(total, count, capacity, error_word);
+  return (int)cudaGetLastError();
+}
+
+int launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, const unsigned long long* n,
+                      uint64_t capacity, cudaStream_t st) {
+  k_gather<<<148 * 8, 256, 0, st>>>(src, idx, dst, n, capacity);
+  return (int)cudaGetLastError();
+}
+
+int launch_rect_counts(const uint4* rects, const uint32_t* depths, uint32_t n, uint32_t* counts, uint32_t* keys,
+                       uint32_t* vals, cudaStream_t st) {
+  if (n == 0) return 0;
+  k_rect_counts<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(rects, depths, n, counts, keys, vals);
+  return (int)cudaGetLastError();
+}
+
+int tile_key_bits(uint32_t num_tiles) {
+  int b = 1;
+  while (b < 32 && (1ull << b) < (unsigned long long)num_tiles) ++b;
+  return b;
+}
+
+}  // namespace gs

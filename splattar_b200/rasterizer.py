@@ -1,0 +1,307 @@
+"""Host-side mirror of the reference's rasterizer surface over the C ABI.
+
+Names and argument meanings follow the reference's public items:
+``Rasterizer`` (crates/gs-kernels/src/rasterizer.rs:56-449), ``RasterCamera``
+(:34-41), ``SceneInput`` (:44-54), ``TileBinner`` (crates/gs-kernels/src/
+binning.rs:22-238), ``SsimLoss`` (first_attempt/crates/gs-train/src/ssim.rs)
+and ``Optimizer`` (first_attempt/crates/gs-train/src/optim.rs). The reference
+records into a wgpu command encoder; here every call is stream-ordered on a
+CUDA stream (``stream`` = a ``cudaStream_t`` as an int, 0 = default stream).
+Where the reference panics on a violated assert, these raise ``GsError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import (BUF, FLAG_COLOR_ONLY, FLAG_DETERMINISTIC, FLAG_PERSISTENT, PREC, AdamConfig, Camera,
+                   DensifyConfig, GsError, RasterConfig, SceneInputC, StepConfig, check, lib)
+
+SH_FLOATS = 48
+TILE = 16
+
+
+@dataclass
+class RasterCamera:
+    """Camera-to-world pose (``quat`` xyzw, normalised on upload), single focal
+    length in pixels, principal point at the image centre."""
+    center: tuple
+    quat: tuple
+    focal: float
+    sh_degree: int
+    width: int
+    height: int
+
+    def c(self) -> Camera:
+        cam = Camera()
+        for k in range(4):
+            cam.quat[k] = float(self.quat[k])
+        for k in range(3):
+            cam.center[k] = float(self.center[k])
+        cam.focal = float(self.focal)
+        cam.width = int(self.width)
+        cam.height = int(self.height)
+        cam.sh_degree = int(self.sh_degree)
+        return cam
+
+
+def camera_array(cams) -> C.Array:
+    if isinstance(cams, RasterCamera):
+        cams = [cams]
+    arr = (Camera * len(cams))()
+    for k, c in enumerate(cams):
+        arr[k] = c.c()
+    return arr
+
+
+def camera_rotation(cam: RasterCamera) -> np.ndarray:
+    """Column-major camera-to-world rotation exactly as the forward builds it."""
+    out = (C.c_float * 9)()
+    c = cam.c()
+    check(lib().gs_camera_rotation(C.byref(c), out))
+    return np.array(out[:], np.float32)
+
+
+@dataclass
+class SceneInput:
+    """Activated parameters, host arrays (float32)."""
+    positions: np.ndarray  # (n,3)
+    scales: np.ndarray     # (n,2)
+    quats: np.ndarray      # (n,4) xyzw
+    opacities: np.ndarray  # (n,)
+    sh: np.ndarray         # (n, sh_coeffs*3) coefficient-major rgb
+    sh_coeffs: int
+    _keep: list = field(default_factory=list, repr=False)
+
+    def c(self) -> SceneInputC:
+        arrs = [np.ascontiguousarray(a, np.float32) for a in
+                (self.positions, self.scales, self.quats, self.opacities, self.sh)]
+        self._keep = arrs
+        n = arrs[0].shape[0]
+        if not (arrs[1].shape == (n, 2) and arrs[2].shape == (n, 4) and arrs[3].shape == (n,)
+                and arrs[4].size == n * self.sh_coeffs * 3):
+            raise GsError(1, "SceneInput arrays disagree in length")
+        return SceneInputC(*[a.ctypes.data for a in arrs], self.sh_coeffs, n)
+
+
+_DTYPES = {
+    "out_ncontrib": np.uint32, "ranges": np.uint32, "sorted_items": np.uint32, "entry_count": np.uint64,
+    "loss": np.float64, "rects": np.uint32, "depth_keys": np.uint32, "depth_order": np.uint32,
+}
+
+
+class Rasterizer:
+    """Rasterizer::new(ctx, capacity, width, height, max_entries), plus the
+    batched-view and precision options of this build."""
+
+    def __init__(self, capacity: int, width: int, height: int, max_entries: int = 0, *, max_views: int = 1,
+                 max_pixels: int = 0, precision: str = "f32", deterministic: bool = False,
+                 persistent: bool = False, color_only: bool = False, batch: int = 128):
+        self._h = None
+        flags = (FLAG_DETERMINISTIC if deterministic else 0) | (FLAG_PERSISTENT if persistent else 0) | (
+            FLAG_COLOR_ONLY if color_only else 0)
+        cfg = RasterConfig(capacity, width, height, max_views, max_pixels, max_entries, 16, batch, PREC[precision],
+                           flags)
+        h = C.c_void_p()
+        check(lib().gs_rasterizer_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.capacity, self.width, self.height = capacity, width, height
+        self._lambda_dist = 0.0
+        self.cams = None
+
+    def close(self):
+        if self._h:
+            lib().gs_rasterizer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, status):
+        check(status, self._h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def lambda_dist(self) -> float:
+        return self._lambda_dist
+
+    @lambda_dist.setter
+    def lambda_dist(self, v: float):
+        self._lambda_dist = float(v)
+        self._chk(lib().gs_rasterizer_set_lambda_dist(self._h, float(v)))
+
+    def upload_scene(self, scene: SceneInput, stream: int = 0):
+        s = scene.c()
+        self._chk(lib().gs_rasterizer_upload_scene(self._h, C.byref(s), stream))
+
+    def forward(self, cameras, num_surfels: int, stream: int = 0):
+        self.cams = camera_array(cameras)
+        self._chk(lib().gs_rasterizer_forward(self._h, self.cams, len(self.cams), num_surfels, stream))
+
+    def backward(self, num_surfels: int, stream: int = 0):
+        self._chk(lib().gs_rasterizer_backward(self._h, num_surfels, stream))
+
+    def check(self, stream: int = 0):
+        """Synchronise and raise on a sticky device error (entry capacity, timeouts)."""
+        self._chk(lib().gs_rasterizer_check(self._h, stream))
+
+    def buffer(self, name: str):
+        p, n = C.c_void_p(), C.c_size_t()
+        self._chk(lib().gs_rasterizer_buffer(self._h, BUF[name], C.byref(p), C.byref(n)))
+        return p.value, n.value
+
+    def view_offset(self, view: int):
+        po, to = C.c_uint64(), C.c_uint32()
+        self._chk(lib().gs_rasterizer_view_offset(self._h, view, C.byref(po), C.byref(to)))
+        return po.value, to.value
+
+    def read(self, name: str, count: int, dtype=None, offset: int = 0, stream: int = 0) -> np.ndarray:
+        """Blocking readback of ``count`` elements (buffers::readback)."""
+        dt = np.dtype(dtype or _DTYPES.get(name, np.float32))
+        out = np.empty(count, dt)
+        self._chk(lib().gs_rasterizer_read(self._h, BUF[name], offset * dt.itemsize, out.ctypes.data, out.nbytes,
+                                           stream))
+        return out
+
+    def write(self, name: str, array: np.ndarray, offset_elems: int = 0, stream: int = 0):
+        """Blocking upload (queue.write_buffer)."""
+        a = np.ascontiguousarray(array)
+        self._chk(lib().gs_rasterizer_write(self._h, BUF[name], offset_elems * a.dtype.itemsize, a.ctypes.data,
+                                            a.nbytes, stream))
+
+    def read_async(self, name: str, host_ptr: int, nbytes: int, offset_bytes: int = 0, stream: int = 0):
+        self._chk(lib().gs_rasterizer_read_async(self._h, BUF[name], offset_bytes, host_ptr, nbytes, stream))
+
+    def write_async(self, name: str, host_ptr: int, nbytes: int, offset_bytes: int = 0, stream: int = 0):
+        self._chk(lib().gs_rasterizer_write_async(self._h, BUF[name], offset_bytes, host_ptr, nbytes, stream))
+
+    def entry_count(self) -> int:
+        return int(self.read("entry_count", 1)[0])
+
+    # --- SsimLoss::encode and Optimizer over the handle's buffers ---
+    def loss_l1_ssim(self, w_l1: float, w_ssim: float, stream: int = 0):
+        self._chk(lib().gs_loss_l1_ssim(self._h, w_l1, w_ssim, stream))
+
+    def optimizer_init(self, num_surfels: int, stream: int = 0):
+        self._chk(lib().gs_optimizer_init(self._h, num_surfels, stream))
+
+    def optimizer_step(self, adam: "AdamSettings", num_surfels: int, stream: int = 0):
+        cfg = adam.c()
+        self._chk(lib().gs_optimizer_step(self._h, C.byref(cfg), num_surfels, stream))
+
+    def train_step(self, cameras, num_surfels: int, step: "StepSettings", stream: int = 0):
+        cams = camera_array(cameras)
+        self.cams = cams
+        cfg = step.c()
+        self._chk(lib().gs_train_step(self._h, cams, len(cams), num_surfels, C.byref(cfg), stream))
+
+    STAGES = ("project", "depth_sort_scan", "expand", "tile_sort", "ranges", "raster_fwd", "l1_ssim",
+              "raster_bwd", "project_bwd_adam")
+
+    def train_step_profiled(self, cameras, num_surfels: int, step: "StepSettings", stream: int = 0) -> dict:
+        cams = camera_array(cameras)
+        self.cams = cams
+        cfg = step.c()
+        ms = (C.c_float * 9)()
+        ns = C.c_uint32()
+        self._chk(lib().gs_train_step_profiled(self._h, cams, len(cams), num_surfels, C.byref(cfg), stream, ms,
+                                               C.byref(ns)))
+        return {k: float(ms[i]) for i, k in enumerate(self.STAGES)}
+
+    def densify_prune(self, grad_threshold: float, opacity_threshold: float, num_surfels: int,
+                      stream: int = 0) -> int:
+        cfg = DensifyConfig(grad_threshold, opacity_threshold)
+        out = C.c_uint32()
+        self._chk(lib().gs_densify_prune(self._h, C.byref(cfg), num_surfels, C.byref(out), stream))
+        return out.value
+
+
+CLASSES = ("pos", "scales", "quat", "opacity", "sh")
+
+
+@dataclass
+class AdamSettings:
+    """Per-class learning rates and L1 priors of the trainer's five classes
+    (first_attempt/crates/gs-train/src/trainer.rs:757-761, defaults :471-476)."""
+    lr: dict = field(default_factory=lambda: {"pos": 1.6e-4, "scales": 5e-3, "quat": 1e-3, "opacity": 5e-2,
+                                              "sh": 2.5e-3})
+    reg: dict = field(default_factory=lambda: {k: 0.0 for k in CLASSES})
+    beta1: float = 0.9
+    beta2: float = 0.999
+    eps: float = 1e-8
+
+    def c(self) -> AdamConfig:
+        a = AdamConfig()
+        for k, name in enumerate(CLASSES):
+            a.lr[k] = float(self.lr[name])
+            a.reg[k] = float(self.reg.get(name, 0.0))
+        a.beta1, a.beta2, a.eps = self.beta1, self.beta2, self.eps
+        return a
+
+
+@dataclass
+class StepSettings:
+    w_l1: float = 0.8
+    w_ssim: float = 0.2
+    adam: AdamSettings = field(default_factory=AdamSettings)
+    form: str = "chosen"  # "plain" or "chosen"
+
+    def c(self) -> StepConfig:
+        return StepConfig(self.w_l1, self.w_ssim, self.adam.c(), 0 if self.form == "plain" else 1)
+
+
+class TileBinner:
+    """TileBinner::new(ctx, max_items, max_entries, num_tiles). ``encode`` takes
+    device pointers of uint4 rects and u32 depth keys (e.g. torch tensors'
+    ``data_ptr()``)."""
+
+    def __init__(self, max_items: int, max_entries: int, num_tiles: int):
+        self._h = None
+        h = C.c_void_p()
+        check(lib().gs_binner_create(max_items, max_entries, num_tiles, C.byref(h)))
+        self._h = h
+        self.num_tiles = num_tiles
+
+    def close(self):
+        if self._h:
+            lib().gs_binner_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def encode(self, rects_ptr: int, depths_ptr: int, num_items: int, tiles_x: int, stream: int = 0):
+        check(lib().gs_binner_encode(self._h, rects_ptr, depths_ptr, num_items, tiles_x, stream))
+
+    def buffer(self, which: str):
+        idx = {"sorted_entries": 0, "entry_items": 1, "ranges": 2, "entry_count": 3}[which]
+        p, n = C.c_void_p(), C.c_size_t()
+        check(lib().gs_binner_buffer(self._h, idx, C.byref(p), C.byref(n)))
+        return p.value, n.value
+
+
+def radix_sort_pairs(keys_ptr: int, vals_ptr: int, n: int, key_bits: int = 32, stream: int = 0):
+    """RadixSorter::encode on caller device arrays (stable, in place)."""
+    check(lib().gs_radix_sort_pairs(keys_ptr, vals_ptr, n, key_bits, stream))
+
+
+def exclusive_scan_u32(in_ptr: int, out_ptr: int, n: int, total_ptr: int = 0, stream: int = 0):
+    """PrefixSum::encode on caller device arrays."""
+    check(lib().gs_exclusive_scan_u32(in_ptr, out_ptr, n, total_ptr or None, stream))
+
+
+def adam_flat(raw_ptr, grad_ptr, m_ptr, v_ptr, act_ptr, n, activation, lr, beta1=0.9, beta2=0.999, eps=1e-8, reg=0.0,
+              t=1, stream=0):
+    check(lib().gs_adam_flat(raw_ptr, grad_ptr, m_ptr, v_ptr, act_ptr or None, n, activation, lr, beta1, beta2, eps,
+                             reg, t, stream))

@@ -1,0 +1,195 @@
+"""Finite-difference gate of the oracle, restating the reference's own gate
+(crates/gs-cpu-ref/tests/gradcheck.rs:109-326): central differences with an
+absolute step of 1e-6 against the analytic backward for every parameter class
+including the camera, tolerance 1e-7 + 1e-3·|g|, on the same seeded scenes.
+Plus the north_star's relative-step variant (step 1e-4·max(|x|, 1e-3)) on
+sampled parameters."""
+import numpy as np
+import pytest
+
+import oracle
+from scenes import XorShift, make_scene, make_weights
+
+
+class Checker:
+    def __init__(self, rel=1e-3, abs_=1e-7):
+        self.rel, self.abs = rel, abs_
+        self.worst, self.label = 0.0, ""
+
+    def check(self, label, analytic, fd):
+        denom = max(abs(analytic), abs(fd))
+        err = abs(analytic - fd)
+        rel = err / denom if denom > 1e-7 else 0.0
+        if err > 1e-7 and rel > self.worst:
+            self.worst, self.label = rel, label
+        assert err <= self.abs + self.rel * denom, f"{label}: analytic {analytic:.9e} vs fd {fd:.9e} (rel {rel:.2e})"
+
+
+def color_loss(scene, cam, w):
+    return float((oracle.render(scene, cam)["color"] * w).sum())
+
+
+def perturbations(scene, cam):
+    """(label, apply(scene, cam, delta)) for every differentiated scalar."""
+    out = []
+    n = scene.n
+    ncoef = (scene.sh_degree + 1) ** 2
+
+    def arr(name, i, d):
+        def f(s, c, h):
+            getattr(s, name)[i, d] += h
+        return f
+
+    for i in range(n):
+        out += [(f"pos[{i}][{d}]", "pos", (i, d), arr("pos", i, d)) for d in range(3)]
+        out += [(f"scale[{i}][{d}]", "scales", (i, d), arr("scales", i, d)) for d in range(2)]
+        out += [(f"quat[{i}][{d}]", "quat", (i, d), arr("quat", i, d)) for d in range(4)]
+
+        def op(s, c, h, i=i):
+            s.opacity[i] += h
+        out.append((f"opacity[{i}]", "opacity", (i,), op))
+        out += [(f"sh[{i}][{k}]", "sh", (i, k), arr("sh", i, k)) for k in range(3 * ncoef)]
+    for d in range(3):
+        def cc(s, c, h, d=d):
+            c.center[d] += h
+        out.append((f"cam_center[{d}]", "cam_center", (d,), cc))
+    for d in range(4):
+        def cq(s, c, h, d=d):
+            c.quat[d] += h
+        out.append((f"cam_quat[{d}]", "cam_quat", (d,), cq))
+
+    def cf(s, c, h):
+        c.focal += h
+    out.append(("focal", "focal", (), cf))
+    return out
+
+
+def analytic_value(g, key, idx):
+    v = g[key]
+    return float(v) if key == "focal" else float(v[idx])
+
+
+def grad_check(seed, n, deg, size, skip_camera_quat=False):
+    scene, cam = make_scene(seed, n, deg, size, focal=30, scale_hi=0.4)
+    w = make_weights(seed ^ 0xABCDEF, size * size)
+    g = oracle.gradients(scene, cam, w)
+    ck = Checker()
+    h = 1e-6
+    for label, key, idx, apply in perturbations(scene, cam):
+        sp, cp = scene.copy(), cam.copy()
+        sm, cm = scene.copy(), cam.copy()
+        apply(sp, cp, h)
+        apply(sm, cm, -h)
+        fd = (color_loss(sp, cp, w) - color_loss(sm, cm, w)) / (2 * h)
+        ck.check(label, analytic_value(g, key, idx), fd)
+    return ck
+
+
+@pytest.mark.parametrize("seed", [11, 23])
+def test_gradcheck_deg0_scenes(seed):
+    ck = grad_check(seed, 12, 0, 24)
+    assert ck.worst < 1e-3
+
+
+def test_gradcheck_deg1_scene():
+    grad_check(37, 10, 1, 24)
+
+
+def test_gradcheck_deg3_scene():
+    grad_check(53, 6, 3, 20)
+
+
+@pytest.mark.parametrize("seed,n,size", [(71, 10, 20), (83, 8, 24)])
+def test_gradcheck_aux_losses(seed, n, size):
+    """Depth, normal and depth-distortion adjoints (gradcheck.rs:232-326)."""
+    scene, cam = make_scene(seed, n, 0, size, focal=30, scale_hi=0.4)
+    P = size * size
+    wc = make_weights(seed ^ 0x11, P)
+    wn = make_weights(seed ^ 0x22, P)
+    rng = XorShift(seed ^ 0x33)
+    wd = np.array([rng.uniform(-0.3, 0.3) for _ in range(P)])
+    lam = 0.35
+
+    def loss(s, c):
+        o = oracle.render(s, c)
+        return float((o["color"] * wc).sum() + (o["depth"] * wd).sum() + (o["normal"] * wn).sum()) + \
+            lam * oracle.distortion_loss(s, c)
+
+    g = oracle.gradients(scene, cam, wc, wd, wn, lam)
+    ck = Checker()
+    h = 1e-6
+    for label, key, idx, apply in perturbations(scene, cam):
+        if key in ("sh", "cam_quat"):
+            continue  # the reference's aux gate covers pos/scale/quat/opacity/centre/focal
+        sp, cp, sm, cm = scene.copy(), cam.copy(), scene.copy(), cam.copy()
+        apply(sp, cp, h)
+        apply(sm, cm, -h)
+        ck.check("aux " + label, analytic_value(g, key, idx), (loss(sp, cp) - loss(sm, cm)) / (2 * h))
+    mag = np.abs(g["pos"]).sum() + np.abs(g["opacity"]).sum()
+    assert mag > 1e-2, "aux losses produced near-zero gradients: vacuous test"
+
+
+def test_relative_step_fd_sampled():
+    """Central differences with relative step 1e-4 on sampled parameters of a
+    larger micro-scene (the north_star's FD protocol at CPU-friendly size)."""
+    scene, cam = make_scene(97, 64, 3, 48)
+    w = make_weights(97 ^ 0x5A5A, 48 * 48)
+    g = oracle.gradients(scene, cam, w)
+    rng = np.random.default_rng(0)
+    ck = Checker(rel=2e-3, abs_=1e-6)
+    checked = jumps = 0
+    for key, shape in (("pos", (64, 3)), ("scales", (64, 2)), ("quat", (64, 4)), ("opacity", (64,)),
+                       ("sh", (64, 48))):
+        for _ in range(6):
+            idx = tuple(int(rng.integers(0, s)) for s in shape)
+            fd = fd_relative(scene, cam, w, key, idx)
+            if fd is None:
+                jumps += 1
+                continue
+            checked += 1
+            ck.check(f"{key}{idx}", float(g[key][idx]), fd)
+    assert checked >= 24 and jumps <= 6, (checked, jumps)
+
+
+def fd_relative(scene, cam, w, key, idx, rel=1e-4):
+    """Central difference with step rel·max(|x|, 1e-3); None when the loss has
+    a jump inside the step (a tile-rect truncation or an alpha-threshold
+    crossing), detected as disagreement between steps h and h/2."""
+    x0 = getattr(scene, key)[idx]
+    h = rel * max(abs(x0), 1e-3)
+
+    def fd_at(hh):
+        sp, sm = scene.copy(), scene.copy()
+        getattr(sp, key)[idx] += hh
+        getattr(sm, key)[idx] -= hh
+        return (color_loss(sp, cam, w) - color_loss(sm, cam, w)) / (2 * hh)
+
+    a, b = fd_at(h), fd_at(h / 2)
+    if abs(a - b) > 1e-3 * max(abs(a), abs(b)) + 1e-6:
+        return None
+    return b
+
+
+def test_forward_renders_something():
+    scene, cam = make_scene(99, 10, 1, 32, focal=30, scale_hi=0.4)
+    assert oracle.render(scene, cam)["alpha"].sum() > 1.0
+
+
+def test_literal_walk_equals_binned_walk():
+    """covers_pixel filtering of the full depth-sorted list (forward.rs:218-244)
+    and the per-tile list walk give identical images and contributor counts."""
+    scene, cam = make_scene(202, 20, 1, 64)
+    a = oracle.render(scene, cam, literal=True)
+    b = oracle.render(scene, cam, literal=False, threads=4)
+    for k in ("color", "alpha", "depth", "normal", "trans"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(a["ncontrib"], b["ncontrib"])
+
+
+def test_gradients_independent_of_thread_count():
+    scene, cam = make_scene(111, 15, 0, 48)
+    w = make_weights(5, 48 * 48)
+    g1 = oracle.gradients(scene, cam, w, threads=1)
+    g4 = oracle.gradients(scene, cam, w, threads=4)
+    for k in ("pos", "scales", "quat", "opacity", "sh", "cam_center", "cam_quat", "dl_dr_cam"):
+        assert np.array_equal(g1[k], g4[k]), k
