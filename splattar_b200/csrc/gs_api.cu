@@ -596,7 +596,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   }
   {
     float4* rec = nullptr;
-    ALLOC(rec, I * 5);
+    ALLOC(rec, I * REC_F4_F32);
     r->records = rec;
   }
   ALLOC(r->rects, I);

@@ -48,16 +48,12 @@ struct ViewInfo {
 // per-pixel intersection three 3-term dot products.
 //   r0 = (M, tn)  r1 = (Bu, px)  r2 = (Bv, py)
 //   r3 = (colour rgb, opacity)  r4 = (normal xyz, centre depth)
-struct RecF32 {
-  float4 r0, r1, r2, r3, r4;
-};
-// Mixed-precision record: geometry stays FP32 (it feeds a ratio of nearly
-// cancelling dot products), colour/opacity/normal/depth are stored as 16-bit.
-template <typename H>
-struct RecH {
-  float4 r0, r1, r2;
-  H a[8];  // r,g,b,opacity,nx,ny,nz,depth
-};
+//   bb = pixel box (x0, x1, y0, y1) outside which α < 1/255 for certain
+// FP32 record: 6 float4 = 96 B. Mixed-precision record: geometry and box stay
+// FP32 (the geometry feeds a ratio of nearly cancelling dot products),
+// colour/opacity/normal/depth are 16-bit: 5 float4 = 80 B.
+constexpr int REC_F4_F32 = 6;
+constexpr int REC_F4_H = 5;
 
 template <typename H> __device__ __forceinline__ float h2f(H x);
 template <> __device__ __forceinline__ float h2f<__half>(__half x) { return __half2float(x); }
@@ -66,16 +62,27 @@ template <typename H> __device__ __forceinline__ H f2h(float x);
 template <> __device__ __forceinline__ __half f2h<__half>(float x) { return __float2half_rn(x); }
 template <> __device__ __forceinline__ __nv_bfloat16 f2h<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
 
-// Loads record `idx` as five float4 (converting 16-bit fields).
+template <int PREC>
+__device__ __forceinline__ const float4* record_ptr(const void* recs, uint32_t idx) {
+  return reinterpret_cast<const float4*>(recs) + (size_t)idx * (PREC == 0 ? REC_F4_F32 : REC_F4_H);
+}
+
+// The α box of record `idx` (read first, so culled entries cost one load).
+template <int PREC>
+__device__ __forceinline__ float4 load_record_box(const void* recs, uint32_t idx) {
+  return __ldg(record_ptr<PREC>(recs, idx) + (PREC == 0 ? 5 : 4));
+}
+
+// Loads the geometry and appearance of record `idx` as five float4
+// (converting 16-bit fields).
 template <int PREC>
 __device__ __forceinline__ void load_record(const void* recs, uint32_t idx, float4& r0, float4& r1, float4& r2,
                                             float4& r3, float4& r4) {
+  const float4* p = record_ptr<PREC>(recs, idx);
   if constexpr (PREC == 0) {
-    const float4* p = reinterpret_cast<const float4*>(recs) + (size_t)idx * 5;
     r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2); r3 = __ldg(p + 3); r4 = __ldg(p + 4);
   } else {
     using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
-    const float4* p = reinterpret_cast<const float4*>(recs) + (size_t)idx * 4;
     r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2);
     float4 raw = __ldg(p + 3);
     const H* h = reinterpret_cast<const H*>(&raw);
@@ -86,23 +93,23 @@ __device__ __forceinline__ void load_record(const void* recs, uint32_t idx, floa
 
 template <int PREC>
 __device__ __forceinline__ void store_record(void* recs, uint32_t idx, float4 r0, float4 r1, float4 r2, float4 r3,
-                                             float4 r4) {
+                                             float4 r4, float4 box) {
+  float4* p = reinterpret_cast<float4*>(recs) + (size_t)idx * (PREC == 0 ? REC_F4_F32 : REC_F4_H);
   if constexpr (PREC == 0) {
-    float4* p = reinterpret_cast<float4*>(recs) + (size_t)idx * 5;
-    p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4;
+    p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = box;
   } else {
     using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
-    float4* p = reinterpret_cast<float4*>(recs) + (size_t)idx * 4;
     p[0] = r0; p[1] = r1; p[2] = r2;
     float4 raw;
     H* h = reinterpret_cast<H*>(&raw);
     h[0] = f2h<H>(r3.x); h[1] = f2h<H>(r3.y); h[2] = f2h<H>(r3.z); h[3] = f2h<H>(r3.w);
     h[4] = f2h<H>(r4.x); h[5] = f2h<H>(r4.y); h[6] = f2h<H>(r4.z); h[7] = f2h<H>(r4.w);
     p[3] = raw;
+    p[4] = box;
   }
 }
 
-inline size_t record_bytes(int prec) { return prec == 0 ? 80 : 64; }
+inline size_t record_bytes(int prec) { return prec == 0 ? 96 : 80; }
 
 // Per-surfel camera-space gradient layout written by the backward raster and
 // consumed by the projection backward ("grad_geom"). The backward raster

@@ -97,7 +97,7 @@ int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, bool det, bool pe
 // Scratch for the scan and the radix sort; sized by the caller through
 // scan_scratch_bytes / sort_scratch_bytes.
 constexpr int SCAN_GRID = 512;    // blocks of the chunked scan
-constexpr int SORT_GRID = 296;    // blocks of the chunked radix passes (2 per SM)
+constexpr int SORT_GRID = 592;    // blocks of the chunked radix passes (4 per SM, one wave)
 size_t scan_scratch_bytes();
 size_t sort_scratch_bytes();
 

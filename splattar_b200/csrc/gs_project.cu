@@ -148,6 +148,63 @@ __device__ __forceinline__ float3 sh_raw_color(const void* sh, size_t i, int deg
   return acc + f3(0.5f, 0.5f, 0.5f);
 }
 
+// Range of f·N(θ)/D(θ) over θ for N = a0 + a1 cosθ + a2 sinθ and
+// D = b0 + b1 cosθ + b2 sinθ > 0: the extremes solve
+// (a0 b1 − a1 b0) sinθ + (a2 b0 − a0 b2) cosθ + (a2 b1 − a1 b2) = 0.
+__device__ __forceinline__ void ratio_range(float a0, float a1, float a2, float b0, float b1, float b2, float& lo,
+                                            float& hi) {
+  const float P = a0 * b1 - a1 * b0, Q = a2 * b0 - a0 * b2, R = a2 * b1 - a1 * b2;
+  const float h = sqrtf(P * P + Q * Q);
+  // Interval bound, always valid: |N| ≤ |a0| + |(a1,a2)|, D ≥ b0 − |(b1,b2)|.
+  const float na = sqrtf(a1 * a1 + a2 * a2), dmin = b0 - sqrtf(b1 * b1 + b2 * b2);
+  float blo = (a0 - na) / (a0 - na < 0.f ? dmin : b0 + sqrtf(b1 * b1 + b2 * b2));
+  float bhi = (a0 + na) / (a0 + na > 0.f ? dmin : b0 + sqrtf(b1 * b1 + b2 * b2));
+  if (h > 1e-12f && fabsf(R) <= h) {
+    const float phi = atan2f(P, Q), dth = acosf(fminf(fmaxf(-R / h, -1.f), 1.f));
+    float s0, c0, s1, c1;
+    sincosf(phi + dth, &s0, &c0);
+    sincosf(phi - dth, &s1, &c1);
+    const float v0 = (a0 + a1 * c0 + a2 * s0) / (b0 + b1 * c0 + b2 * s0);
+    const float v1 = (a0 + a1 * c1 + a2 * s1) / (b0 + b1 * c1 + b2 * s1);
+    lo = fmaxf(fminf(v0, v1), blo);
+    hi = fminf(fmaxf(v0, v1), bhi);
+    if (!(lo <= hi)) { lo = blo; hi = bhi; }
+  } else {
+    lo = blo;
+    hi = bhi;
+  }
+}
+
+// Pixel-space bounding box of the region where the surfel can reach
+// α = o·ĝ ≥ 1/255 (the kernels' skip threshold): ĝ ≥ τ = 1/(255 o) holds
+// inside the screen low-pass disc (dx²+dy² ≤ ln(1/τ)) or where the ray hits
+// the surfel plane inside the disc u²+v² ≤ 2 ln(1/τ) in front of the near
+// plane — the perspective image of a 3D ellipse whose x and y extremes have a
+// closed form. The box is widened by a safety margin; it is used only to skip
+// evaluations that are guaranteed to fall below the threshold, so colours and
+// contributor counts are unchanged. Returns (x0, x1, y0, y1) in pixel
+// coordinates of pixel centres; an unbounded region gives ±1e30.
+__device__ __forceinline__ float4 alpha_bbox(const Cam& k, float3 c, float3 tu, float3 tv, float px, float py, float o) {
+  const float L = logf(255.0f * o) + 1e-3f;
+  if (!(L > 0.f)) return make_float4(1e30f, -1e30f, 1e30f, -1e30f);  // never reaches the threshold
+  const float rs = sqrtf(L);
+  float x0 = px - rs, x1 = px + rs, y0 = py - rs, y1 = py + rs;
+  const float r = sqrtf(2.0f * L);
+  // Ellipse c + r cosθ τu + r sinθ τv, depth D = −Z.
+  const float b0 = -c.z, b1 = -r * tu.z, b2 = -r * tv.z;
+  if (b0 - sqrtf(b1 * b1 + b2 * b2) <= NEAR_DEPTH * 1.01f + 1e-6f) return make_float4(-1e30f, 1e30f, -1e30f, 1e30f);
+  float lo, hi;
+  ratio_range(c.x, r * tu.x, r * tv.x, b0, b1, b2, lo, hi);
+  x0 = fminf(x0, k.cx + k.f * lo);
+  x1 = fmaxf(x1, k.cx + k.f * hi);
+  ratio_range(c.y, r * tu.y, r * tv.y, b0, b1, b2, lo, hi);
+  y0 = fminf(y0, k.cy - k.f * hi);
+  y1 = fmaxf(y1, k.cy - k.f * lo);
+  const float m = 1.0f;  // pixels of margin for rounding in the box and in the per-pixel evaluation
+  return make_float4(x0 - m - 1e-4f * fabsf(x0), x1 + m + 1e-4f * fabsf(x1), y0 - m - 1e-4f * fabsf(y0),
+                     y1 + m + 1e-4f * fabsf(y1));
+}
+
 template <int PREC>
 __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -217,9 +274,11 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float3 Bu = cross3(tv, c);
   const float3 Bv = cross3(c, tu);
   const float tn = -dot3(c, M);
+  const float o = __ldg(a.opac + i);
+  const float4 box = count ? alpha_bbox(k, c, tu, tv, px, py, o) : make_float4(1e30f, -1e30f, 1e30f, -1e30f);
   store_record<PREC>(a.records, item, make_float4(M.x, M.y, M.z, tn), make_float4(Bu.x, Bu.y, Bu.z, px),
-                     make_float4(Bv.x, Bv.y, Bv.z, py), make_float4(color.x, color.y, color.z, __ldg(a.opac + i)),
-                     make_float4(nrm.x, nrm.y, nrm.z, depth));
+                     make_float4(Bv.x, Bv.y, Bv.z, py), make_float4(color.x, color.y, color.z, o),
+                     make_float4(nrm.x, nrm.y, nrm.z, depth), box);
 }
 
 // dL/dq for the unnormalised quaternion from the first two columns of dL/dR_q

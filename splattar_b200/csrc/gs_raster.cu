@@ -3,11 +3,18 @@
 // Forward: crates/gs-kernels/src/shaders/rasterize_fwd.wgsl:20-85 with the hit
 // test of raster_common.wgsl:69-95. One CTA of 256 threads per 16×16 tile,
 // one pixel per thread; the tile's depth-sorted entries are staged in shared
-// memory in batches and composited front to back in FP32. Unlike the
-// reference the whole CTA stops as soon as every pixel has terminated
-// (__syncthreads_count), and the ray–splat intersection is evaluated from the
-// precomputed record (three 3-term dot products, one reciprocal, one exp):
-// ĝ = max(G_ray, G_screen) is taken as exp(−min(q_ray, q_screen)).
+// memory in batches and composited front to back in FP32. Beyond the
+// reference:
+//   * the whole CTA stops as soon as every pixel has terminated
+//     (__syncthreads_count);
+//   * while a batch is staged, entries whose α-box (the projection's
+//     conservative pixel box of α ≥ 1/255) misses the tile are dropped and
+//     the rest compacted, each keeping its original list position, and a
+//     pixel outside an entry's box skips it — exact, because such entries
+//     cannot reach the 1/255 threshold there;
+//   * the ray–splat intersection is evaluated from the precomputed record
+//     (three 3-term dot products, one reciprocal, one exp):
+//     ĝ = max(G_ray, G_screen) = exp(−min(q_ray, q_screen)).
 //
 // Backward: rasterize_bwd.wgsl:113-312. Each pixel walks its contributors in
 // reverse from the stored final transmittance and last-contributor index,
@@ -57,9 +64,72 @@ __device__ __forceinline__ Hit eval_hit(const float4& r0, const float4& r1, cons
   return h;
 }
 
+struct TileGeo {
+  int v, x, y, W, H;
+  bool inside;
+  float pxc, pyc, sx, sy;
+  float bx0, bx1, by0, by1;  // pixel-centre extent of the tile's in-image pixels
+  long long pix;
+};
+
+__device__ __forceinline__ TileGeo tile_geo(const RasterArgs& a, int tile) {
+  TileGeo g;
+  int v = 0;
+  while (v + 1 < a.n_views && tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
+  const ViewInfo* V = a.views + v;
+  const int tiles_x = __ldg(&V->tiles_x);
+  g.v = v;
+  g.W = __ldg(&V->width);
+  g.H = __ldg(&V->height);
+  const int lt = tile - __ldg(&V->tile_base);
+  const int x0 = (lt % tiles_x) * TILE, y0 = (lt / tiles_x) * TILE;
+  g.x = x0 + (threadIdx.x & 15);
+  g.y = y0 + (threadIdx.x >> 4);
+  g.inside = g.x < g.W && g.y < g.H;
+  const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
+  g.pxc = (float)g.x + 0.5f;
+  g.pyc = (float)g.y + 0.5f;
+  g.sx = -((g.pxc - cx) / f);  // s = −d
+  g.sy = (g.pyc - cy) / f;
+  g.bx0 = (float)x0 + 0.5f;
+  g.bx1 = (float)(min(x0 + TILE, g.W) - 1) + 0.5f;
+  g.by0 = (float)y0 + 0.5f;
+  g.by1 = (float)(min(y0 + TILE, g.H) - 1) + 0.5f;
+  g.pix = __ldg(&V->pix_base) + (long long)g.y * g.W + g.x;
+  return g;
+}
+
+__device__ __forceinline__ bool box_hits_tile(const float4& b, const TileGeo& g) {
+  return b.x <= g.bx1 && b.y >= g.bx0 && b.z <= g.by1 && b.w >= g.by0;
+}
+__device__ __forceinline__ bool box_has_pixel(const float4& b, float pxc, float pyc) {
+  return pxc >= b.x && pxc <= b.y && pyc >= b.z && pyc <= b.w;
+}
+
+// Compaction of the staged batch: returns this thread's slot among the kept
+// entries (valid when keep) and the number kept. Order is preserved.
+__device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(FULL, keep);
+  if (lane == 0) s_wcount[warp] = __popc(bal);
+  __syncthreads();
+  int off = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    const int c = s_wcount[w];
+    if (w < warp) off += c;
+    tot += c;
+  }
+  kept = tot;
+  return off + __popc(bal & lanemask_lt());
+}
+
 template <int BATCH, int PREC, bool DET, bool PERSIST>
 __global__ void __launch_bounds__(256) k_raster_fwd(RasterArgs a) {
-  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_r4[BATCH];
+  static_assert(BATCH <= 256, "one staging pass per batch");
+  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_r4[BATCH], s_bb[BATCH];
+  __shared__ int s_j[BATCH];
+  __shared__ int s_wcount[8];
   __shared__ int s_tile;
   const int tid = threadIdx.x;
   int tile = blockIdx.x;
@@ -70,37 +140,40 @@ __global__ void __launch_bounds__(256) k_raster_fwd(RasterArgs a) {
       tile = s_tile;
       if (tile >= a.total_tiles) return;
     }
-    int v = 0;
-    while (v + 1 < a.n_views && tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
-    const ViewInfo* V = a.views + v;
-    const int tiles_x = __ldg(&V->tiles_x), W = __ldg(&V->width), H = __ldg(&V->height);
-    const int lt = tile - __ldg(&V->tile_base);
-    const int x = (lt % tiles_x) * TILE + (tid & 15), y = (lt / tiles_x) * TILE + (tid >> 4);
-    const bool inside = x < W && y < H;
-    const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
-    const float pxc = (float)x + 0.5f, pyc = (float)y + 0.5f;
-    const float sx = -((pxc - cx) / f), sy = (pyc - cy) / f;  // s = −d
+    const TileGeo g = tile_geo(a, tile);
     const uint2 range = __ldg(&a.ranges[tile]);
     float T = 1.0f, cr = 0.f, cg = 0.f, cb = 0.f, aa = 0.f, ad = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
     uint32_t nc = 0;
-    bool done = !inside;
+    bool done = !g.inside;
     for (uint32_t base = range.x; base < range.y; base += BATCH) {
       if (__syncthreads_count(done) == 256) break;
       const int count = (int)min((uint32_t)BATCH, range.y - base);
-      for (int j = tid; j < count; j += 256) {
-        uint32_t item = __ldg(&a.sorted_vals[base + j]);
+      bool keep = false;
+      uint32_t item = 0;
+      float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (tid < count) {
+        item = __ldg(&a.sorted_vals[base + tid]);
         if (DET) item = __ldg(&a.exp_item[item]);
+        bb = load_record_box<PREC>(a.records, item);
+        keep = box_hits_tile(bb, g);
+      }
+      int kept;
+      const int slot = compact_slot(keep, s_wcount, kept);
+      if (keep) {
         float4 r0, r1, r2, r3, r4;
         load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
-        s_r0[j] = r0; s_r1[j] = r1; s_r2[j] = r2; s_r3[j] = r3; s_r4[j] = r4;
+        s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3; s_r4[slot] = r4;
+        s_bb[slot] = bb;
+        s_j[slot] = tid;
       }
       __syncthreads();
       if (!done) {
-        for (int j = 0; j < count; ++j) {
-          const float4 r0 = s_r0[j], r1 = s_r1[j], r2 = s_r2[j];
-          const float4 r4 = s_r4[j];
-          const Hit h = eval_hit(r0, r1, r2, r4.w, sx, sy, pxc, pyc);
-          const float4 r3 = s_r3[j];
+        for (int k = 0; k < kept; ++k) {
+          if (!box_has_pixel(s_bb[k], g.pxc, g.pyc)) continue;
+          const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
+          const float4 r4 = s_r4[k];
+          const Hit h = eval_hit(r0, r1, r2, r4.w, g.sx, g.sy, g.pxc, g.pyc);
+          const float4 r3 = s_r3[k];
           const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
           if (alpha < ALPHA_SKIP) continue;
           const float w = T * alpha;
@@ -109,17 +182,16 @@ __global__ void __launch_bounds__(256) k_raster_fwd(RasterArgs a) {
           ad += h.t * w;
           nx += r4.x * w; ny += r4.y * w; nz += r4.z * w;
           T = __fmul_rn(T, 1.0f - alpha);
-          nc = base - range.x + (uint32_t)j + 1u;
+          nc = base - range.x + (uint32_t)s_j[k] + 1u;
           if (T < T_TERMINATE) { done = true; break; }
         }
       }
     }
-    if (inside) {
-      const long long pix = __ldg(&V->pix_base) + (long long)y * W + x;
-      a.out_color[pix] = make_float4(cr, cg, cb, aa);
-      a.out_aux[pix] = make_float4(T, ad, 0.f, 0.f);
-      a.out_normal[pix] = make_float4(nx, ny, nz, 0.f);
-      a.out_nc[pix] = nc;
+    if (g.inside) {
+      a.out_color[g.pix] = make_float4(cr, cg, cb, aa);
+      a.out_aux[g.pix] = make_float4(T, ad, 0.f, 0.f);
+      a.out_normal[g.pix] = make_float4(nx, ny, nz, 0.f);
+      a.out_nc[g.pix] = nc;
     }
     if (!PERSIST) return;
     __syncthreads();
@@ -130,11 +202,14 @@ template <int BATCH, int PREC, bool AUX, bool DET, bool PERSIST>
 __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
   constexpr int NW = 8;
   constexpr int NG = AUX ? 32 : 16;  // reduced components per entry (AUX: 20 used)
-  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH];
+  constexpr int NQ = AUX ? 5 : 4;    // float4 groups per entry written out
+  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
   __shared__ float4 s_r4[AUX ? BATCH : 1];
   __shared__ uint32_t s_item[BATCH];
   __shared__ uint32_t s_q[DET ? BATCH : 1];
+  __shared__ int s_j[BATCH];
   __shared__ float s_part[NW][BATCH][NG];
+  __shared__ int s_wcount[8];
   __shared__ int s_tile, s_maxnc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int tile = blockIdx.x;
@@ -151,46 +226,45 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
       __syncthreads();
       continue;
     }
-    int v = 0;
-    while (v + 1 < a.n_views && tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
-    const ViewInfo* V = a.views + v;
-    const int tiles_x = __ldg(&V->tiles_x), W = __ldg(&V->width), H = __ldg(&V->height);
-    const int lt = tile - __ldg(&V->tile_base);
-    const int x = (lt % tiles_x) * TILE + (tid & 15), y = (lt / tiles_x) * TILE + (tid >> 4);
-    const bool inside = x < W && y < H;
-    const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
-    const float pxc = (float)x + 0.5f, pyc = (float)y + 0.5f;
-    const float sx = -((pxc - cx) / f), sy = (pyc - cy) / f;
-    const long long pix = __ldg(&V->pix_base) + (long long)y * W + x;
-
+    const TileGeo g = tile_geo(a, tile);
     float3 dlc = make_float3(0.f, 0.f, 0.f);
     float dld = 0.f, wtot = 0.f, wttot = 0.f;
     float3 dln = make_float3(0.f, 0.f, 0.f);
     float T = 1.0f;
     uint32_t nc = 0;
-    if (inside) {
-      const float4 g = a.dl_dcolor[pix];
-      dlc = make_float3(g.x, g.y, g.z);
-      const float4 aux = a.out_aux[pix];
+    if (g.inside) {
+      const float4 gc = a.dl_dcolor[g.pix];
+      dlc = make_float3(gc.x, gc.y, gc.z);
+      const float4 aux = a.out_aux[g.pix];
       T = aux.x;
-      nc = a.out_nc[pix];
+      nc = a.out_nc[g.pix];
       if (AUX) {
-        dld = g.w;
-        const float4 gn = a.dl_dnormal[pix];
+        dld = gc.w;
+        const float4 gn = a.dl_dnormal[g.pix];
         dln = make_float3(gn.x, gn.y, gn.z);
-        wtot = a.out_color[pix].w;
+        wtot = a.out_color[g.pix].w;
         wttot = aux.y;
       }
     }
-    bool has_loss = inside && (dlc.x != 0.f || dlc.y != 0.f || dlc.z != 0.f);
-    if (AUX) has_loss = inside && (has_loss || dld != 0.f || dln.x != 0.f || dln.y != 0.f || dln.z != 0.f ||
-                                   a.lambda_dist != 0.f);
+    bool has_loss = g.inside && (dlc.x != 0.f || dlc.y != 0.f || dlc.z != 0.f);
+    if (AUX) has_loss = g.inside && (has_loss || dld != 0.f || dln.x != 0.f || dln.y != 0.f || dln.z != 0.f ||
+                                     a.lambda_dist != 0.f);
     if (!has_loss) nc = 0;
     if (tid == 0) s_maxnc = 0;
     __syncthreads();
     if (nc) atomicMax(&s_maxnc, (int)nc);
     __syncthreads();
     const uint32_t maxnc = min((uint32_t)s_maxnc, range.y - range.x);
+
+    if (DET) {
+      // Entries past the tile's last contributor get zero partials.
+      for (uint32_t e = range.x + maxnc + tid; e < range.y; e += 256) {
+        const uint32_t q = __ldg(&a.sorted_vals[e]);
+        float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)q * GG_STRIDE);
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
 
     float3 suf_c = make_float3(0.f, 0.f, 0.f), suf_n = make_float3(0.f, 0.f, 0.f);
     float suf_d = 0.f, suf_w = 0.f, suf_cw = 0.f;
@@ -199,29 +273,46 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
     while (hi > range.x) {
       const uint32_t lo = (hi - range.x > (uint32_t)BATCH) ? hi - BATCH : range.x;
       const int count = (int)(hi - lo);
-      for (int j = tid; j < count; j += 256) {
-        uint32_t item = __ldg(&a.sorted_vals[lo + j]);
-        if (DET) { s_q[j] = item; item = __ldg(&a.exp_item[item]); }
-        s_item[j] = item;
+      bool keep = false;
+      uint32_t item = 0, q = 0;
+      float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (tid < count) {
+        item = __ldg(&a.sorted_vals[lo + tid]);
+        q = item;
+        if (DET) item = __ldg(&a.exp_item[q]);
+        bb = load_record_box<PREC>(a.records, item);
+        keep = box_hits_tile(bb, g);
+        if (DET && !keep) {
+          float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)q * GG_STRIDE);
+#pragma unroll
+          for (int k = 0; k < NQ; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      int kept;
+      const int slot = compact_slot(keep, s_wcount, kept);
+      if (keep) {
         float4 r0, r1, r2, r3, r4;
         load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
-        s_r0[j] = r0; s_r1[j] = r1; s_r2[j] = r2; s_r3[j] = r3;
-        if (AUX) s_r4[j] = r4;
+        s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
+        if (AUX) s_r4[slot] = r4;
+        s_bb[slot] = bb;
+        s_item[slot] = item;
+        if (DET) s_q[slot] = q;
+        s_j[slot] = tid;
       }
       __syncthreads();
-      for (int j = count - 1; j >= 0; --j) {
-        const uint32_t cidx = lo - range.x + (uint32_t)j;
-        float g[NG];
+      for (int k = kept - 1; k >= 0; --k) {
+        const uint32_t cidx = lo - range.x + (uint32_t)s_j[k];
+        float gg[NG];
 #pragma unroll
-        for (int k = 0; k < NG; ++k) g[k] = 0.f;
+        for (int c = 0; c < NG; ++c) gg[c] = 0.f;
         bool contrib = false;
-        if (has_loss && cidx < nc) {
-          const float4 r0 = s_r0[j], r1 = s_r1[j], r2 = s_r2[j], r3 = s_r3[j];
+        if (has_loss && cidx < nc && box_has_pixel(s_bb[k], g.pxc, g.pyc)) {
+          const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
-          float depth;
-          if (AUX) { r4 = s_r4[j]; depth = r4.w; }
-          else depth = 0.f;  // only feeds t in the screen branch, used by aux terms alone
-          const Hit h = eval_hit(r0, r1, r2, depth, sx, sy, pxc, pyc);
+          float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
+          if (AUX) { r4 = s_r4[k]; depth = r4.w; }
+          const Hit h = eval_hit(r0, r1, r2, depth, g.sx, g.sy, g.pxc, g.pyc);
           const float raw_alpha = __fmul_rn(r3.w, h.ghat);
           const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
           if (alpha >= ALPHA_SKIP) {
@@ -251,28 +342,28 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
               suf_n.x += r4.x * w; suf_n.y += r4.y * w; suf_n.z += r4.z * w;
               suf_w += w;
               suf_cw += coef * w;
-              g[17] = dln.x * w; g[18] = dln.y * w; g[19] = dln.z * w;
+              gg[17] = dln.x * w; gg[18] = dln.y * w; gg[19] = dln.z * w;
             }
             suf_c.x += r3.x * w; suf_c.y += r3.y * w; suf_c.z += r3.z * w;
             T = t_before;
-            g[11] = dlc.x * w; g[12] = dlc.y * w; g[13] = dlc.z * w;
+            gg[11] = dlc.x * w; gg[12] = dlc.y * w; gg[13] = dlc.z * w;
             if (raw_alpha <= ALPHA_CLAMP) {
-              g[14] = dl_dalpha * h.ghat;
+              gg[14] = dl_dalpha * h.ghat;
               const float dl_dghat = dl_dalpha * r3.w;
               if (h.ray) {
                 const float gu = -h.u * h.ghat * dl_dghat;
                 const float gv = -h.v * h.ghat * dl_dghat;
                 const float gun = gu * h.inv_det, gvn = gv * h.inv_det;
                 const float gdet = -(h.u * gu + h.v * gv + (AUX ? h.t * dl_dt : 0.f)) * h.inv_det;
-                g[0] = gdet * sx; g[1] = gdet * sy; g[2] = gdet;
-                g[3] = gun * sx; g[4] = gun * sy; g[5] = gun;
-                g[6] = gvn * sx; g[7] = gvn * sy; g[8] = gvn;
-                if (AUX) g[15] = dl_dt * h.inv_det;
+                gg[0] = gdet * g.sx; gg[1] = gdet * g.sy; gg[2] = gdet;
+                gg[3] = gun * g.sx; gg[4] = gun * g.sy; gg[5] = gun;
+                gg[6] = gvn * g.sx; gg[7] = gvn * g.sy; gg[8] = gvn;
+                if (AUX) gg[15] = dl_dt * h.inv_det;
               } else {
-                const float k = h.ghat * dl_dghat / LOWPASS_SIGMA2;
-                g[9] = (pxc - r1.w) * k;
-                g[10] = (pyc - r2.w) * k;
-                if (AUX) g[16] = dl_dt;
+                const float kk = h.ghat * dl_dghat / LOWPASS_SIGMA2;
+                gg[9] = (g.pxc - r1.w) * kk;
+                gg[10] = (g.pyc - r2.w) * kk;
+                if (AUX) gg[16] = dl_dt;
               }
             }
           }
@@ -280,37 +371,36 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
         if (__any_sync(FULL, contrib)) {
           float lo16[16];
 #pragma unroll
-          for (int k = 0; k < 16; ++k) lo16[k] = g[k];
+          for (int c = 0; c < 16; ++c) lo16[c] = gg[c];
           const float r = warp_reduce16(lo16);
-          if (!(lane & 1)) s_part[warp][j][lane >> 1] = r;
+          if (!(lane & 1)) s_part[warp][k][lane >> 1] = r;
           if (AUX) {
             float hi16[16];
 #pragma unroll
-            for (int k = 0; k < 16; ++k) hi16[k] = g[16 + k];
+            for (int c = 0; c < 16; ++c) hi16[c] = gg[16 + c];
             const float r2 = warp_reduce16(hi16);
-            if (!(lane & 1)) s_part[warp][j][16 + (lane >> 1)] = r2;
+            if (!(lane & 1)) s_part[warp][k][16 + (lane >> 1)] = r2;
           }
         } else {
-          if (lane < 16) s_part[warp][j][lane] = 0.f;
-          if (AUX && lane >= 16) s_part[warp][j][lane] = 0.f;
+          if (lane < 16) s_part[warp][k][lane] = 0.f;
+          if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
         }
       }
       __syncthreads();
       // Cross-warp sum in fixed warp order, then one vector reduction (or
       // one ordered store) per 4 components.
-      constexpr int NQ = AUX ? 5 : 4;  // float4 groups per entry
-      for (int w4 = tid; w4 < count * NQ; w4 += 256) {
-        const int j = w4 / NQ, q4 = w4 % NQ;
+      for (int w4 = tid; w4 < kept * NQ; w4 += 256) {
+        const int k = w4 / NQ, q4 = w4 % NQ;
         float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
         for (int ww = 0; ww < NW; ++ww) {
-          s0 += s_part[ww][j][4 * q4]; s1 += s_part[ww][j][4 * q4 + 1];
-          s2 += s_part[ww][j][4 * q4 + 2]; s3 += s_part[ww][j][4 * q4 + 3];
+          s0 += s_part[ww][k][4 * q4]; s1 += s_part[ww][k][4 * q4 + 1];
+          s2 += s_part[ww][k][4 * q4 + 2]; s3 += s_part[ww][k][4 * q4 + 3];
         }
         if (DET) {
-          reinterpret_cast<float4*>(a.partials + (size_t)s_q[j] * GG_STRIDE)[q4] = make_float4(s0, s1, s2, s3);
+          reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[q4] = make_float4(s0, s1, s2, s3);
         } else if (s0 != 0.f || s1 != 0.f || s2 != 0.f || s3 != 0.f) {
-          red_add_v4(a.grad_geom + (size_t)s_item[j] * GG_STRIDE + 4 * q4, s0, s1, s2, s3);
+          red_add_v4(a.grad_geom + (size_t)s_item[k] * GG_STRIDE + 4 * q4, s0, s1, s2, s3);
         }
       }
       __syncthreads();
@@ -333,13 +423,14 @@ void fwd_batch(const RasterArgs& a, int batch, int grid, cudaStream_t st) {
   else fwd_launch<128, PREC, DET, PERSIST>(a, grid, st);
 }
 
+// The per-warp partial buffer is NW*BATCH*NG floats of static shared memory,
+// so the backward stages 32 entries at a time with aux losses and 64 without.
+template <bool AUX>
+constexpr int bwd_batch() { return AUX ? 32 : 64; }
+
 template <int PREC, bool AUX, bool DET, bool PERSIST>
 void bwd_launch(const RasterArgs& a, int grid, cudaStream_t st) {
-  // The per-warp partial buffer is NW*BATCH*NG floats of static shared
-  // memory, so the backward stages 32 entries at a time with aux losses and
-  // 64 without.
-  if constexpr (AUX) k_raster_bwd<32, PREC, AUX, DET, PERSIST><<<grid, 256, 0, st>>>(a);
-  else k_raster_bwd<64, PREC, AUX, DET, PERSIST><<<grid, 256, 0, st>>>(a);
+  k_raster_bwd<bwd_batch<AUX>(), PREC, AUX, DET, PERSIST><<<grid, 256, 0, st>>>(a);
 }
 
 template <typename K>
@@ -360,7 +451,7 @@ int raster_fwd_occupancy(int prec, int batch, bool det) {
 }
 
 int raster_bwd_occupancy(int prec, bool aux, bool det) {
-#define GS_O(P, X, D) occ(k_raster_bwd<(X ? 32 : 64), P, X, D, true>)
+#define GS_O(P, X, D) occ(k_raster_bwd<bwd_batch<X>(), P, X, D, true>)
 #define GS_O2(P) (aux ? (det ? GS_O(P, true, true) : GS_O(P, true, false)) : (det ? GS_O(P, false, true) : GS_O(P, false, false)))
   return prec == 0 ? GS_O2(0) : (prec == 1 ? GS_O2(1) : GS_O2(2));
 #undef GS_O2

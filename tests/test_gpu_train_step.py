@@ -1,0 +1,173 @@
+"""The training step end to end: batched multi-view passes against per-view
+passes, the chosen form against the plain form, mixed-precision storage
+against the f64 oracle (image PSNR, gradient relative error), and
+deterministic-mode reproducibility."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_util import f32_cam, f32_scene, raster_camera, scene_input
+from scenes import make_scene
+from splattar_b200 import AdamSettings, Rasterizer, StepSettings
+from splattar_b200.synthetic import look_at, make_surfels
+
+pytestmark = pytest.mark.gpu
+
+
+def multi_view_setup(seed=21, n=400):
+    scene, cam = make_scene(seed, n, 3, 64)
+    cams = []
+    for k, (w, h) in enumerate([(64, 64), (80, 48), (40, 72)]):
+        c = cam.copy()
+        c.width, c.height = w, h
+        c.quat = np.array(cam.quat) + np.array([0.02 * k, -0.01 * k, 0.0, 0.0])
+        cams.append(c)
+    return scene, cams
+
+
+def psnr(a, b):
+    mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
+    return 99.0 if mse == 0 else -10 * np.log10(mse)
+
+
+def test_batched_forward_equals_per_view_forward():
+    scene, cams = multi_view_setup()
+    P = sum(c.width * c.height for c in cams)
+    rc = [raster_camera(c, 3) for c in cams]
+    rb = Rasterizer(scene.n, 0, 0, 0, max_views=3, max_pixels=P)
+    rb.upload_scene(scene_input(scene))
+    rb.forward(rc, scene.n)
+    rb.check()
+    allc = rb.read("out_color", 4 * P).reshape(P, 4)
+    allnc = rb.read("out_ncontrib", P)
+    for v, c in enumerate(cams):
+        off, _ = rb.view_offset(v)
+        rs = Rasterizer(scene.n, c.width, c.height)
+        rs.upload_scene(scene_input(scene))
+        rs.forward(rc[v], scene.n)
+        rs.check()
+        Pv = c.width * c.height
+        assert np.array_equal(rs.read("out_color", 4 * Pv).reshape(Pv, 4), allc[off:off + Pv])
+        assert np.array_equal(rs.read("out_ncontrib", Pv), allnc[off:off + Pv])
+
+
+def _trainer(scene, cams, precision="f32", deterministic=False):
+    P = sum(c.width * c.height for c in cams)
+    r = Rasterizer(scene.n, 0, 0, 0, max_views=len(cams), max_pixels=P, precision=precision,
+                   deterministic=deterministic, color_only=True)
+    r.upload_scene(scene_input(scene))
+    tgt = np.random.default_rng(1).uniform(0, 1, (P, 4)).astype(np.float32)
+    r.write("target", tgt.ravel())
+    r.optimizer_init(scene.n)
+    return r
+
+
+def _params(r, n):
+    return {k: r.read(k, w * n) for k, w in (("raw_pos", 4), ("raw_scales", 2), ("raw_quat", 4),
+                                             ("raw_opacity", 1), ("raw_sh", 48))}
+
+
+def test_chosen_step_matches_plain_step_fp32():
+    scene, cams = multi_view_setup()
+    rc = [raster_camera(c, 3) for c in cams]
+    adam = AdamSettings(eps=1e-15)
+    outs = []
+    for form in ("plain", "chosen"):
+        r = _trainer(scene, cams)
+        for _ in range(2):
+            r.train_step(rc, scene.n, StepSettings(0.8, 0.2, adam, form))
+        r.check()
+        outs.append((_params(r, scene.n), r.read("loss", 6)))
+    (pa, la), (pb, lb) = outs
+    assert np.allclose(la, lb, rtol=1e-5, atol=1e-6)
+    for k in pa:
+        d = np.abs(pa[k] - pb[k])
+        # Adam normalises each step to ~lr; differences come from float
+        # reduction order of the per-surfel gradient sums only.
+        assert d.max() < 2e-4, (k, float(d.max()))
+
+
+def test_gradient_sum_over_views_matches_oracle():
+    """Backward over a 3-view forward = Σ over views of the oracle's single-view gradients."""
+    scene, cams = multi_view_setup(33, 60)
+    P = sum(c.width * c.height for c in cams)
+    rc = [raster_camera(c, 3) for c in cams]
+    r = Rasterizer(scene.n, 0, 0, 0, max_views=3, max_pixels=P)
+    r.upload_scene(scene_input(scene))
+    r.forward(rc, scene.n)
+    rng = np.random.default_rng(4)
+    w = rng.uniform(-1, 1, (P, 3))
+    r.write("dl_dcolor", np.concatenate([w, np.zeros((P, 1))], 1).astype(np.float32).ravel())
+    r.write("dl_dnormal", np.zeros(4 * P, np.float32))
+    r.backward(scene.n)
+    r.check()
+    n = scene.n
+    g = r.read("grad_pos", 4 * n).reshape(n, 4)[:, :3]
+    want = np.zeros((n, 3))
+    off = 0
+    for c in cams:
+        Pv = c.width * c.height
+        want += oracle.gradients(f32_scene(scene), f32_cam(c), w[off:off + Pv])["pos"]
+        off += Pv
+    err = np.abs(g - want)
+    assert np.all(err <= 1e-5 + 2e-3 * np.maximum(np.abs(g), np.abs(want)))
+
+
+@pytest.mark.parametrize("precision,min_psnr", [("f16", 60.0), ("bf16", 45.0)])
+def test_mixed_precision_image_psnr_vs_f64_oracle(precision, min_psnr):
+    s = make_surfels(20_000, 11, True, 3, 0.1)
+    cam = look_at((0.0, 0.0, 4.0), (0, 0, 0), 320, 240, sh_degree=3)
+    r = Rasterizer(s.n, 320, 240, precision=precision)
+    r.upload_scene(s.scene_input())
+    # the forward through the public API uses the handle's storage precision
+    r.forward(cam, s.n)
+    r.check()
+    img = r.read("out_color", 4 * 320 * 240).reshape(-1, 4)[:, :3]
+    sc = oracle.Scene(s.positions.astype(np.float64), s.scales.astype(np.float64), s.quats.astype(np.float64),
+                      s.opacities.astype(np.float64), s.sh48().astype(np.float64), 3)
+    oc = oracle.Camera(np.array(cam.center, np.float32).astype(np.float64),
+                       np.array(cam.quat, np.float32).astype(np.float64), float(np.float32(cam.focal)), 320, 240)
+    ref = oracle.render(sc, oc)["color"]
+    p = psnr(img, ref)
+    print(f"{precision}: PSNR {p:.1f} dB vs the f64 oracle")
+    assert p >= min_psnr
+
+
+def test_deterministic_step_is_bitwise_reproducible():
+    scene, cams = multi_view_setup(44, 300)
+    rc = [raster_camera(c, 3) for c in cams]
+    outs = []
+    for _ in range(2):
+        r = _trainer(scene, cams, deterministic=True)
+        for _ in range(2):
+            r.train_step(rc, scene.n, StepSettings(form="chosen"))
+        r.check()
+        outs.append(_params(r, scene.n))
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_train_step_reduces_loss():
+    """A few chosen-form steps toward a target rendered from a perturbed scene lower the loss."""
+    scene, cams = multi_view_setup(55, 300)
+    rc = [raster_camera(c, 3) for c in cams]
+    P = sum(c.width * c.height for c in cams)
+    tgt_scene = scene.copy()
+    tgt_scene.pos = tgt_scene.pos + 0.02
+    rt = Rasterizer(scene.n, 0, 0, 0, max_views=3, max_pixels=P)
+    rt.upload_scene(scene_input(tgt_scene))
+    rt.forward(rc, scene.n)
+    target = rt.read("out_color", 4 * P)
+    r = Rasterizer(scene.n, 0, 0, 0, max_views=3, max_pixels=P, color_only=True)
+    r.upload_scene(scene_input(scene))
+    r.write("target", target)
+    r.optimizer_init(scene.n)
+    losses = []
+    for _ in range(30):
+        r.train_step(rc, scene.n, StepSettings(0.8, 0.2, AdamSettings(lr={"pos": 1e-3, "scales": 5e-3,
+                                                                         "quat": 1e-3, "opacity": 5e-2,
+                                                                         "sh": 2.5e-3}), "chosen"))
+        l = r.read("loss", 6)
+        losses.append(sum(0.8 * l[2 * v] / (3 * c.width * c.height) + 0.2 * (1 - l[2 * v + 1] / (3 * c.width * c.height))
+                          for v, c in enumerate(cams)))
+    assert losses[-1] < 0.8 * losses[0], losses[::5]
