@@ -47,7 +47,10 @@ typedef enum { GS_PREC_F32 = 0, GS_PREC_F16 = 1, GS_PREC_BF16 = 2 } gs_precision
 enum {
   GS_FLAG_DETERMINISTIC = 1u << 0, /* ordered per-entry gradient reduction, no float atomics */
   GS_FLAG_PERSISTENT = 1u << 1,    /* persistent raster kernels over a global tile queue */
-  GS_FLAG_COLOR_ONLY = 1u << 2     /* backward ignores dl_dcolor.w, dl_dnormal and lambda_dist */
+  GS_FLAG_COLOR_ONLY = 1u << 2,    /* backward ignores dl_dcolor.w, dl_dnormal and lambda_dist */
+  GS_FLAG_TIGHT_BINNING = 1u << 3  /* bin a surfel only into the tiles its alpha >= 1/255 box overlaps: images and
+                                      gradients are unchanged; tile lists, ranges and OUT_NCONTRIB then refer to the
+                                      shorter lists instead of the reference's conservative rects */
 };
 
 /* Rasterizer::new(ctx, capacity, width, height, max_entries)
@@ -204,9 +207,10 @@ gs_status gs_adam_flat(float* raw, const float* grad_act, float* m, float* v, fl
  * out-of-scope appearance, pose and noise stages): forward over n_views
  * cameras, L1+SSIM against TARGET, backward summing over views, Adam.
  * form 0 = plain: views one at a time, FP32, separate kernels per stage.
- * form 1 = chosen: all views batched in one pass per stage, persistent raster
- *          kernels, projection backward fused with Adam, storage precision
- *          from the config, the whole step replayed as one CUDA graph. */
+ * form 1 = chosen: all views batched in one pass per stage, tight binning
+ *          (GS_FLAG_TIGHT_BINNING), persistent raster kernels, projection
+ *          backward fused with Adam, storage precision from the config, the
+ *          whole step replayed as one CUDA graph. */
 typedef struct {
   float w_l1;
   float w_ssim;

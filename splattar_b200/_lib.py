@@ -19,6 +19,7 @@ PREC = {"f32": 0, "f16": 1, "bf16": 2}
 FLAG_DETERMINISTIC = 1
 FLAG_PERSISTENT = 2
 FLAG_COLOR_ONLY = 4
+FLAG_TIGHT_BINNING = 8
 
 BUF = {
     "positions": 0, "scales": 1, "quats": 2, "opacities": 3, "sh": 4, "out_color": 5, "out_aux": 6,

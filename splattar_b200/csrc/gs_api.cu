@@ -64,7 +64,7 @@ struct gs_rasterizer {
   uint64_t max_pixels = 0, max_entries = 0, max_items = 0;
   uint32_t max_tiles = 0;
   float lambda_dist = 0.f;
-  bool det = false, persistent = false, color_only = false;
+  bool det = false, persistent = false, color_only = false, tight = false;
   std::string err;
 
   // activated parameters (fp32) and the 16-bit SH copy
@@ -276,7 +276,7 @@ const void* sh_for(gs_rasterizer* r, int prec) { return prec == 0 ? (const void*
 // Projection + binning + forward raster for `nv` views starting at views_dev
 // (already uploaded), `tiles` tiles in total, storage precision `prec`.
 gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vhost, uint32_t nv, int tiles, uint32_t n,
-                      int prec, bool persistent, cudaStream_t st, Prof* prof = nullptr) {
+                      int prec, bool persistent, bool tight, cudaStream_t st, Prof* prof = nullptr) {
   const uint32_t items = nv * n;
   mark(prof, -1, st);
   ProjectArgs pa{};
@@ -285,6 +285,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   pa.sh = sh_for(r, prec);
   pa.records = r->records; pa.rects = r->rects;
   pa.keys = r->item_keys[0]; pa.vals = r->item_vals[0]; pa.counts = r->counts;
+  pa.tight = tight ? 1 : 0;
   TRY_LAUNCH(r, launch_project(pa, prec, nv, st));
   mark(prof, 0, st);
   int in1 = 0;
@@ -470,7 +471,7 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   const ViewInfo* vdev = r->views_dev;
   int tiles = 0;
   for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
-  gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, st, prof);
+  gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, prof);
   if (s) return s;
   TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
   s = run_loss(r, vdev, r->views_batched.data(), nv, cfg->w_l1, cfg->w_ssim, r->loss_sums, st);
@@ -503,7 +504,7 @@ gs_status plain_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_co
     const ViewInfo* vd = r->views_dev + r->max_views + v;
     const ViewInfo& vi = r->views_single[v];
     const int tiles = vi.tiles_x * vi.tiles_y;
-    s = run_forward(r, vd, &r->views_single[v], 1, tiles, n, 0, false, st, prof);
+    s = run_forward(r, vd, &r->views_single[v], 1, tiles, n, 0, false, false, st, prof);
     if (s) return s;
     s = run_loss(r, vd, &r->views_single[v], 1, cfg->w_l1, cfg->w_ssim, r->loss_sums + 2 * v, st);
     if (s) return s;
@@ -574,6 +575,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   r->det = (c.flags & GS_FLAG_DETERMINISTIC) != 0;
   r->persistent = (c.flags & GS_FLAG_PERSISTENT) != 0;
   r->color_only = (c.flags & GS_FLAG_COLOR_ONLY) != 0;
+  r->tight = (c.flags & GS_FLAG_TIGHT_BINNING) != 0;
   auto bail = [&](cudaError_t e, const char* what) {
     std::string m = std::string("allocation of ") + what + " failed: " + cudaGetErrorString(e);
     gs_rasterizer_destroy(r);
@@ -709,7 +711,8 @@ gs_status gs_rasterizer_forward(gs_rasterizer* r, const gs_camera* cams, uint32_
   int tiles = 0;
   for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
   r->last_batched = true;
-  return run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, (int)r->cfg.precision, r->persistent, st);
+  return run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, (int)r->cfg.precision, r->persistent,
+                     r->tight, st);
 }
 
 gs_status gs_rasterizer_backward(gs_rasterizer* r, uint32_t n, void* stream) {

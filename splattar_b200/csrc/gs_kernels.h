@@ -22,6 +22,7 @@ struct ProjectArgs {
   uint32_t* keys;
   uint32_t* vals;
   uint32_t* counts;
+  int tight;              // bin only tiles the α-box overlaps (contributor indices then refer to that list)
 };
 
 struct ProjectBwdArgs {

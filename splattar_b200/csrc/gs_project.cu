@@ -267,6 +267,26 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     rect = make_uint4(x0, y0, x1, y1);
     count = (x1 - x0 + 1u) * (y1 - y0 + 1u);
   }
+  const float o = __ldg(a.opac + i);
+  const float4 box = count ? alpha_bbox(k, c, tu, tv, px, py, o) : make_float4(1e30f, -1e30f, 1e30f, -1e30f);
+  if (a.tight && count) {
+    // Tight binning: only the tiles of the reference rect that the α-box
+    // overlaps. Tile t holds pixel centres [16t + 0.5, 16t + 15.5].
+    const float lim = 1e8f;
+    const float fx0 = ceilf((fminf(fmaxf(box.x, -lim), lim) - 15.5f) / tf);
+    const float fx1 = floorf((fminf(fmaxf(box.y, -lim), lim) - 0.5f) / tf);
+    const float fy0 = ceilf((fminf(fmaxf(box.z, -lim), lim) - 15.5f) / tf);
+    const float fy1 = floorf((fminf(fmaxf(box.w, -lim), lim) - 0.5f) / tf);
+    const int tx0 = max((int)x0, (int)fmaxf(fx0, -1.f)), tx1 = min((int)x1, (int)fminf(fx1, 1e7f));
+    const int ty0 = max((int)y0, (int)fmaxf(fy0, -1.f)), ty1 = min((int)y1, (int)fminf(fy1, 1e7f));
+    if (tx0 <= tx1 && ty0 <= ty1) {
+      rect = make_uint4(tx0, ty0, tx1, ty1);
+      count = (uint32_t)(tx1 - tx0 + 1) * (uint32_t)(ty1 - ty0 + 1);
+    } else {
+      rect = make_uint4(1u, 1u, 0u, 0u);
+      count = 0;
+    }
+  }
   a.rects[item] = rect;
   a.keys[item] = __float_as_uint(depth);
   a.counts[item] = count;
@@ -274,8 +294,6 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float3 Bu = cross3(tv, c);
   const float3 Bv = cross3(c, tu);
   const float tn = -dot3(c, M);
-  const float o = __ldg(a.opac + i);
-  const float4 box = count ? alpha_bbox(k, c, tu, tv, px, py, o) : make_float4(1e30f, -1e30f, 1e30f, -1e30f);
   store_record<PREC>(a.records, item, make_float4(M.x, M.y, M.z, tn), make_float4(Bu.x, Bu.y, Bu.z, px),
                      make_float4(Bv.x, Bv.y, Bv.z, py), make_float4(color.x, color.y, color.z, o),
                      make_float4(nrm.x, nrm.y, nrm.z, depth), box);

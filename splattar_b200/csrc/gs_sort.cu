@@ -102,10 +102,16 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t* in, 
 }
 
 // ------------------------------------------------------------ radix sort
+// Reduce-then-scan LSD passes of 8-bit digits. Every block owns a contiguous
+// chunk of the input and walks it in tiles of RS_TILE keys; within a tile,
+// warp w holds keys [256w, 256w+256) in 8 rounds of 32 (all loads issued
+// before any ranking), ranks them stably by ballot multi-split, and the block
+// combines the warps' digit counts in warp order. The per-(digit, block)
+// counts are scanned between the upsweep and the downsweep.
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ROUNDS = 16;                       // keys per thread per tile
-constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;     // 4096
+constexpr int RS_ROUNDS = 8;                        // keys per thread per tile
+constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;     // 2048
 constexpr int RS_BINS = 256;
 
 // Lanes of the warp whose digit equals this lane's (multi-split by ballots).
@@ -122,8 +128,9 @@ __device__ __forceinline__ uint32_t match_digit(uint32_t d, int nbits, uint32_t 
   return peers;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* keys, uint64_t n_host, const uint32_t* n_dev,
-                                                           int shift, int nbits, uint32_t* hist) {
+__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* __restrict__ keys, uint64_t n_host,
+                                                           const uint32_t* n_dev, int shift, int nbits,
+                                                           uint32_t* __restrict__ hist) {
   __shared__ uint32_t s_hist[RS_WARPS][RS_BINS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_hist[0][0])[k] = 0;
@@ -132,51 +139,41 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* keys,
   const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
   const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
   const uint32_t mask = (1u << nbits) - 1u;
-  for (uint64_t base = beg + (uint64_t)warp * 32; base < end; base += RS_THREADS) {
-    const uint64_t i = base + lane;
-    const bool valid = i < end;
-    const uint32_t d = valid ? (keys[i] >> shift) & mask : 0u;
-    const uint32_t act = __ballot_sync(FULL, valid);
-    const uint32_t peers = match_digit(d, nbits, act);
-    if (valid && (peers & lanemask_lt()) == 0) s_hist[warp][d] += __popc(peers);
+  for (uint64_t t0 = beg; t0 < end; t0 += RS_TILE) {
+    uint32_t d[RS_ROUNDS];
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const uint64_t i = t0 + warp * (RS_ROUNDS * 32) + r * 32 + lane;
+      d[r] = i < end ? (__ldg(keys + i) >> shift) & mask : 0xffffffffu;
+    }
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const bool valid = d[r] != 0xffffffffu;
+      const uint32_t act = __ballot_sync(FULL, valid);
+      if (act == 0) break;
+      const uint32_t peers = match_digit(d[r], nbits, act);
+      if (valid && (peers & lanemask_lt()) == 0) s_hist[warp][d[r]] += __popc(peers);
+    }
   }
   __syncthreads();
-  for (int d = tid; d < RS_BINS; d += RS_THREADS) {
+  for (int dd = tid; dd < RS_BINS; dd += RS_THREADS) {
     uint32_t s = 0;
 #pragma unroll
-    for (int w = 0; w < RS_WARPS; ++w) s += s_hist[w][d];
-    hist[(size_t)d * gridDim.x + blockIdx.x] = s;
+    for (int w = 0; w < RS_WARPS; ++w) s += s_hist[w][dd];
+    hist[(size_t)dd * gridDim.x + blockIdx.x] = s;
   }
 }
 
-// Single-block exclusive scan of m u32 values in place.
-__global__ void __launch_bounds__(1024) k_scan_small(uint32_t* a, int m) {
-  using BS = cub::BlockScan<uint32_t, 1024>;
-  __shared__ typename BS::TempStorage tmp;
-  const int per = (m + 1023) / 1024;
-  const int beg = threadIdx.x * per;
-  uint32_t s = 0;
-  for (int k = 0; k < per; ++k)
-    if (beg + k < m) s += a[beg + k];
-  uint32_t excl;
-  BS(tmp).ExclusiveSum(s, excl);
-  for (int k = 0; k < per; ++k)
-    if (beg + k < m) {
-      const uint32_t v = a[beg + k];
-      a[beg + k] = excl;
-      excl += v;
-    }
-}
-
-__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __restrict__ kin,
-                                                             const uint32_t* __restrict__ vin,
-                                                             uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                             uint64_t n_host, const uint32_t* n_dev, int shift,
-                                                             int nbits, const uint32_t* __restrict__ hist) {
+__global__ void __launch_bounds__(RS_THREADS, 4) k_rs_downsweep(const uint32_t* __restrict__ kin,
+                                                                const uint32_t* __restrict__ vin,
+                                                                uint32_t* __restrict__ kout,
+                                                                uint32_t* __restrict__ vout, uint64_t n_host,
+                                                                const uint32_t* n_dev, int shift, int nbits,
+                                                                const uint32_t* __restrict__ hist) {
   __shared__ uint32_t s_k[RS_TILE];
   __shared__ uint32_t s_v[RS_TILE];
   __shared__ uint32_t s_wh[RS_WARPS][RS_BINS];
-  __shared__ uint32_t s_start[RS_BINS], s_cnt[RS_BINS], s_run[RS_BINS], s_base[RS_BINS];
+  __shared__ uint32_t s_start[RS_BINS], s_gofs[RS_BINS], s_run[RS_BINS];
   using BS = cub::BlockScan<uint32_t, RS_THREADS>;
   __shared__ typename BS::TempStorage tmp;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -185,21 +182,25 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
   const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
   if (beg >= end) return;
   const uint32_t mask = (1u << nbits) - 1u;
-  for (int d = tid; d < RS_BINS; d += RS_THREADS) {
-    s_run[d] = 0;
-    s_base[d] = hist[(size_t)d * gridDim.x + blockIdx.x];
-  }
+  s_run[tid] = hist[(size_t)tid * gridDim.x + blockIdx.x];  // RS_THREADS == RS_BINS
   for (uint64_t t0 = beg; t0 < end; t0 += RS_TILE) {
     const int tn = (int)min((uint64_t)RS_TILE, end - t0);
-    for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_wh[0][0])[k] = 0;
-    __syncthreads();
-    uint32_t key[RS_ROUNDS], val[RS_ROUNDS], pre[RS_ROUNDS];
+    uint32_t key[RS_ROUNDS], val[RS_ROUNDS];
 #pragma unroll
     for (int r = 0; r < RS_ROUNDS; ++r) {
       const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
       const bool valid = idx < tn;
-      key[r] = valid ? kin[t0 + idx] : 0u;
-      val[r] = valid ? vin[t0 + idx] : 0u;
+      key[r] = valid ? __ldg(kin + t0 + idx) : 0u;
+      val[r] = valid ? __ldg(vin + t0 + idx) : 0u;
+    }
+#pragma unroll
+    for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_wh[0][0])[k] = 0;
+    __syncthreads();
+    uint32_t pre[RS_ROUNDS];
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
+      const bool valid = idx < tn;
       const uint32_t d = (key[r] >> shift) & mask;
       const uint32_t act = __ballot_sync(FULL, valid);
       const uint32_t peers = match_digit(d, nbits, act);
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
     }
     __syncthreads();
     {
-      const int d = tid;  // RS_THREADS == RS_BINS
+      const int d = tid;
       uint32_t s = 0;
 #pragma unroll
       for (int w = 0; w < RS_WARPS; ++w) {
@@ -220,10 +221,11 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
         s_wh[w][d] = s;
         s += c;
       }
-      s_cnt[d] = s;
       uint32_t excl;
       BS(tmp).ExclusiveSum(s, excl);
       s_start[d] = excl;
+      s_gofs[d] = s_run[d] - excl;  // global position = s_gofs[d] + position in the tile
+      s_run[d] += s;
     }
     __syncthreads();
 #pragma unroll
@@ -237,15 +239,13 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
       }
     }
     __syncthreads();
+#pragma unroll 4
     for (int i = tid; i < tn; i += RS_THREADS) {
       const uint32_t k = s_k[i];
-      const uint32_t d = (k >> shift) & mask;
-      const size_t g = (size_t)s_base[d] + s_run[d] + (uint32_t)(i - (int)s_start[d]);
+      const size_t g = (size_t)(s_gofs[(k >> shift) & mask] + (uint32_t)i);
       kout[g] = k;
       vout[g] = s_v[i];
     }
-    __syncthreads();
-    s_run[tid] += s_cnt[tid];
     __syncthreads();
   }
 }
@@ -375,7 +375,7 @@ int grid_for(uint64_t n_max, int per_block, int cap_blocks) {
 }  // namespace
 
 size_t scan_scratch_bytes() { return sizeof(unsigned long long) * SCAN_GRID; }
-size_t sort_scratch_bytes() { return sizeof(uint32_t) * RS_BINS * SORT_GRID; }
+size_t sort_scratch_bytes() { return sizeof(uint32_t) * RS_BINS * SORT_GRID + scan_scratch_bytes(); }
 
 int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_t n_host, const uint32_t* n_dev,
                 uint32_t* total_u32, unsigned long long* total_u64, void* scratch, cudaStream_t st) {
@@ -394,7 +394,9 @@ int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, ui
   for (int shift = 0; shift < key_bits; shift += 8) {
     const int nbits = key_bits - shift < 8 ? key_bits - shift : 8;
     k_rs_upsweep<<<SORT_GRID, RS_THREADS, 0, st>>>(ki, n_host, n_dev, shift, nbits, hist);
-    k_scan_small<<<1, 1024, 0, st>>>(hist, RS_BINS * SORT_GRID);
+    const int e = launch_scan(hist, nullptr, hist, (uint64_t)RS_BINS * SORT_GRID, nullptr, nullptr, nullptr,
+                              hist + RS_BINS * SORT_GRID, st);
+    if (e) return e;
     k_rs_downsweep<<<SORT_GRID, RS_THREADS, 0, st>>>(ki, vi, ko, vo, n_host, n_dev, shift, nbits, hist);
     uint32_t* t = ki; ki = ko; ko = t;
     t = vi; vi = vo; vo = t;
