@@ -200,6 +200,7 @@ def run_ours(args, ws, rank, local):
     rast.write("target", target)
     rast.upload_scene(wl.surfels.scene_input())
     rast.optimizer_init(n)
+    tuned = rast.autotune(cams, n)
     adam = AdamSettings(eps=1e-15)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
@@ -264,7 +265,7 @@ def run_ours(args, ws, rank, local):
     stages = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
     n_tiles = sum(((c.width + 15) // 16) * ((c.height + 15) // 16) for c in cams)
     rast.check(sp)
-    result = dict(wl=wl, n=n, nv=nv, P=P, E=E, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
+    result = dict(tuned=tuned, wl=wl, n=n, nv=nv, P=P, E=E, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
                   stages=stages, n_tiles=n_tiles, loss=loss_vals, h2d=tgt_host.numel() * 4,
                   d2h=loss_host.numel() * 8)
     rast.close()
@@ -322,6 +323,7 @@ def main():
             "adam": "lr pos 1.6e-4 scales 5e-3 quat 1e-3 opacity 5e-2 sh 2.5e-3, betas 0.9/0.999, eps 1e-15",
             "l2": "inputs larger than L2 (params+optimizer state ~1.5 GB, tile entries ~%.1f GB)" % (E * 16 / 1e9),
             "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+            "autotuned": r["tuned"],
         },
         "mpix_per_s": round(steps_s * P / 1e6 * ws, 2),
         "plain": None if r["ms_plain"] is None else {

@@ -70,6 +70,8 @@ typedef struct {
   uint32_t batch;       /* shared-memory staging depth of the raster kernels: 64, 128 or 256 (0 = 128) */
   uint32_t precision;   /* gs_precision */
   uint32_t flags;       /* GS_FLAG_* */
+  uint32_t pixels_per_thread; /* forward raster: 1 or 2 vertically adjacent pixels per thread (0 = 2, or 1 with
+                                 batch 256) */
 } gs_raster_config;
 
 /* RasterCamera (crates/gs-kernels/src/rasterizer.rs:34-41) plus the image
@@ -227,6 +229,15 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t n_view
  * 7 backward raster, 8 projection backward + Adam. */
 gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
                                  const gs_step_config* cfg, void* stream, float stage_ms[9], uint32_t* n_stages);
+
+/* Autotuner: times the forward raster over staging batch {64,128,256} x
+ * {1,2} pixels per thread and the backward raster over (pixels per thread,
+ * batch) {(1,64),(2,64),(2,128)} on these cameras (the batched form, tight
+ * binning, the config's precision) and keeps the fastest for this handle.
+ * out = {fwd batch, fwd pixels/thread, bwd batch, bwd pixels/thread}. Tile
+ * size is fixed at 16 in this build. Blocking. */
+gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels, void* stream,
+                      uint32_t out[4]);
 
 /* Densify/prune compaction (no reference counterpart; the reference only
  * relocates at fixed budget, trainer.rs:1558-1689): surfels whose mean

@@ -39,7 +39,8 @@ class GsError(RuntimeError):
 class RasterConfig(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("max_views", C.c_uint32),
                 ("max_pixels", C.c_uint64), ("max_entries", C.c_uint64), ("tile", C.c_uint32),
-                ("batch", C.c_uint32), ("precision", C.c_uint32), ("flags", C.c_uint32)]
+                ("batch", C.c_uint32), ("precision", C.c_uint32), ("flags", C.c_uint32),
+                ("pixels_per_thread", C.c_uint32)]
 
 
 class Camera(C.Structure):
@@ -99,6 +100,7 @@ def lib():
         "gs_train_step_profiled": [vp, C.POINTER(Camera), u32, u32, C.POINTER(StepConfig), vp,
                                    C.POINTER(C.c_float), C.POINTER(u32)],
         "gs_densify_prune": [vp, C.POINTER(DensifyConfig), u32, C.POINTER(u32), vp],
+        "gs_autotune": [vp, C.POINTER(Camera), u32, u32, vp, C.POINTER(u32)],
         "gs_binner_create": [u32, u64, u32, C.POINTER(vp)],
         "gs_binner_destroy": [vp],
         "gs_binner_encode": [vp, vp, vp, u32, u32, vp],
@@ -137,6 +139,6 @@ def exported_symbols() -> list[str]:
         "gs_rasterizer_forward", "gs_rasterizer_backward", "gs_rasterizer_buffer", "gs_rasterizer_view_offset",
         "gs_rasterizer_read", "gs_rasterizer_write", "gs_rasterizer_read_async", "gs_rasterizer_write_async",
         "gs_rasterizer_check", "gs_last_error", "gs_loss_l1_ssim", "gs_optimizer_init", "gs_optimizer_step",
-        "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_binner_create", "gs_binner_destroy",
+        "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_binner_create", "gs_binner_destroy",
         "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_exclusive_scan_u32",
         "gs_camera_rotation", "gs_shutdown"]

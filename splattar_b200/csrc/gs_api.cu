@@ -18,7 +18,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/gs_cuda.h"
+#include "gs_cuda.h"
 #include "gs_common.cuh"
 #include "gs_kernels.h"
 
@@ -65,6 +65,8 @@ struct gs_rasterizer {
   uint32_t max_tiles = 0;
   float lambda_dist = 0.f;
   bool det = false, persistent = false, color_only = false, tight = false;
+  // Raster launch shapes (autotuned): staging batch and pixels per thread.
+  int fwd_batch = 128, fwd_ppt = 1, bwd_batch = 128, bwd_ppt = 2;
   std::string err;
 
   // activated parameters (fp32) and the 16-bit SH copy
@@ -320,13 +322,13 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ra.records = r->records;
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.tile_counter = r->words + 2;
-  const int batch = r->cfg.batch ? (int)r->cfg.batch : 128;
+  const int batch = r->fwd_batch, ppt = r->fwd_ppt;
   int grid = tiles;
   if (persistent) {
     TRY_CUDA(r, cudaMemsetAsync(r->words + 2, 0, sizeof(uint32_t), st));
-    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(prec, batch, r->det));
+    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(prec, batch, ppt, r->det));
   }
-  TRY_LAUNCH(r, launch_raster_fwd(ra, prec, batch, r->det, persistent, grid, st));
+  TRY_LAUNCH(r, launch_raster_fwd(ra, prec, batch, ppt, r->det, persistent, grid, st));
   mark(prof, 5, st);
   r->last_nv = nv; r->last_n = n; r->last_tiles = tiles; r->last_views_dev = vdev; r->last_views_host = vhost;
   r->have_forward = true;
@@ -353,9 +355,9 @@ gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t n
   int grid = tiles;
   if (persistent) {
     TRY_CUDA(r, cudaMemsetAsync(r->words + 3, 0, sizeof(uint32_t), st));
-    grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(prec, aux, r->det));
+    grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(prec, aux, r->bwd_ppt, r->bwd_batch, r->det));
   }
-  TRY_LAUNCH(r, launch_raster_bwd(ra, prec, aux, r->det, persistent, grid, st));
+  TRY_LAUNCH(r, launch_raster_bwd(ra, prec, aux, r->bwd_ppt, r->bwd_batch, r->det, persistent, grid, st));
   return GS_OK;
 }
 
@@ -553,6 +555,9 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   if (c.max_views > MAX_VIEWS_HARD) return fail(nullptr, GS_ERR_INVALID_ARG, "max_views > 64");
   if (c.batch == 0) c.batch = 128;
   if (c.batch != 64 && c.batch != 128 && c.batch != 256) return fail(nullptr, GS_ERR_INVALID_ARG, "batch must be 64/128/256");
+  if (c.pixels_per_thread == 0) c.pixels_per_thread = 1;
+  if (c.pixels_per_thread > 2 || (c.pixels_per_thread == 2 && c.batch == 256))
+    return fail(nullptr, GS_ERR_INVALID_ARG, "pixels_per_thread must be 1, or 2 with batch 64/128");
   if (c.precision > 2) return fail(nullptr, GS_ERR_INVALID_ARG, "bad precision");
   if (c.max_pixels == 0) c.max_pixels = (uint64_t)c.width * c.height * c.max_views;
   if (c.max_pixels == 0) return fail(nullptr, GS_ERR_INVALID_ARG, "width/height or max_pixels required");
@@ -576,6 +581,8 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   r->persistent = (c.flags & GS_FLAG_PERSISTENT) != 0;
   r->color_only = (c.flags & GS_FLAG_COLOR_ONLY) != 0;
   r->tight = (c.flags & GS_FLAG_TIGHT_BINNING) != 0;
+  r->fwd_batch = (int)c.batch;
+  r->fwd_ppt = (int)c.pixels_per_thread;
   auto bail = [&](cudaError_t e, const char* what) {
     std::string m = std::string("allocation of ") + what + " failed: " + cudaGetErrorString(e);
     gs_rasterizer_destroy(r);
@@ -966,6 +973,72 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
     if (stg >= 0 && stg < N_STAGES) stage_ms[stg] += ms;
   }
   *n_stages = N_STAGES;
+  return GS_OK;
+}
+
+gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32_t n, void* stream, uint32_t out[4]) {
+  if (!r || !out) return GS_ERR_INVALID_ARG;
+  gs_status s = set_views(r, cams, nv, n);
+  if (s) return s;
+  cudaStream_t st = S(stream);
+  s = upload_views(r, st);
+  if (s) return s;
+  int tiles = 0;
+  for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
+  const int prec = (int)r->cfg.precision;
+  cudaEvent_t e0, e1;
+  TRY_CUDA(r, cudaEventCreate(&e0));
+  TRY_CUDA(r, cudaEventCreate(&e1));
+  auto time_it = [&](auto&& fn) -> float {
+    fn();  // warm-up
+    cudaEventRecord(e0, st);
+    for (int k = 0; k < 3; ++k) fn();
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  // Forward: every (batch, pixels per thread) shape.
+  const int fshape[5][2] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}};
+  float best = 1e30f;
+  int bf = 1;
+  for (int k = 0; k < 5; ++k) {
+    r->fwd_batch = fshape[k][0];
+    r->fwd_ppt = fshape[k][1];
+    gs_status fs = GS_OK;
+    const float ms = time_it([&] { fs = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true,
+                                                    true, st); });
+    if (fs) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fs; }
+    if (ms < best) { best = ms; bf = k; }
+  }
+  r->fwd_batch = fshape[bf][0];
+  r->fwd_ppt = fshape[bf][1];
+  s = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true, true, st);
+  if (!s) {
+    TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
+    s = run_loss(r, r->views_dev, r->views_batched.data(), nv, 0.8f, 0.2f, r->loss_sums, st);
+  }
+  if (s) { cudaEventDestroy(e0); cudaEventDestroy(e1); return s; }
+  // Backward (colour-only, as in the training step): every shape.
+  const int bshape[3][2] = {{64, 1}, {64, 2}, {128, 2}};
+  best = 1e30f;
+  int bb = 2;
+  for (int k = 0; k < 3; ++k) {
+    r->bwd_batch = bshape[k][0];
+    r->bwd_ppt = bshape[k][1];
+    gs_status bs = GS_OK;
+    const float ms = time_it([&] { bs = run_backward_raster(r, r->views_dev, nv, tiles, n, prec, false, true, st); });
+    if (bs) { cudaEventDestroy(e0); cudaEventDestroy(e1); return bs; }
+    if (ms < best) { best = ms; bb = k; }
+  }
+  r->bwd_batch = bshape[bb][0];
+  r->bwd_ppt = bshape[bb][1];
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
+  out[0] = (uint32_t)r->fwd_batch; out[1] = (uint32_t)r->fwd_ppt;
+  out[2] = (uint32_t)r->bwd_batch; out[3] = (uint32_t)r->bwd_ppt;
   return GS_OK;
 }
 

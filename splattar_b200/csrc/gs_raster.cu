@@ -38,68 +38,82 @@ struct Hit {
   bool ray;
 };
 
-// raster_common.wgsl:69-95 on the record parameterisation. Written with
-// explicit rounding intrinsics so the forward and backward kernels compute
-// bit-identical alphas.
+// Approximate reciprocal (MUFU, ≤ 1 ulp): the only reciprocal either kernel
+// uses, so forward and backward stay bit-consistent.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// raster_common.wgsl:69-95 on the record parameterisation, branch-free.
+// Written with explicit rounding intrinsics so the forward and backward
+// kernels compute bit-identical alphas. When the ray branch is unavailable
+// (|det| ≤ 1e-12 or t ≤ near) q_ray is +inf and u, v, t are unused.
 __device__ __forceinline__ Hit eval_hit(const float4& r0, const float4& r1, const float4& r2, float depth, float sx,
                                         float sy, float pxc, float pyc) {
   Hit h;
   const float det = fmaf(r0.x, sx, fmaf(r0.y, sy, r0.z));
-  float qr = __int_as_float(0x7f800000);  // +inf: ray branch unavailable
-  h.u = 0.0f; h.v = 0.0f; h.t = 0.0f; h.inv_det = 0.0f;
-  if (fabsf(det) > 1e-12f) {
-    const float inv = __frcp_rn(det);
-    const float u = __fmul_rn(fmaf(r1.x, sx, fmaf(r1.y, sy, r1.z)), inv);
-    const float v = __fmul_rn(fmaf(r2.x, sx, fmaf(r2.y, sy, r2.z)), inv);
-    const float t = __fmul_rn(r0.w, inv);
-    h.u = u; h.v = v; h.t = t; h.inv_det = inv;
-    if (t > NEAR_DEPTH) qr = __fmul_rn(0.5f, fmaf(u, u, __fmul_rn(v, v)));
-  }
+  const float inv = rcp_approx(det);
+  const float u = __fmul_rn(fmaf(r1.x, sx, fmaf(r1.y, sy, r1.z)), inv);
+  const float v = __fmul_rn(fmaf(r2.x, sx, fmaf(r2.y, sy, r2.z)), inv);
+  const float t = __fmul_rn(r0.w, inv);
+  const bool ray_ok = fabsf(det) > 1e-12f && t > NEAR_DEPTH;
+  const float qr = ray_ok ? __fmul_rn(0.5f, fmaf(u, u, __fmul_rn(v, v))) : __int_as_float(0x7f800000);
   const float dx = pxc - r1.w, dy = pyc - r2.w;
   const float qs = fmaf(dx, dx, __fmul_rn(dy, dy));  // (dx²+dy²)/(2σ²) with σ² = 0.5
   h.ray = qr <= qs;
   const float q = h.ray ? qr : qs;
-  if (!h.ray) h.t = depth;
+  h.u = u; h.v = v; h.inv_det = inv;
+  h.t = h.ray ? t : depth;
   h.ghat = __expf(-q);
   return h;
 }
 
+// Tile geometry for a CTA working on `tile` with PPT vertically adjacent
+// pixels per thread: thread t owns column t & 15 and rows (t >> 4)·PPT + p,
+// so each warp covers a compact 16 × (2·PPT) block.
+template <int PPT>
 struct TileGeo {
-  int v, x, y, W, H;
-  bool inside;
-  float pxc, pyc, sx, sy;
-  float bx0, bx1, by0, by1;  // pixel-centre extent of the tile's in-image pixels
-  long long pix;
+  int W, H;
+  long long row0;               // pix_base + y(p=0)·W + x
+  float pxc, sx;
+  float pyc[PPT], sy[PPT];
+  bool inside[PPT];
+  float bx0, bx1, by0, by1;     // pixel-centre extent of the tile's in-image pixels
 };
 
-__device__ __forceinline__ TileGeo tile_geo(const RasterArgs& a, int tile) {
-  TileGeo g;
+template <int PPT>
+__device__ __forceinline__ TileGeo<PPT> tile_geo(const RasterArgs& a, int tile) {
+  TileGeo<PPT> g;
   int v = 0;
   while (v + 1 < a.n_views && tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
   const ViewInfo* V = a.views + v;
   const int tiles_x = __ldg(&V->tiles_x);
-  g.v = v;
   g.W = __ldg(&V->width);
   g.H = __ldg(&V->height);
   const int lt = tile - __ldg(&V->tile_base);
   const int x0 = (lt % tiles_x) * TILE, y0 = (lt / tiles_x) * TILE;
-  g.x = x0 + (threadIdx.x & 15);
-  g.y = y0 + (threadIdx.x >> 4);
-  g.inside = g.x < g.W && g.y < g.H;
+  const int x = x0 + (threadIdx.x & 15), yb = y0 + (threadIdx.x >> 4) * PPT;
   const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
-  g.pxc = (float)g.x + 0.5f;
-  g.pyc = (float)g.y + 0.5f;
+  g.pxc = (float)x + 0.5f;
   g.sx = -((g.pxc - cx) / f);  // s = −d
-  g.sy = (g.pyc - cy) / f;
+#pragma unroll
+  for (int p = 0; p < PPT; ++p) {
+    g.pyc[p] = (float)(yb + p) + 0.5f;
+    g.sy[p] = (g.pyc[p] - cy) / f;
+    g.inside[p] = x < g.W && yb + p < g.H;
+  }
+  g.row0 = __ldg(&V->pix_base) + (long long)yb * g.W + x;
   g.bx0 = (float)x0 + 0.5f;
   g.bx1 = (float)(min(x0 + TILE, g.W) - 1) + 0.5f;
   g.by0 = (float)y0 + 0.5f;
   g.by1 = (float)(min(y0 + TILE, g.H) - 1) + 0.5f;
-  g.pix = __ldg(&V->pix_base) + (long long)g.y * g.W + g.x;
   return g;
 }
 
-__device__ __forceinline__ bool box_hits_tile(const float4& b, const TileGeo& g) {
+template <int PPT>
+__device__ __forceinline__ bool box_hits_tile(const float4& b, const TileGeo<PPT>& g) {
   return b.x <= g.bx1 && b.y >= g.bx0 && b.z <= g.by1 && b.w >= g.by0;
 }
 __device__ __forceinline__ bool box_has_pixel(const float4& b, float pxc, float pyc) {
@@ -108,6 +122,7 @@ __device__ __forceinline__ bool box_has_pixel(const float4& b, float pxc, float 
 
 // Compaction of the staged batch: returns this thread's slot among the kept
 // entries (valid when keep) and the number kept. Order is preserved.
+template <int NW>
 __device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned bal = __ballot_sync(FULL, keep);
@@ -115,7 +130,7 @@ __device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept)
   __syncthreads();
   int off = 0, tot = 0;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) {
+  for (int w = 0; w < NW; ++w) {
     const int c = s_wcount[w];
     if (w < warp) off += c;
     tot += c;
@@ -124,12 +139,13 @@ __device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept)
   return off + __popc(bal & lanemask_lt());
 }
 
-template <int BATCH, int PREC, bool DET, bool PERSIST>
-__global__ void __launch_bounds__(256) k_raster_fwd(RasterArgs a) {
-  static_assert(BATCH <= 256, "one staging pass per batch");
+template <int BATCH, int PREC, bool DET, bool PERSIST, int PPT>
+__global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
+  constexpr int NT = 256 / PPT, NW = NT / 32;
+  static_assert(BATCH <= NT, "one staging pass per batch");
   __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_r4[BATCH], s_bb[BATCH];
   __shared__ int s_j[BATCH];
-  __shared__ int s_wcount[8];
+  __shared__ int s_wcount[NW];
   __shared__ int s_tile;
   const int tid = threadIdx.x;
   int tile = blockIdx.x;
@@ -140,13 +156,21 @@ __global__ void __launch_bounds__(256) k_raster_fwd(RasterArgs a) {
       tile = s_tile;
       if (tile >= a.total_tiles) return;
     }
-    const TileGeo g = tile_geo(a, tile);
+    const TileGeo<PPT> g = tile_geo<PPT>(a, tile);
     const uint2 range = __ldg(&a.ranges[tile]);
-    float T = 1.0f, cr = 0.f, cg = 0.f, cb = 0.f, aa = 0.f, ad = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
-    uint32_t nc = 0;
-    bool done = !g.inside;
+    float T[PPT], cr[PPT], cg[PPT], cb[PPT], aa[PPT], ad[PPT], nx[PPT], ny[PPT], nz[PPT];
+    uint32_t nc[PPT];
+    bool done[PPT];
+    bool tdone = true;
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) {
+      T[p] = 1.f; cr[p] = cg[p] = cb[p] = aa[p] = ad[p] = nx[p] = ny[p] = nz[p] = 0.f;
+      nc[p] = 0;
+      done[p] = !g.inside[p];
+      tdone &= done[p];
+    }
     for (uint32_t base = range.x; base < range.y; base += BATCH) {
-      if (__syncthreads_count(done) == 256) break;
+      if (__syncthreads_count(tdone) == NT) break;
       const int count = (int)min((uint32_t)BATCH, range.y - base);
       bool keep = false;
       uint32_t item = 0;
@@ -158,7 +182,7 @@ __global__ void __launch_bounds__(256) k_raster_fwd(RasterArgs a) {
         keep = box_hits_tile(bb, g);
       }
       int kept;
-      const int slot = compact_slot(keep, s_wcount, kept);
+      const int slot = compact_slot<NW>(keep, s_wcount, kept);
       if (keep) {
         float4 r0, r1, r2, r3, r4;
         load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
@@ -167,49 +191,62 @@ __global__ void __launch_bounds__(256) k_raster_fwd(RasterArgs a) {
         s_j[slot] = tid;
       }
       __syncthreads();
-      if (!done) {
+      if (!tdone) {
         for (int k = 0; k < kept; ++k) {
-          if (!box_has_pixel(s_bb[k], g.pxc, g.pyc)) continue;
+          const float4 bbk = s_bb[k];
+          if (g.pxc < bbk.x || g.pxc > bbk.y) continue;
           const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
-          const float4 r4 = s_r4[k];
-          const Hit h = eval_hit(r0, r1, r2, r4.w, g.sx, g.sy, g.pxc, g.pyc);
-          const float4 r3 = s_r3[k];
-          const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
-          if (alpha < ALPHA_SKIP) continue;
-          const float w = T * alpha;
-          cr += r3.x * w; cg += r3.y * w; cb += r3.z * w;
-          aa += w;
-          ad += h.t * w;
-          nx += r4.x * w; ny += r4.y * w; nz += r4.z * w;
-          T = __fmul_rn(T, 1.0f - alpha);
-          nc = base - range.x + (uint32_t)s_j[k] + 1u;
-          if (T < T_TERMINATE) { done = true; break; }
+          const float4 r3 = s_r3[k], r4 = s_r4[k];
+          const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) {
+            if (done[p] || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
+            const Hit h = eval_hit(r0, r1, r2, r4.w, g.sx, g.sy[p], g.pxc, g.pyc[p]);
+            const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
+            if (alpha < ALPHA_SKIP) continue;
+            const float w = T[p] * alpha;
+            cr[p] += r3.x * w; cg[p] += r3.y * w; cb[p] += r3.z * w;
+            aa[p] += w;
+            ad[p] += h.t * w;
+            nx[p] += r4.x * w; ny[p] += r4.y * w; nz[p] += r4.z * w;
+            T[p] = __fmul_rn(T[p], 1.0f - alpha);
+            nc[p] = idx1;
+            if (T[p] < T_TERMINATE) done[p] = true;
+          }
+          bool all = true;
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) all &= done[p];
+          if (all) { tdone = true; break; }
         }
       }
     }
-    if (g.inside) {
-      a.out_color[g.pix] = make_float4(cr, cg, cb, aa);
-      a.out_aux[g.pix] = make_float4(T, ad, 0.f, 0.f);
-      a.out_normal[g.pix] = make_float4(nx, ny, nz, 0.f);
-      a.out_nc[g.pix] = nc;
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) {
+      if (!g.inside[p]) continue;
+      const long long pix = g.row0 + (long long)p * g.W;
+      a.out_color[pix] = make_float4(cr[p], cg[p], cb[p], aa[p]);
+      a.out_aux[pix] = make_float4(T[p], ad[p], 0.f, 0.f);
+      a.out_normal[pix] = make_float4(nx[p], ny[p], nz[p], 0.f);
+      a.out_nc[pix] = nc[p];
     }
     if (!PERSIST) return;
     __syncthreads();
   }
 }
 
-template <int BATCH, int PREC, bool AUX, bool DET, bool PERSIST>
-__global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
-  constexpr int NW = 8;
+template <int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT>
+__global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
+  constexpr int NT = 256 / PPT, NW = NT / 32;
   constexpr int NG = AUX ? 32 : 16;  // reduced components per entry (AUX: 20 used)
   constexpr int NQ = AUX ? 5 : 4;    // float4 groups per entry written out
+  static_assert(BATCH <= NT, "one staging pass per batch");
   __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
   __shared__ float4 s_r4[AUX ? BATCH : 1];
   __shared__ uint32_t s_item[BATCH];
   __shared__ uint32_t s_q[DET ? BATCH : 1];
   __shared__ int s_j[BATCH];
   __shared__ float s_part[NW][BATCH][NG];
-  __shared__ int s_wcount[8];
+  __shared__ int s_wcount[NW];
   __shared__ int s_tile, s_maxnc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int tile = blockIdx.x;
@@ -226,48 +263,53 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
       __syncthreads();
       continue;
     }
-    const TileGeo g = tile_geo(a, tile);
-    float3 dlc = make_float3(0.f, 0.f, 0.f);
-    float dld = 0.f, wtot = 0.f, wttot = 0.f;
-    float3 dln = make_float3(0.f, 0.f, 0.f);
-    float T = 1.0f;
-    uint32_t nc = 0;
-    if (g.inside) {
-      const float4 gc = a.dl_dcolor[g.pix];
-      dlc = make_float3(gc.x, gc.y, gc.z);
-      const float4 aux = a.out_aux[g.pix];
-      T = aux.x;
-      nc = a.out_nc[g.pix];
-      if (AUX) {
-        dld = gc.w;
-        const float4 gn = a.dl_dnormal[g.pix];
-        dln = make_float3(gn.x, gn.y, gn.z);
-        wtot = a.out_color[g.pix].w;
-        wttot = aux.y;
+    const TileGeo<PPT> g = tile_geo<PPT>(a, tile);
+    float3 dlc[PPT], dln[PPT], suf_c[PPT], suf_n[PPT];
+    float dld[PPT], wtot[PPT], wttot[PPT], T[PPT], suf_d[PPT], suf_w[PPT], suf_cw[PPT];
+    uint32_t nc[PPT];
+    uint32_t my_max = 0;
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) {
+      dlc[p] = dln[p] = suf_c[p] = suf_n[p] = make_float3(0.f, 0.f, 0.f);
+      dld[p] = wtot[p] = wttot[p] = suf_d[p] = suf_w[p] = suf_cw[p] = 0.f;
+      T[p] = 1.f;
+      nc[p] = 0;
+      if (g.inside[p]) {
+        const long long pix = g.row0 + (long long)p * g.W;
+        const float4 gc = a.dl_dcolor[pix];
+        dlc[p] = make_float3(gc.x, gc.y, gc.z);
+        const float4 aux = a.out_aux[pix];
+        T[p] = aux.x;
+        nc[p] = a.out_nc[pix];
+        if (AUX) {
+          dld[p] = gc.w;
+          const float4 gn = a.dl_dnormal[pix];
+          dln[p] = make_float3(gn.x, gn.y, gn.z);
+          wtot[p] = a.out_color[pix].w;
+          wttot[p] = aux.y;
+        }
       }
+      bool has_loss = g.inside[p] && (dlc[p].x != 0.f || dlc[p].y != 0.f || dlc[p].z != 0.f);
+      if (AUX) has_loss = g.inside[p] && (has_loss || dld[p] != 0.f || dln[p].x != 0.f || dln[p].y != 0.f ||
+                                          dln[p].z != 0.f || a.lambda_dist != 0.f);
+      if (!has_loss) nc[p] = 0;  // nc = 0 disables the pixel's walk
+      my_max = max(my_max, nc[p]);
     }
-    bool has_loss = g.inside && (dlc.x != 0.f || dlc.y != 0.f || dlc.z != 0.f);
-    if (AUX) has_loss = g.inside && (has_loss || dld != 0.f || dln.x != 0.f || dln.y != 0.f || dln.z != 0.f ||
-                                     a.lambda_dist != 0.f);
-    if (!has_loss) nc = 0;
     if (tid == 0) s_maxnc = 0;
     __syncthreads();
-    if (nc) atomicMax(&s_maxnc, (int)nc);
+    if (my_max) atomicMax(&s_maxnc, (int)my_max);
     __syncthreads();
     const uint32_t maxnc = min((uint32_t)s_maxnc, range.y - range.x);
 
     if (DET) {
       // Entries past the tile's last contributor get zero partials.
-      for (uint32_t e = range.x + maxnc + tid; e < range.y; e += 256) {
+      for (uint32_t e = range.x + maxnc + tid; e < range.y; e += NT) {
         const uint32_t q = __ldg(&a.sorted_vals[e]);
         float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)q * GG_STRIDE);
 #pragma unroll
         for (int k = 0; k < NQ; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
-
-    float3 suf_c = make_float3(0.f, 0.f, 0.f), suf_n = make_float3(0.f, 0.f, 0.f);
-    float suf_d = 0.f, suf_w = 0.f, suf_cw = 0.f;
 
     uint32_t hi = range.x + maxnc;
     while (hi > range.x) {
@@ -289,7 +331,7 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
         }
       }
       int kept;
-      const int slot = compact_slot(keep, s_wcount, kept);
+      const int slot = compact_slot<NW>(keep, s_wcount, kept);
       if (keep) {
         float4 r0, r1, r2, r3, r4;
         load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
@@ -303,67 +345,70 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
       __syncthreads();
       for (int k = kept - 1; k >= 0; --k) {
         const uint32_t cidx = lo - range.x + (uint32_t)s_j[k];
+        const float4 bbk = s_bb[k];
         float gg[NG];
 #pragma unroll
         for (int c = 0; c < NG; ++c) gg[c] = 0.f;
         bool contrib = false;
-        if (has_loss && cidx < nc && box_has_pixel(s_bb[k], g.pxc, g.pyc)) {
+        if (g.pxc >= bbk.x && g.pxc <= bbk.y) {
           const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
           if (AUX) { r4 = s_r4[k]; depth = r4.w; }
-          const Hit h = eval_hit(r0, r1, r2, depth, g.sx, g.sy, g.pxc, g.pyc);
-          const float raw_alpha = __fmul_rn(r3.w, h.ghat);
-          const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
-          if (alpha >= ALPHA_SKIP) {
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) {
+            if (!(cidx < nc[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
+            const Hit h = eval_hit(r0, r1, r2, depth, g.sx, g.sy[p], g.pxc, g.pyc[p]);
+            const float raw_alpha = __fmul_rn(r3.w, h.ghat);
+            const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
+            if (alpha < ALPHA_SKIP) continue;
             contrib = true;
-            const float oma = 1.0f - alpha;
-            const float inv_oma = 1.0f / oma;
-            const float t_before = T / oma;
+            const float inv_oma = rcp_approx(1.0f - alpha);
+            const float t_before = T[p] * inv_oma;
             const float w = t_before * alpha;
-            float dl_dalpha = (dlc.x * r3.x + dlc.y * r3.y + dlc.z * r3.z) * t_before -
-                              (dlc.x * suf_c.x + dlc.y * suf_c.y + dlc.z * suf_c.z) * inv_oma;
+            float dl_dalpha = (dlc[p].x * r3.x + dlc[p].y * r3.y + dlc[p].z * r3.z) * t_before -
+                              (dlc[p].x * suf_c[p].x + dlc[p].y * suf_c[p].y + dlc[p].z * suf_c[p].z) * inv_oma;
             float dl_dt = 0.f;
             if (AUX) {
               const float t_hit = h.t;
               float dt_dist = 0.f, coef = 0.f;
               if (a.lambda_dist != 0.f) {
-                const float a_pre = wtot - suf_w - w;
-                const float b_pre = wttot - suf_d - w * t_hit;
-                dt_dist = a.lambda_dist * 2.0f * w * (a_pre - suf_w);
-                coef = a.lambda_dist * (2.0f * (t_hit * a_pre - b_pre) + 2.0f * (suf_d - t_hit * suf_w));
+                const float a_pre = wtot[p] - suf_w[p] - w;
+                const float b_pre = wttot[p] - suf_d[p] - w * t_hit;
+                dt_dist = a.lambda_dist * 2.0f * w * (a_pre - suf_w[p]);
+                coef = a.lambda_dist * (2.0f * (t_hit * a_pre - b_pre) + 2.0f * (suf_d[p] - t_hit * suf_w[p]));
               }
-              dl_dt = dld * w + dt_dist;
-              dl_dalpha += dld * (t_hit * t_before - suf_d * inv_oma) +
-                           (dln.x * r4.x + dln.y * r4.y + dln.z * r4.z) * t_before -
-                           (dln.x * suf_n.x + dln.y * suf_n.y + dln.z * suf_n.z) * inv_oma + coef * t_before -
-                           suf_cw * inv_oma;
-              suf_d += t_hit * w;
-              suf_n.x += r4.x * w; suf_n.y += r4.y * w; suf_n.z += r4.z * w;
-              suf_w += w;
-              suf_cw += coef * w;
-              gg[17] = dln.x * w; gg[18] = dln.y * w; gg[19] = dln.z * w;
+              dl_dt = dld[p] * w + dt_dist;
+              dl_dalpha += dld[p] * (t_hit * t_before - suf_d[p] * inv_oma) +
+                           (dln[p].x * r4.x + dln[p].y * r4.y + dln[p].z * r4.z) * t_before -
+                           (dln[p].x * suf_n[p].x + dln[p].y * suf_n[p].y + dln[p].z * suf_n[p].z) * inv_oma +
+                           coef * t_before - suf_cw[p] * inv_oma;
+              suf_d[p] += t_hit * w;
+              suf_n[p].x += r4.x * w; suf_n[p].y += r4.y * w; suf_n[p].z += r4.z * w;
+              suf_w[p] += w;
+              suf_cw[p] += coef * w;
+              gg[17] += dln[p].x * w; gg[18] += dln[p].y * w; gg[19] += dln[p].z * w;
             }
-            suf_c.x += r3.x * w; suf_c.y += r3.y * w; suf_c.z += r3.z * w;
-            T = t_before;
-            gg[11] = dlc.x * w; gg[12] = dlc.y * w; gg[13] = dlc.z * w;
+            suf_c[p].x += r3.x * w; suf_c[p].y += r3.y * w; suf_c[p].z += r3.z * w;
+            T[p] = t_before;
+            gg[11] += dlc[p].x * w; gg[12] += dlc[p].y * w; gg[13] += dlc[p].z * w;
             if (raw_alpha <= ALPHA_CLAMP) {
-              gg[14] = dl_dalpha * h.ghat;
+              gg[14] += dl_dalpha * h.ghat;
               const float dl_dghat = dl_dalpha * r3.w;
               if (h.ray) {
                 const float gu = -h.u * h.ghat * dl_dghat;
                 const float gv = -h.v * h.ghat * dl_dghat;
                 const float gun = gu * h.inv_det, gvn = gv * h.inv_det;
                 const float gdet = -(h.u * gu + h.v * gv + (AUX ? h.t * dl_dt : 0.f)) * h.inv_det;
-                gg[0] = gdet * g.sx; gg[1] = gdet * g.sy; gg[2] = gdet;
-                gg[3] = gun * g.sx; gg[4] = gun * g.sy; gg[5] = gun;
-                gg[6] = gvn * g.sx; gg[7] = gvn * g.sy; gg[8] = gvn;
-                if (AUX) gg[15] = dl_dt * h.inv_det;
+                gg[0] += gdet * g.sx; gg[1] += gdet * g.sy[p]; gg[2] += gdet;
+                gg[3] += gun * g.sx; gg[4] += gun * g.sy[p]; gg[5] += gun;
+                gg[6] += gvn * g.sx; gg[7] += gvn * g.sy[p]; gg[8] += gvn;
+                if (AUX) gg[15] += dl_dt * h.inv_det;
               } else {
                 const float kk = h.ghat * dl_dghat / LOWPASS_SIGMA2;
-                gg[9] = (g.pxc - r1.w) * kk;
-                gg[10] = (g.pyc - r2.w) * kk;
-                if (AUX) gg[16] = dl_dt;
+                gg[9] += (g.pxc - r1.w) * kk;
+                gg[10] += (g.pyc[p] - r2.w) * kk;
+                if (AUX) gg[16] += dl_dt;
               }
             }
           }
@@ -389,7 +434,7 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
       __syncthreads();
       // Cross-warp sum in fixed warp order, then one vector reduction (or
       // one ordered store) per 4 components.
-      for (int w4 = tid; w4 < kept * NQ; w4 += 256) {
+      for (int w4 = tid; w4 < kept * NQ; w4 += NT) {
         const int k = w4 / NQ, q4 = w4 % NQ;
         float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
@@ -411,56 +456,72 @@ __global__ void __launch_bounds__(256) k_raster_bwd(RasterArgs a) {
   }
 }
 
-template <int BATCH, int PREC, bool DET, bool PERSIST>
-void fwd_launch(const RasterArgs& a, int grid, cudaStream_t st) {
-  k_raster_fwd<BATCH, PREC, DET, PERSIST><<<grid, 256, 0, st>>>(a);
-}
-
+// ------------------------------------------------------------- launchers
+// Forward variants: (pixels per thread, staging batch) ∈ {(1, 64), (1, 128),
+// (1, 256), (2, 64), (2, 128)}; `batch` selects one, `ppt` the pixel split.
+// Backward: two pixels per thread and 128-entry batches without aux
+// losses; one pixel per thread and 32-entry batches with aux losses (the
+// per-warp partial buffer is NW·BATCH·NG floats of static shared memory).
 template <int PREC, bool DET, bool PERSIST>
-void fwd_batch(const RasterArgs& a, int batch, int grid, cudaStream_t st) {
-  if (batch == 64) fwd_launch<64, PREC, DET, PERSIST>(a, grid, st);
-  else if (batch == 256) fwd_launch<256, PREC, DET, PERSIST>(a, grid, st);
-  else fwd_launch<128, PREC, DET, PERSIST>(a, grid, st);
+void fwd_dispatch(const RasterArgs& a, int batch, int ppt, int grid, cudaStream_t st) {
+  if (ppt == 2) {
+    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
+    else k_raster_fwd<128, PREC, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
+  } else {
+    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
+    else if (batch == 256) k_raster_fwd<256, PREC, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
+    else k_raster_fwd<128, PREC, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
+  }
 }
 
-// The per-warp partial buffer is NW*BATCH*NG floats of static shared memory,
-// so the backward stages 32 entries at a time with aux losses and 64 without.
-template <bool AUX>
-constexpr int bwd_batch() { return AUX ? 32 : 64; }
-
+// Backward variants without aux losses: (pixels per thread, batch) ∈
+// {(1, 64), (2, 64), (2, 128)}; with aux losses (1, 32).
 template <int PREC, bool AUX, bool DET, bool PERSIST>
-void bwd_launch(const RasterArgs& a, int grid, cudaStream_t st) {
-  k_raster_bwd<bwd_batch<AUX>(), PREC, AUX, DET, PERSIST><<<grid, 256, 0, st>>>(a);
+void bwd_dispatch(const RasterArgs& a, int ppt, int batch, int grid, cudaStream_t st) {
+  if constexpr (AUX) {
+    k_raster_bwd<32, PREC, true, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
+  } else {
+    if (ppt == 1) k_raster_bwd<64, PREC, false, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
+    else if (batch == 64) k_raster_bwd<64, PREC, false, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
+    else k_raster_bwd<128, PREC, false, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
+  }
 }
 
 template <typename K>
-int occ(K kernel) {
+int occ(K kernel, int threads) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 256, 0) != cudaSuccess) return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess) return 1;
   return n < 1 ? 1 : n;
 }
 
 }  // namespace
 
-int raster_fwd_occupancy(int prec, int batch, bool det) {
-#define GS_O(B, P) (det ? occ(k_raster_fwd<B, P, true, true>) : occ(k_raster_fwd<B, P, false, true>))
-#define GS_OB(P) (batch == 64 ? GS_O(64, P) : (batch == 256 ? GS_O(256, P) : GS_O(128, P)))
+int raster_fwd_occupancy(int prec, int batch, int ppt, bool det) {
+#define GS_O1(B, P) (det ? occ(k_raster_fwd<B, P, true, true, 1>, 256) : occ(k_raster_fwd<B, P, false, true, 1>, 256))
+#define GS_O2(B, P) (det ? occ(k_raster_fwd<B, P, true, true, 2>, 128) : occ(k_raster_fwd<B, P, false, true, 2>, 128))
+#define GS_OB(P) (ppt == 2 ? (batch == 64 ? GS_O2(64, P) : GS_O2(128, P)) \
+                           : (batch == 64 ? GS_O1(64, P) : (batch == 256 ? GS_O1(256, P) : GS_O1(128, P))))
   return prec == 0 ? GS_OB(0) : (prec == 1 ? GS_OB(1) : GS_OB(2));
 #undef GS_OB
-#undef GS_O
+#undef GS_O2
+#undef GS_O1
 }
 
-int raster_bwd_occupancy(int prec, bool aux, bool det) {
-#define GS_O(P, X, D) occ(k_raster_bwd<bwd_batch<X>(), P, X, D, true>)
-#define GS_O2(P) (aux ? (det ? GS_O(P, true, true) : GS_O(P, true, false)) : (det ? GS_O(P, false, true) : GS_O(P, false, false)))
+int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det) {
+#define GS_OV(P, D) (aux ? occ(k_raster_bwd<32, P, true, D, true, 1>, 256)                         \
+                         : (ppt == 1 ? occ(k_raster_bwd<64, P, false, D, true, 1>, 256)               \
+                                     : (batch == 64 ? occ(k_raster_bwd<64, P, false, D, true, 2>, 128) \
+                                                    : occ(k_raster_bwd<128, P, false, D, true, 2>, 128))))
+#define GS_O2(P) (det ? GS_OV(P, true) : GS_OV(P, false))
   return prec == 0 ? GS_O2(0) : (prec == 1 ? GS_O2(1) : GS_O2(2));
 #undef GS_O2
-#undef GS_O
+#undef GS_OV
 }
 
-int launch_raster_fwd(const RasterArgs& a, int prec, int batch, bool det, bool persistent, int grid, cudaStream_t st) {
+int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, int grid,
+                      cudaStream_t st) {
   if (a.total_tiles == 0) return 0;
-#define GS_F(P, D, S) fwd_batch<P, D, S>(a, batch, grid, st)
+#define GS_F(P, D, S) fwd_dispatch<P, D, S>(a, batch, ppt, grid, st)
 #define GS_F2(P)                                   \
   if (det) { if (persistent) GS_F(P, true, true); else GS_F(P, true, false); } \
   else { if (persistent) GS_F(P, false, true); else GS_F(P, false, false); }
@@ -470,9 +531,10 @@ int launch_raster_fwd(const RasterArgs& a, int prec, int batch, bool det, bool p
   return (int)cudaGetLastError();
 }
 
-int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, bool det, bool persistent, int grid, cudaStream_t st) {
+int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, int ppt, int batch, bool det, bool persistent, int grid,
+                      cudaStream_t st) {
   if (a.total_tiles == 0) return 0;
-#define GS_B(P, X, D, S) bwd_launch<P, X, D, S>(a, grid, st)
+#define GS_B(P, X, D, S) bwd_dispatch<P, X, D, S>(a, ppt, batch, grid, st)
 #define GS_B3(P, X)                                \
   if (det) { if (persistent) GS_B(P, X, true, true); else GS_B(P, X, true, false); } \
   else { if (persistent) GS_B(P, X, false, true); else GS_B(P, X, false, false); }

@@ -98,12 +98,13 @@ class Rasterizer:
 
     def __init__(self, capacity: int, width: int, height: int, max_entries: int = 0, *, max_views: int = 1,
                  max_pixels: int = 0, precision: str = "f32", deterministic: bool = False,
-                 persistent: bool = False, color_only: bool = False, tight: bool = False, batch: int = 128):
+                 persistent: bool = False, color_only: bool = False, tight: bool = False, batch: int = 128,
+                 pixels_per_thread: int = 0):
         self._h = None
         flags = (FLAG_DETERMINISTIC if deterministic else 0) | (FLAG_PERSISTENT if persistent else 0) | (
             FLAG_COLOR_ONLY if color_only else 0) | (FLAG_TIGHT_BINNING if tight else 0)
         cfg = RasterConfig(capacity, width, height, max_views, max_pixels, max_entries, 16, batch, PREC[precision],
-                           flags)
+                           flags, pixels_per_thread)
         h = C.c_void_p()
         check(lib().gs_rasterizer_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -215,6 +216,14 @@ class Rasterizer:
         self._chk(lib().gs_train_step_profiled(self._h, cams, len(cams), num_surfels, C.byref(cfg), stream, ms,
                                                C.byref(ns)))
         return {k: float(ms[i]) for i, k in enumerate(self.STAGES)}
+
+    def autotune(self, cameras, num_surfels: int, stream: int = 0) -> dict:
+        """Time the raster launch shapes on these cameras and keep the fastest."""
+        cams = camera_array(cameras)
+        out = (C.c_uint32 * 4)()
+        self._chk(lib().gs_autotune(self._h, cams, len(cams), num_surfels, stream, out))
+        return {"fwd_batch": out[0], "fwd_pixels_per_thread": out[1], "bwd_batch": out[2],
+                "bwd_pixels_per_thread": out[3]}
 
     def densify_prune(self, grad_threshold: float, opacity_threshold: float, num_surfels: int,
                       stream: int = 0) -> int:

@@ -44,6 +44,15 @@ def test_forward_batch_depths_agree(batch):
     assert np.array_equal(a["color"], b["color"]) and np.array_equal(a["ncontrib"], b["ncontrib"])
 
 
+@pytest.mark.parametrize("batch,ppt", [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2)])
+def test_forward_pixel_splits_agree(batch, ppt):
+    scene, cam = make_scene(404, 50, 1, 128)
+    _, a = forward(scene, cam, batch=128, pixels_per_thread=1)
+    _, b = forward(scene, cam, batch=batch, pixels_per_thread=ppt)
+    for k in ("color", "aux", "normal", "ncontrib"):
+        assert np.array_equal(a[k], b[k]), k
+
+
 def test_forward_persistent_equals_plain_grid():
     scene, cam = make_scene(202, 40, 3, 96)
     _, a = forward(scene, cam)

@@ -207,3 +207,20 @@ def test_train_step_reduces_loss():
         losses.append(sum(0.8 * l[2 * v] / (3 * c.width * c.height) + 0.2 * (1 - l[2 * v + 1] / (3 * c.width * c.height))
                           for v, c in enumerate(cams)))
     assert losses[-1] < 0.8 * losses[0], losses[::5]
+
+
+def test_autotune_keeps_results():
+    scene, cams = multi_view_setup(66, 400)
+    rc = [raster_camera(c, 3) for c in cams]
+    P = sum(c.width * c.height for c in cams)
+    r = Rasterizer(scene.n, 0, 0, 0, max_views=3, max_pixels=P)
+    r.upload_scene(scene_input(scene))
+    r.optimizer_init(scene.n)  # re-derives the activated values through raw space
+    r.forward(rc, scene.n)
+    before = r.read("out_color", 4 * P)
+    r.write("target", before)
+    shapes = r.autotune(rc, scene.n)
+    assert shapes["fwd_batch"] in (64, 128, 256) and shapes["fwd_pixels_per_thread"] in (1, 2)
+    assert (shapes["bwd_batch"], shapes["bwd_pixels_per_thread"]) in ((64, 1), (64, 2), (128, 2))
+    r.forward(rc, scene.n)
+    assert np.array_equal(r.read("out_color", 4 * P), before)
