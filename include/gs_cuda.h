@@ -70,8 +70,8 @@ typedef struct {
   uint32_t batch;       /* shared-memory staging depth of the raster kernels: 64, 128 or 256 (0 = 128) */
   uint32_t precision;   /* gs_precision */
   uint32_t flags;       /* GS_FLAG_* */
-  uint32_t pixels_per_thread; /* forward raster: 1 or 2 vertically adjacent pixels per thread (0 = 2, or 1 with
-                                 batch 256) */
+  uint32_t pixels_per_thread; /* forward raster: vertically adjacent pixels per thread, 1 (any batch), 2 (batch
+                                 64/128) or 4 (batch 64); 0 = 1 */
 } gs_raster_config;
 
 /* RasterCamera (crates/gs-kernels/src/rasterizer.rs:34-41) plus the image
@@ -230,9 +230,9 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t n_view
 gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
                                  const gs_step_config* cfg, void* stream, float stage_ms[9], uint32_t* n_stages);
 
-/* Autotuner: times the forward raster over staging batch {64,128,256} x
- * {1,2} pixels per thread and the backward raster over (pixels per thread,
- * batch) {(1,64),(2,64),(2,128)} on these cameras (the batched form, tight
+/* Autotuner: times the forward raster over (batch, pixels per thread)
+ * {(64,1),(128,1),(256,1),(64,2),(128,2),(64,4)} and the backward raster over
+ * {(64,1),(64,2),(128,2),(64,4)} on these cameras (the batched form, tight
  * binning, the config's precision) and keeps the fastest for this handle.
  * out = {fwd batch, fwd pixels/thread, bwd batch, bwd pixels/thread}. Tile
  * size is fixed at 16 in this build. Blocking. */

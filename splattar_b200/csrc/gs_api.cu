@@ -556,8 +556,9 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   if (c.batch == 0) c.batch = 128;
   if (c.batch != 64 && c.batch != 128 && c.batch != 256) return fail(nullptr, GS_ERR_INVALID_ARG, "batch must be 64/128/256");
   if (c.pixels_per_thread == 0) c.pixels_per_thread = 1;
-  if (c.pixels_per_thread > 2 || (c.pixels_per_thread == 2 && c.batch == 256))
-    return fail(nullptr, GS_ERR_INVALID_ARG, "pixels_per_thread must be 1, or 2 with batch 64/128");
+  if (c.pixels_per_thread == 3 || c.pixels_per_thread > 4 || (c.pixels_per_thread == 2 && c.batch == 256) ||
+      (c.pixels_per_thread == 4 && c.batch != 64))
+    return fail(nullptr, GS_ERR_INVALID_ARG, "pixels_per_thread must be 1, 2 with batch <= 128, or 4 with batch 64");
   if (c.precision > 2) return fail(nullptr, GS_ERR_INVALID_ARG, "bad precision");
   if (c.max_pixels == 0) c.max_pixels = (uint64_t)c.width * c.height * c.max_views;
   if (c.max_pixels == 0) return fail(nullptr, GS_ERR_INVALID_ARG, "width/height or max_pixels required");
@@ -1000,10 +1001,10 @@ gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint
     return ms;
   };
   // Forward: every (batch, pixels per thread) shape.
-  const int fshape[5][2] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}};
+  const int fshape[6][2] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}, {64, 4}};
   float best = 1e30f;
   int bf = 1;
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < 6; ++k) {
     r->fwd_batch = fshape[k][0];
     r->fwd_ppt = fshape[k][1];
     gs_status fs = GS_OK;
@@ -1021,10 +1022,10 @@ gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint
   }
   if (s) { cudaEventDestroy(e0); cudaEventDestroy(e1); return s; }
   // Backward (colour-only, as in the training step): every shape.
-  const int bshape[3][2] = {{64, 1}, {64, 2}, {128, 2}};
+  const int bshape[4][2] = {{64, 1}, {64, 2}, {128, 2}, {64, 4}};
   best = 1e30f;
   int bb = 2;
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < 4; ++k) {
     r->bwd_batch = bshape[k][0];
     r->bwd_ppt = bshape[k][1];
     gs_status bs = GS_OK;

@@ -295,6 +295,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
       if (!has_loss) nc[p] = 0;  // nc = 0 disables the pixel's walk
       my_max = max(my_max, nc[p]);
     }
+    // Entries at or past this warp's last contributor are skipped warp-wide.
+    const uint32_t warp_maxnc = __reduce_max_sync(FULL, my_max);
     if (tid == 0) s_maxnc = 0;
     __syncthreads();
     if (my_max) atomicMax(&s_maxnc, (int)my_max);
@@ -345,6 +347,11 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
       __syncthreads();
       for (int k = kept - 1; k >= 0; --k) {
         const uint32_t cidx = lo - range.x + (uint32_t)s_j[k];
+        if (cidx >= warp_maxnc) {
+          if (lane < 16) s_part[warp][k][lane] = 0.f;
+          if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
+          continue;
+        }
         const float4 bbk = s_bb[k];
         float gg[NG];
 #pragma unroll
@@ -464,7 +471,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
 // per-warp partial buffer is NW·BATCH·NG floats of static shared memory).
 template <int PREC, bool DET, bool PERSIST>
 void fwd_dispatch(const RasterArgs& a, int batch, int ppt, int grid, cudaStream_t st) {
-  if (ppt == 2) {
+  if (ppt == 4) {
+    k_raster_fwd<64, PREC, DET, PERSIST, 4><<<grid, 64, 0, st>>>(a);
+  } else if (ppt == 2) {
     if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
     else k_raster_fwd<128, PREC, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
   } else {
@@ -481,7 +490,8 @@ void bwd_dispatch(const RasterArgs& a, int ppt, int batch, int grid, cudaStream_
   if constexpr (AUX) {
     k_raster_bwd<32, PREC, true, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
   } else {
-    if (ppt == 1) k_raster_bwd<64, PREC, false, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
+    if (ppt == 4) k_raster_bwd<64, PREC, false, DET, PERSIST, 4><<<grid, 64, 0, st>>>(a);
+    else if (ppt == 1) k_raster_bwd<64, PREC, false, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
     else if (batch == 64) k_raster_bwd<64, PREC, false, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
     else k_raster_bwd<128, PREC, false, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
   }
@@ -499,17 +509,20 @@ int occ(K kernel, int threads) {
 int raster_fwd_occupancy(int prec, int batch, int ppt, bool det) {
 #define GS_O1(B, P) (det ? occ(k_raster_fwd<B, P, true, true, 1>, 256) : occ(k_raster_fwd<B, P, false, true, 1>, 256))
 #define GS_O2(B, P) (det ? occ(k_raster_fwd<B, P, true, true, 2>, 128) : occ(k_raster_fwd<B, P, false, true, 2>, 128))
-#define GS_OB(P) (ppt == 2 ? (batch == 64 ? GS_O2(64, P) : GS_O2(128, P)) \
+#define GS_O4(P) (det ? occ(k_raster_fwd<64, P, true, true, 4>, 64) : occ(k_raster_fwd<64, P, false, true, 4>, 64))
+#define GS_OB(P) (ppt == 4 ? GS_O4(P) : ppt == 2 ? (batch == 64 ? GS_O2(64, P) : GS_O2(128, P)) \
                            : (batch == 64 ? GS_O1(64, P) : (batch == 256 ? GS_O1(256, P) : GS_O1(128, P))))
   return prec == 0 ? GS_OB(0) : (prec == 1 ? GS_OB(1) : GS_OB(2));
 #undef GS_OB
+#undef GS_O4
 #undef GS_O2
 #undef GS_O1
 }
 
 int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det) {
 #define GS_OV(P, D) (aux ? occ(k_raster_bwd<32, P, true, D, true, 1>, 256)                         \
-                         : (ppt == 1 ? occ(k_raster_bwd<64, P, false, D, true, 1>, 256)               \
+                         : (ppt == 4 ? occ(k_raster_bwd<64, P, false, D, true, 4>, 64)                \
+                         : ppt == 1 ? occ(k_raster_bwd<64, P, false, D, true, 1>, 256)               \
                                      : (batch == 64 ? occ(k_raster_bwd<64, P, false, D, true, 2>, 128) \
                                                     : occ(k_raster_bwd<128, P, false, D, true, 2>, 128))))
 #define GS_O2(P) (det ? GS_OV(P, true) : GS_OV(P, false))

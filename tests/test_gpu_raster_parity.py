@@ -44,7 +44,7 @@ def test_forward_batch_depths_agree(batch):
     assert np.array_equal(a["color"], b["color"]) and np.array_equal(a["ncontrib"], b["ncontrib"])
 
 
-@pytest.mark.parametrize("batch,ppt", [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2)])
+@pytest.mark.parametrize("batch,ppt", [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2), (64, 4)])
 def test_forward_pixel_splits_agree(batch, ppt):
     scene, cam = make_scene(404, 50, 1, 128)
     _, a = forward(scene, cam, batch=128, pixels_per_thread=1)
