@@ -274,6 +274,20 @@ gs_status gs_binner_buffer(gs_binner* b, uint32_t which, void** dptr, size_t* by
 gs_status gs_radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint64_t n, uint32_t key_bits, void* stream);
 gs_status gs_exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total_dev, void* stream);
 
+/* No counterpart in the reference. The same stable LSD sort as
+ * gs_radix_sort_pairs for callers that cannot let the library allocate device
+ * memory (a host that owns all device memory through its own pool, a loop
+ * that must not pay an allocation's latency or implicit synchronisation, a
+ * binding that forbids hidden allocations): it calls no allocator. Its
+ * scratch is a fixed array in the library's device image sized for at most
+ * 1,048,576 pairs (about 8.6 MB, held by every GPU that loads the library
+ * until exit); larger n returns GS_ERR_CAPACITY. The first call on a device
+ * looks up that array's device address, so make it before any stream
+ * capture. Calls share the array: calls that overlap on the GPU (different
+ * streams, or different host threads) race and corrupt each other's
+ * results. Stream-ordered, does not synchronise. */
+gs_status gs_radix_sort_pairs_noalloc(uint32_t* keys, uint32_t* vals, uint64_t n, uint32_t key_bits, void* stream);
+
 /* Camera-to-world rotation (column-major 3x3) exactly as the forward computes
  * it from gs_camera.quat (glam Mat3::from_quat of the normalised quaternion,
  * rasterizer.rs:410). Host-only, no GPU needed. */

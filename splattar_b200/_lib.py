@@ -106,6 +106,7 @@ def lib():
         "gs_binner_encode": [vp, vp, vp, u32, u32, vp],
         "gs_binner_buffer": [vp, u32, C.POINTER(vp), C.POINTER(C.c_size_t)],
         "gs_radix_sort_pairs": [vp, vp, u64, u32, vp],
+        "gs_radix_sort_pairs_noalloc": [vp, vp, u64, u32, vp],
         "gs_exclusive_scan_u32": [vp, vp, u64, vp, vp],
         "gs_camera_rotation": [C.POINTER(Camera), C.POINTER(C.c_float)],
         "gs_shutdown": [],
@@ -140,5 +141,6 @@ def exported_symbols() -> list[str]:
         "gs_rasterizer_read", "gs_rasterizer_write", "gs_rasterizer_read_async", "gs_rasterizer_write_async",
         "gs_rasterizer_check", "gs_last_error", "gs_loss_l1_ssim", "gs_optimizer_init", "gs_optimizer_step",
         "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_binner_create", "gs_binner_destroy",
-        "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_exclusive_scan_u32",
+        "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_radix_sort_pairs_noalloc",
+        "gs_exclusive_scan_u32",
         "gs_camera_rotation", "gs_shutdown"]

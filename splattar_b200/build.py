@@ -25,6 +25,7 @@ UNITS = {
     "gs_sort.cu": [],
     "gs_loss.cu": [],
     "gs_optim.cu": [],
+    "gs_noalloc.cu": [],
 }
 HEADERS = ["gs_common.cuh", "gs_kernels.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -26,6 +26,8 @@ namespace gs {
 
 static thread_local std::string g_last_error;
 
+void set_error_message(const std::string& msg) { g_last_error = msg; }
+
 int cuda_fail(cudaError_t e, const char* expr, const char* file, int line) {
   char buf[512];
   snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", expr, cudaGetErrorString(e), file, line);

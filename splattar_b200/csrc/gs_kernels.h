@@ -5,9 +5,14 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "gs_common.cuh"
 
 namespace gs {
+
+// Sets the text gs_last_error(NULL) reports.
+void set_error_message(const std::string& msg);
 
 struct ProjectArgs {
   const ViewInfo* views;

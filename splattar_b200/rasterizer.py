@@ -305,6 +305,13 @@ def radix_sort_pairs(keys_ptr: int, vals_ptr: int, n: int, key_bits: int = 32, s
     check(lib().gs_radix_sort_pairs(keys_ptr, vals_ptr, n, key_bits, stream))
 
 
+def radix_sort_pairs_noalloc(keys_ptr: int, vals_ptr: int, n: int, key_bits: int = 32, stream: int = 0):
+    """The same sort for callers that cannot let the library allocate: scratch
+    is a fixed device array for at most 1,048,576 pairs; overlapping calls on
+    the GPU race. Stream-ordered (does not synchronise)."""
+    check(lib().gs_radix_sort_pairs_noalloc(keys_ptr, vals_ptr, n, key_bits, stream))
+
+
 def exclusive_scan_u32(in_ptr: int, out_ptr: int, n: int, total_ptr: int = 0, stream: int = 0):
     """PrefixSum::encode on caller device arrays."""
     check(lib().gs_exclusive_scan_u32(in_ptr, out_ptr, n, total_ptr or None, stream))
