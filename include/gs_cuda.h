@@ -238,6 +238,10 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
  * size is fixed at 16 in this build. Blocking. */
 gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels, void* stream,
                       uint32_t out[4]);
+/* Applies launch shapes (the layout of gs_autotune's out, e.g. a stored
+ * result) without timing. Each pair must be one of the shapes gs_autotune
+ * tries, else GS_ERR_INVALID_ARG and nothing changes. Host-only. */
+gs_status gs_set_launch_shapes(gs_rasterizer* r, const uint32_t shapes[4]);
 
 /* Densify/prune compaction (no reference counterpart; the reference only
  * relocates at fixed budget, trainer.rs:1558-1689): surfels whose mean

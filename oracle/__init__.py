@@ -70,6 +70,16 @@ def lib():
         L.orc_camera_rotation_f32.argtypes = [vp, vp]
         L.orc_camera_rotation_f32.restype = None
         L.orc_gauss_weights.argtypes = [vp]
+        L.orc_sh_color.argtypes = [i32, vp, vp, vp, vp]
+        L.orc_sh_color.restype = i32
+        L.orc_triple.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.orc_quat_to_mat.argtypes = [vp, vp]
+        L.orc_quat_to_mat.restype = None
+        L.orc_quat_grad.argtypes = [vp, vp, vp]
+        L.orc_quat_grad.restype = None
+        L.orc_sh_basis.argtypes = [i32, vp, vp, vp]
+        L.orc_sh_basis.restype = i32
+        L.orc_triple.restype = f64
         L.orc_gauss_weights.restype = None
         L.orc_l1_ssim.argtypes = [vp, vp, i32, i32, f64, f64, vp, vp, vp]
         L.orc_l1_ssim.restype = f64
@@ -207,6 +217,51 @@ def project_f32(pos4, scales2, quats4, rot9, center3, focal, width, height, tile
     lib().orc_project_f32(n, _p(pos4), _p(scales2), _p(quats4), _p(rot9), _p(center3), float(focal), width, height,
                           tile, _p(rects), _p(keys), _p(camo))
     return rects, keys, camo
+
+
+def sh_color(degree: int, coeffs, direction):
+    """(rgb, clamp mask) of max(0.5 + sum sh_k basis_k(dir), 0); coeffs (k, 3)."""
+    sh = np.zeros(48)
+    c = np.asarray(coeffs, np.float64).reshape(-1)
+    sh[:c.size] = c
+    d = np.ascontiguousarray(direction, np.float64)
+    rgb = np.zeros(3)
+    cm = np.zeros(3, np.int32)
+    lib().orc_sh_color(degree, _p(sh), _p(d), _p(rgb), cm.ctypes.data)
+    return rgb, cm.astype(bool)
+
+
+def quat_to_mat(q) -> np.ndarray:
+    """Column-major rotation (as a 3x3 array indexed [col][row]) of an xyzw quaternion."""
+    q = np.ascontiguousarray(q, np.float64)
+    r = np.zeros(9)
+    lib().orc_quat_to_mat(_p(q), _p(r))
+    return r.reshape(3, 3)
+
+
+def quat_grad(q, dl_dr_cols) -> np.ndarray:
+    """dL/dq for dL/dR given as [col][row]."""
+    q = np.ascontiguousarray(q, np.float64)
+    w = np.ascontiguousarray(dl_dr_cols, np.float64).reshape(9)
+    out = np.zeros(4)
+    lib().orc_quat_grad(_p(q), _p(w), _p(out))
+    return out
+
+
+def sh_basis(degree: int, direction):
+    """(basis values (k,), d basis / d dir (k, 3))."""
+    d = np.ascontiguousarray(direction, np.float64)
+    b, g = np.zeros(16), np.zeros(48)
+    nb = lib().orc_sh_basis(degree, _p(d), _p(b), _p(g))
+    return b[:nb], g[:3 * nb].reshape(nb, 3)
+
+
+def triple(a, b, c):
+    """(a . (b x c), d/da, d/db, d/dc)."""
+    a, b, c = (np.ascontiguousarray(x, np.float64) for x in (a, b, c))
+    ga, gb, gc = np.zeros(3), np.zeros(3), np.zeros(3)
+    t = lib().orc_triple(_p(a), _p(b), _p(c), _p(ga), _p(gb), _p(gc))
+    return t, ga, gb, gc
 
 
 def gauss_weights() -> np.ndarray:

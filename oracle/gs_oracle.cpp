@@ -306,6 +306,50 @@ static void blur_sep(const std::vector<double>& src, std::vector<double>& dst, i
     }
 }
 
+// SH colour of one surfel seen along dir (coefficient-major rgb, up to 16
+// coefficients); clamped[3] receives the clamp mask. Returns the number of
+// basis functions of the degree.
+int orc_sh_color(int degree, const double* sh, const double* dir, double* rgb, int* clamped) {
+  bool cm[3];
+  V3 c = sh_color(degree, sh, V3(dir[0], dir[1], dir[2]), cm);
+  rgb[0] = c.x; rgb[1] = c.y; rgb[2] = c.z;
+  for (int k = 0; k < 3; ++k) clamped[k] = cm[k] ? 1 : 0;
+  return (degree + 1) * (degree + 1);
+}
+
+// Rotation of a (not necessarily unit) xyzw quaternion, column-major 3x3.
+void orc_quat_to_mat(const double* q, double* r9) {
+  M3 m = quat_to_mat(q);
+  for (int c = 0; c < 3; ++c) { r9[3 * c] = m.c[c].x; r9[3 * c + 1] = m.c[c].y; r9[3 * c + 2] = m.c[c].z; }
+}
+
+// dL/dq through the normalisation for dL/dR given column-major.
+void orc_quat_grad(const double* q, const double* dl_dr9, double* out4) {
+  M3 w;
+  for (int c = 0; c < 3; ++c) w.c[c] = V3(dl_dr9[3 * c], dl_dr9[3 * c + 1], dl_dr9[3 * c + 2]);
+  quat_grad(q, w, out4);
+}
+
+// SH basis values (b[16]) and their gradients w.r.t. the direction (g[48],
+// xyz per basis function); returns the number of basis functions.
+int orc_sh_basis(int degree, const double* d, double* b, double* g) {
+  V3 dir(d[0], d[1], d[2]), gg[16];
+  const int nb = sh_basis(degree, dir, b);
+  sh_basis_grad(degree, dir, gg);
+  for (int k = 0; k < nb; ++k) { g[3 * k] = gg[k].x; g[3 * k + 1] = gg[k].y; g[3 * k + 2] = gg[k].z; }
+  return nb;
+}
+
+// Scalar triple product a . (b x c) and its gradients (math.rs triple_grads).
+double orc_triple(const double* a, const double* b, const double* c, double* ga, double* gb, double* gc) {
+  V3 A(a[0], a[1], a[2]), B(b[0], b[1], b[2]), Cc(c[0], c[1], c[2]), GA, GB, GC;
+  triple_grads(A, B, Cc, GA, GB, GC);
+  const V3* g[3] = {&GA, &GB, &GC};
+  double* o[3] = {ga, gb, gc};
+  for (int k = 0; k < 3; ++k) { o[k][0] = g[k]->x; o[k][1] = g[k]->y; o[k][2] = g[k]->z; }
+  return triple(A, B, Cc);
+}
+
 void orc_gauss_weights(double* w6) {
   double s = 0, g[6];
   for (int k = 0; k <= 5; ++k) g[k] = std::exp(-(double)(k * k) / (2.0 * 1.5 * 1.5));

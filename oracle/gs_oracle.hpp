@@ -192,6 +192,18 @@ inline int sh_basis_grad(int degree, const V3& d, V3 g[16]) {
   return k;
 }
 
+// View-dependent colour of one surfel: max(0.5 + sum_k sh_k * basis_k(dir), 0)
+// per channel, with the clamp mask (crates/gs-cpu-ref/src/forward.rs
+// prepare; crates/gs-core/src/sh.rs sh_to_color). sh is coefficient-major rgb.
+inline V3 sh_color(int degree, const double* sh, const V3& dir, bool clamped[3]) {
+  double b[16];
+  const int nb = sh_basis(degree, dir, b);
+  V3 raw(0.5, 0.5, 0.5);
+  for (int k = 0; k < nb; ++k) raw += V3(sh[3 * k], sh[3 * k + 1], sh[3 * k + 2]) * b[k];
+  clamped[0] = raw.x < 0; clamped[1] = raw.y < 0; clamped[2] = raw.z < 0;
+  return vmax0(raw);
+}
+
 // ------------------------------------------------------------------ scene.rs
 // Surfels are stored SoA. SH is always padded to 16 coefficients (48 doubles
 // per surfel, coefficient-major rgb), the same padding the GPU uses.
@@ -283,16 +295,10 @@ inline std::vector<SurfelCam> prepare(const Scene& s, const Camera& cam, int til
     V3 tu = r_cam.mul_t(rs.c[0] * s.scales[2 * i]);
     V3 tv = r_cam.mul_t(rs.c[1] * s.scales[2 * i + 1]);
     V3 dir = normalize(p - C);
-    double b[16];
-    int nb = sh_basis(s.sh_degree, dir, b);
-    V3 raw(0.5, 0.5, 0.5);
-    const double* sh = s.sh + 48 * i;
-    for (int k = 0; k < nb; ++k) raw += V3(sh[3 * k], sh[3 * k + 1], sh[3 * k + 2]) * b[k];
     SurfelCam sc;
     sc.idx = i;
     sc.c = c; sc.tu = tu; sc.tv = tv;
-    sc.clamped[0] = raw.x < 0; sc.clamped[1] = raw.y < 0; sc.clamped[2] = raw.z < 0;
-    sc.color = vmax0(raw);
+    sc.color = sh_color(s.sh_degree, s.sh + 48 * i, dir, sc.clamped);
     V3 nrm = cross(tu, tv);
     if (dot(nrm, nrm) > 0.0) {
       nrm = normalize(nrm);

@@ -979,6 +979,29 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
   return GS_OK;
 }
 
+// Launch shapes (batch, pixels per thread) the raster dispatchers instantiate.
+static const int FWD_SHAPES[6][2] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}, {64, 4}};
+static const int BWD_SHAPES[4][2] = {{64, 1}, {64, 2}, {128, 2}, {64, 4}};
+
+gs_status gs_set_launch_shapes(gs_rasterizer* r, const uint32_t shapes[4]) {
+  if (!r || !shapes) return GS_ERR_INVALID_ARG;
+  auto listed = [](const auto& tab, uint32_t b, uint32_t p) {
+    for (const auto& s : tab)
+      if ((uint32_t)s[0] == b && (uint32_t)s[1] == p) return true;
+    return false;
+  };
+  if (!listed(FWD_SHAPES, shapes[0], shapes[1]))
+    return fail(r, GS_ERR_INVALID_ARG, "gs_set_launch_shapes: unsupported forward (batch, pixels per thread)");
+  if (!listed(BWD_SHAPES, shapes[2], shapes[3]))
+    return fail(r, GS_ERR_INVALID_ARG, "gs_set_launch_shapes: unsupported backward (batch, pixels per thread)");
+  r->fwd_batch = (int)shapes[0];
+  r->fwd_ppt = (int)shapes[1];
+  r->bwd_batch = (int)shapes[2];
+  r->bwd_ppt = (int)shapes[3];
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
+  return GS_OK;
+}
+
 gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32_t n, void* stream, uint32_t out[4]) {
   if (!r || !out) return GS_ERR_INVALID_ARG;
   gs_status s = set_views(r, cams, nv, n);
@@ -1003,7 +1026,7 @@ gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint
     return ms;
   };
   // Forward: every (batch, pixels per thread) shape.
-  const int fshape[6][2] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}, {64, 4}};
+  const auto& fshape = FWD_SHAPES;
   float best = 1e30f;
   int bf = 1;
   for (int k = 0; k < 6; ++k) {
@@ -1024,7 +1047,7 @@ gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint
   }
   if (s) { cudaEventDestroy(e0); cudaEventDestroy(e1); return s; }
   // Backward (colour-only, as in the training step): every shape.
-  const int bshape[4][2] = {{64, 1}, {64, 2}, {128, 2}, {64, 4}};
+  const auto& bshape = BWD_SHAPES;
   best = 1e30f;
   int bb = 2;
   for (int k = 0; k < 4; ++k) {

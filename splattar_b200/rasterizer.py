@@ -225,6 +225,12 @@ class Rasterizer:
         return {"fwd_batch": out[0], "fwd_pixels_per_thread": out[1], "bwd_batch": out[2],
                 "bwd_pixels_per_thread": out[3]}
 
+    def set_launch_shapes(self, fwd_batch: int, fwd_pixels_per_thread: int, bwd_batch: int,
+                          bwd_pixels_per_thread: int):
+        """Apply raster launch shapes (e.g. a stored autotune result) without timing."""
+        arr = (C.c_uint32 * 4)(fwd_batch, fwd_pixels_per_thread, bwd_batch, bwd_pixels_per_thread)
+        self._chk(lib().gs_set_launch_shapes(self._h, arr))
+
     def densify_prune(self, grad_threshold: float, opacity_threshold: float, num_surfels: int,
                       stream: int = 0) -> int:
         cfg = DensifyConfig(grad_threshold, opacity_threshold)
