@@ -121,7 +121,8 @@ typedef enum {
   GS_BUF_GRAD_CAM = 16,   /* 16 floats per view: dL/dR (column-major 9), dL/dC 3, dL/dfocal, pad 3 */
   GS_BUF_TARGET = 17,     /* float4 loss target per pixel (SsimLoss::target) */
   GS_BUF_RANGES = 18,     /* uint2 per tile (all views' tiles back to back): [start, end) */
-  GS_BUF_SORTED_ITEMS = 19,/* u32 per entry: item view*num_surfels + surfel, tile-major, depth-ascending */
+  GS_BUF_SORTED_ITEMS = 19,/* uint2 per entry, tile-major, depth-ascending: (tile id counted from the first view's
+                              first tile, item view*num_surfels + surfel; the expansion index in deterministic mode) */
   GS_BUF_ENTRY_COUNT = 20,/* u64: total tile entries of the last forward */
   GS_BUF_LOSS = 21,       /* double per view x2: sum |x-y| over rgb, sum SSIM over rgb */
   GS_BUF_RAW_POS = 22,    /* optimizer raw parameters (Optimizer ParamClass::raw) */

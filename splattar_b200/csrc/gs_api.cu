@@ -89,9 +89,8 @@ struct gs_rasterizer {
   uint32_t* offsets = nullptr;
   uint32_t* entry_offset = nullptr;
 
-  // per entry
-  uint32_t* ent_keys[2] = {nullptr, nullptr};
-  uint32_t* ent_vals[2] = {nullptr, nullptr};
+  // per entry: (tile, item) pairs, ping-pong buffers of the tile sort
+  uint2* ent_pairs[2] = {nullptr, nullptr};
   uint32_t* exp_item = nullptr;
   float* partials = nullptr;
   uint2* ranges = nullptr;
@@ -160,8 +159,8 @@ struct gs_binner {
   uint32_t* offsets = nullptr;
   uint32_t* item_keys[2] = {nullptr, nullptr};
   uint32_t* item_vals[2] = {nullptr, nullptr};
-  uint32_t* ent_keys[2] = {nullptr, nullptr};
-  uint32_t* ent_vals[2] = {nullptr, nullptr};
+  uint2* ent_pairs[2] = {nullptr, nullptr};
+  uint32_t* sorted_entries = nullptr;
   uint32_t* entry_items = nullptr;
   uint2* ranges = nullptr;
   unsigned long long* total = nullptr;
@@ -305,7 +304,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ea.views = vdev; ea.items_per_view = n; ea.tiles_x = 0;
   ea.n_items_dev = nullptr; ea.n_items_host = items;
   ea.total = r->entry_total; ea.capacity = r->max_entries;
-  ea.keys = r->ent_keys[0]; ea.vals = r->ent_vals[0];
+  ea.pairs = r->ent_pairs[0];
   ea.val_mode = r->det ? 1 : 0;
   ea.exp_item = r->exp_item;
   ea.entry_offset = r->det ? r->entry_offset : nullptr;
@@ -313,14 +312,14 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   TRY_LAUNCH(r, launch_expand(ea, st));
   mark(prof, 2, st);
   const int bits = tile_key_bits((uint32_t)std::max(tiles, 1));
-  TRY_LAUNCH(r, launch_radix_sort(r->ent_keys[0], r->ent_vals[0], r->ent_keys[1], r->ent_vals[1], r->max_entries,
-                                  n_entries, bits, r->sort_scratch, &r->ent_in1, st));
+  TRY_LAUNCH(r, launch_radix_sort_pairs(r->ent_pairs[0], r->ent_pairs[1], r->max_entries, n_entries, bits,
+                                        r->sort_scratch, &r->ent_in1, st));
   mark(prof, 3, st);
-  TRY_LAUNCH(r, launch_ranges(r->ent_keys[r->ent_in1], r->entry_total, r->max_entries, r->ranges, (uint32_t)tiles, st));
+  TRY_LAUNCH(r, launch_ranges(r->ent_pairs[r->ent_in1], r->entry_total, r->max_entries, r->ranges, (uint32_t)tiles, st));
   mark(prof, 4, st);
   RasterArgs ra{};
   ra.views = vdev; ra.n_views = (int)nv; ra.total_tiles = tiles;
-  ra.ranges = r->ranges; ra.sorted_vals = r->ent_vals[r->ent_in1]; ra.exp_item = r->exp_item;
+  ra.ranges = r->ranges; ra.sorted_pairs = r->ent_pairs[r->ent_in1]; ra.exp_item = r->exp_item;
   ra.records = r->records;
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.tile_counter = r->words + 2;
@@ -340,7 +339,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
 RasterArgs bwd_args(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, int tiles) {
   RasterArgs ra{};
   ra.views = vdev; ra.n_views = (int)nv; ra.total_tiles = tiles;
-  ra.ranges = r->ranges; ra.sorted_vals = r->ent_vals[r->ent_in1]; ra.exp_item = r->exp_item;
+  ra.ranges = r->ranges; ra.sorted_pairs = r->ent_pairs[r->ent_in1]; ra.exp_item = r->exp_item;
   ra.records = r->records;
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.dl_dcolor = r->dl_dcolor; ra.dl_dnormal = r->dl_dnormal;
@@ -614,7 +613,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   ALLOC(r->rects, I);
   for (int k = 0; k < 2; ++k) { ALLOC(r->item_keys[k], I); ALLOC(r->item_vals[k], I); }
   ALLOC(r->counts, I); ALLOC(r->offsets, I);
-  for (int k = 0; k < 2; ++k) { ALLOC(r->ent_keys[k], E); ALLOC(r->ent_vals[k], E); }
+  for (int k = 0; k < 2; ++k) ALLOC(r->ent_pairs[k], E);
   if (r->det) {
     ALLOC(r->exp_item, E);
     ALLOC(r->partials, E * GG_STRIDE);
@@ -661,7 +660,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
   if (r->cap_stream) cudaStreamDestroy(r->cap_stream);
   void* ptrs[] = {r->positions, r->scales, r->quats, r->opacities, r->sh, r->sh_half, r->records, r->rects,
                   r->item_keys[0], r->item_keys[1], r->item_vals[0], r->item_vals[1], r->counts, r->offsets,
-                  r->entry_offset, r->ent_keys[0], r->ent_keys[1], r->ent_vals[0], r->ent_vals[1], r->exp_item,
+                  r->entry_offset, r->ent_pairs[0], r->ent_pairs[1], r->exp_item,
                   r->partials, r->ranges, r->entry_total, r->words, r->out_color, r->out_aux, r->out_normal,
                   r->dl_dcolor, r->dl_dnormal, r->target, r->out_nc, r->coef, r->loss_sums, r->grad_geom,
                   r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
@@ -760,7 +759,7 @@ static gs_status buffer_info(gs_rasterizer* r, gs_buffer_id id, void** p, size_t
     case GS_BUF_GRAD_CAM: *p = r->grad_cam; *bytes = 64 * (size_t)r->max_views; break;
     case GS_BUF_TARGET: *p = r->target; *bytes = 16 * P; break;
     case GS_BUF_RANGES: *p = r->ranges; *bytes = 8 * (size_t)r->max_tiles; break;
-    case GS_BUF_SORTED_ITEMS: *p = r->ent_vals[r->ent_in1]; *bytes = 4 * E; break;
+    case GS_BUF_SORTED_ITEMS: *p = r->ent_pairs[r->ent_in1]; *bytes = 8 * E; break;
     case GS_BUF_ENTRY_COUNT: *p = r->entry_total; *bytes = 8; break;
     case GS_BUF_LOSS: *p = r->loss_sums; *bytes = 16 * (size_t)r->max_views; break;
     case GS_BUF_RAW_POS: *p = r->raw[0]; *bytes = 16 * N; break;
@@ -1119,8 +1118,8 @@ gs_status gs_binner_create(uint32_t max_items, uint64_t max_entries, uint32_t nu
   cudaError_t e = cudaSuccess;
   auto A = [&](auto*& p, size_t n) { if (e == cudaSuccess) e = dalloc(p, n); };
   A(b->counts, I); A(b->ref_offsets, I); A(b->offsets, I);
-  for (int k = 0; k < 2; ++k) { A(b->item_keys[k], I); A(b->item_vals[k], I); A(b->ent_keys[k], E); A(b->ent_vals[k], E); }
-  A(b->entry_items, E); A(b->ranges, num_tiles); A(b->total, 1); A(b->words, 8);
+  for (int k = 0; k < 2; ++k) { A(b->item_keys[k], I); A(b->item_vals[k], I); A(b->ent_pairs[k], E); }
+  A(b->sorted_entries, E); A(b->entry_items, E); A(b->ranges, num_tiles); A(b->total, 1); A(b->words, 8);
   unsigned char *s1 = nullptr, *s2 = nullptr;
   A(s1, scan_scratch_bytes()); A(s2, sort_scratch_bytes());
   b->scan_scratch = s1; b->sort_scratch = s2;
@@ -1137,7 +1136,7 @@ gs_status gs_binner_create(uint32_t max_items, uint64_t max_entries, uint32_t nu
 gs_status gs_binner_destroy(gs_binner* b) {
   if (!b) return GS_OK;
   void* ptrs[] = {b->counts, b->ref_offsets, b->offsets, b->item_keys[0], b->item_keys[1], b->item_vals[0],
-                  b->item_vals[1], b->ent_keys[0], b->ent_keys[1], b->ent_vals[0], b->ent_vals[1],
+                  b->item_vals[1], b->ent_pairs[0], b->ent_pairs[1], b->sorted_entries,
                   b->entry_items, b->ranges, b->total, b->words, b->scan_scratch, b->sort_scratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1173,14 +1172,15 @@ extern "C" gs_status gs_binner_encode(gs_binner* b, const uint32_t* rects_dev, c
     ea.views = nullptr; ea.items_per_view = n ? n : 1; ea.tiles_x = tiles_x;
     ea.n_items_dev = nullptr; ea.n_items_host = n;
     ea.total = b->total; ea.capacity = b->max_entries;
-    ea.keys = b->ent_keys[0]; ea.vals = b->ent_vals[0];
+    ea.pairs = b->ent_pairs[0];
     ea.val_mode = 2; ea.ref_offsets = b->ref_offsets; ea.entry_items = b->entry_items;
     ea.error_word = b->words + 1;
     e = launch_expand(ea, st);
   }
-  if (!e) e = launch_radix_sort(b->ent_keys[0], b->ent_vals[0], b->ent_keys[1], b->ent_vals[1], b->max_entries,
-                                b->words, tile_key_bits(b->num_tiles), b->sort_scratch, &b->ent_in1, st);
-  if (!e) e = launch_ranges(b->ent_keys[b->ent_in1], b->total, b->max_entries, b->ranges, b->num_tiles, st);
+  if (!e) e = launch_radix_sort_pairs(b->ent_pairs[0], b->ent_pairs[1], b->max_entries, b->words,
+                                      tile_key_bits(b->num_tiles), b->sort_scratch, &b->ent_in1, st);
+  if (!e) e = launch_ranges(b->ent_pairs[b->ent_in1], b->total, b->max_entries, b->ranges, b->num_tiles, st);
+  if (!e) e = launch_pair_values(b->ent_pairs[b->ent_in1], b->sorted_entries, b->total, b->max_entries, st);
   if (e) return fail(nullptr, GS_ERR_CUDA, std::string("binner encode: ") + cudaGetErrorString((cudaError_t)e));
   // The reference asserts on overflow; report it here (blocking).
   uint32_t w = 0;
@@ -1197,7 +1197,7 @@ extern "C" gs_status gs_binner_encode(gs_binner* b, const uint32_t* rects_dev, c
 extern "C" gs_status gs_binner_buffer(gs_binner* b, uint32_t which, void** dptr, size_t* bytes) {
   if (!b || !dptr || !bytes) return GS_ERR_INVALID_ARG;
   switch (which) {
-    case 0: *dptr = b->ent_vals[b->ent_in1]; *bytes = 4 * b->max_entries; break;
+    case 0: *dptr = b->sorted_entries; *bytes = 4 * b->max_entries; break;
     case 1: *dptr = b->entry_items; *bytes = 4 * b->max_entries; break;
     case 2: *dptr = b->ranges; *bytes = 8ull * b->num_tiles; break;
     case 3: *dptr = b->total; *bytes = 8; break;

@@ -75,7 +75,7 @@ struct RasterArgs {
   int n_views;
   int total_tiles;
   const uint2* ranges;
-  const uint32_t* sorted_vals;  // item id (atomic mode) or expansion index (deterministic mode)
+  const uint2* sorted_pairs;    // (tile, item id) (atomic mode) or (tile, expansion index) (deterministic mode)
   const uint32_t* exp_item;     // expansion index -> item (deterministic mode)
   const void* records;
   float4* out_color;
@@ -105,7 +105,7 @@ int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, int ppt, int batc
 // Scratch for the scan and the radix sort; sized by the caller through
 // scan_scratch_bytes / sort_scratch_bytes.
 constexpr int SCAN_GRID = 512;    // blocks of the chunked scan
-constexpr int SORT_GRID = 592;    // blocks of the chunked radix passes (4 per SM, one wave)
+constexpr int SORT_GRID = 444;    // blocks of the chunked radix passes (3 per SM, one wave)
 size_t scan_scratch_bytes();
 size_t sort_scratch_bytes();
 
@@ -118,6 +118,12 @@ int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_
 // between (k0,v0) and (k1,v1); returns in *result_in_1 where the output is.
 int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n_host, const uint32_t* n_dev,
                       int key_bits, void* scratch, int* result_in_1, cudaStream_t st);
+// The same sort on interleaved (key, val) pairs, ping-ponging between p0 and p1.
+int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch,
+                            int* result_in_1, cudaStream_t st);
+// dst[i] = src[i].y for i < min(*n, capacity).
+int launch_pair_values(const uint2* src, uint32_t* dst, const unsigned long long* n, uint64_t capacity,
+                       cudaStream_t st);
 
 struct ExpandArgs {
   const uint32_t* perm;        // depth-sorted item order
@@ -131,8 +137,8 @@ struct ExpandArgs {
   uint32_t n_items_host;
   const unsigned long long* total;  // entries
   uint64_t capacity;
-  uint32_t* keys;              // tile id (relative to the launch's first view) per entry
-  uint32_t* vals;              // per val_mode: 0 item, 1 expansion index, 2 reference entry index
+  uint2* pairs;                // per entry: (tile id relative to the launch's first view, value per val_mode:
+                               // 0 item, 1 expansion index, 2 reference entry index)
   int val_mode;
   uint32_t* exp_item;          // val_mode 1: expansion index -> item
   uint32_t* entry_offset;      // item -> first expansion index, or null
@@ -141,8 +147,8 @@ struct ExpandArgs {
   uint32_t* error_word;
 };
 int launch_expand(const ExpandArgs& a, cudaStream_t st);
-// ranges[t] = [start, end) of tile t in the sorted key stream (ranges zeroed by the callee).
-int launch_ranges(const uint32_t* sorted_keys, const unsigned long long* total, uint64_t capacity, uint2* ranges,
+// ranges[t] = [start, end) of tile t in the sorted pairs (ranges zeroed by the callee).
+int launch_ranges(const uint2* sorted_pairs, const unsigned long long* total, uint64_t capacity, uint2* ranges,
                   uint32_t num_tiles, cudaStream_t st);
 // After the entry scan: on overflow flag the error and zero the entry counts.
 int launch_entry_guard(unsigned long long* total, uint32_t* count, uint64_t capacity, uint32_t* error_word,

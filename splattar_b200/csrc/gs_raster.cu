@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
       uint32_t item = 0;
       float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
       if (tid < count) {
-        item = __ldg(&a.sorted_vals[base + tid]);
+        item = __ldg(&a.sorted_pairs[base + tid].y);
         if (DET) item = __ldg(&a.exp_item[item]);
         bb = load_record_box<PREC>(a.records, item);
         keep = box_hits_tile(bb, g);
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
     if (DET) {
       // Entries past the tile's last contributor get zero partials.
       for (uint32_t e = range.x + maxnc + tid; e < range.y; e += NT) {
-        const uint32_t q = __ldg(&a.sorted_vals[e]);
+        const uint32_t q = __ldg(&a.sorted_pairs[e].y);
         float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)q * GG_STRIDE);
 #pragma unroll
         for (int k = 0; k < NQ; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
       uint32_t item = 0, q = 0;
       float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
       if (tid < count) {
-        item = __ldg(&a.sorted_vals[lo + tid]);
+        item = __ldg(&a.sorted_pairs[lo + tid].y);
         q = item;
         if (DET) item = __ldg(&a.exp_item[q]);
         bb = load_record_box<PREC>(a.records, item);

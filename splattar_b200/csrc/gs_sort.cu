@@ -103,16 +103,22 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t* in, 
 
 // ------------------------------------------------------------ radix sort
 // Reduce-then-scan LSD passes of 8-bit digits. Every block owns a contiguous
-// chunk of the input and walks it in tiles of RS_TILE keys; within a tile,
-// warp w holds keys [256w, 256w+256) in 8 rounds of 32 (all loads issued
-// before any ranking), ranks them stably by ballot multi-split, and the block
-// combines the warps' digit counts in warp order. The per-(digit, block)
-// counts are scanned between the upsweep and the downsweep.
+// chunk of the input and walks it in tiles of RS_TILE elements.
+//   upsweep: per-warp digit histograms in shared memory by shared atomics
+//     (four independent loads in flight per thread), summed per block;
+//   downsweep: warp w holds elements [256w, 256w+256) of the tile in 8 rounds
+//     of 32, ranks them stably by ballot multi-split, the block combines the
+//     warps' digit counts in warp order, the tile is reordered through shared
+//     memory and written out in digit runs. The next tile's elements are
+//     loaded while the current one is ranked and written.
+// The per-(digit, block) counts are scanned between the two. Elements are
+// (key, value) pairs, either in two arrays or interleaved as uint2.
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ROUNDS = 8;                        // keys per thread per tile
+constexpr int RS_ROUNDS = 8;                        // elements per thread per tile
 constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;     // 2048
 constexpr int RS_BINS = 256;
+static_assert(SORT_GRID % 148 == 0, "whole waves of the downsweep (3 blocks per SM)");
 
 // Lanes of the warp whose digit equals this lane's (multi-split by ballots).
 __device__ __forceinline__ uint32_t match_digit(uint32_t d, int nbits, uint32_t active) {
@@ -128,33 +134,44 @@ __device__ __forceinline__ uint32_t match_digit(uint32_t d, int nbits, uint32_t 
   return peers;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* __restrict__ keys, uint64_t n_host,
-                                                           const uint32_t* n_dev, int shift, int nbits,
-                                                           uint32_t* __restrict__ hist) {
+// Element access: two arrays, or one interleaved uint2 array.
+struct SplitIO {
+  const uint32_t* kin; const uint32_t* vin; uint32_t* kout; uint32_t* vout;
+  __device__ __forceinline__ uint32_t key(uint64_t i) const { return __ldg(kin + i); }
+  __device__ __forceinline__ uint2 load(uint64_t i) const { return make_uint2(__ldg(kin + i), __ldg(vin + i)); }
+  __device__ __forceinline__ void store(size_t g, uint2 e) const { kout[g] = e.x; vout[g] = e.y; }
+};
+struct PairIO {
+  const uint2* in; uint2* out;
+  __device__ __forceinline__ uint32_t key(uint64_t i) const {
+    return __ldg(reinterpret_cast<const uint32_t*>(in + i));
+  }
+  __device__ __forceinline__ uint2 load(uint64_t i) const { return __ldg(in + i); }
+  __device__ __forceinline__ void store(size_t g, uint2 e) const { out[g] = e; }
+};
+
+template <class IO>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(IO io, uint64_t n_host, const uint32_t* n_dev, int shift,
+                                                           int nbits, uint32_t* __restrict__ hist) {
   __shared__ uint32_t s_hist[RS_WARPS][RS_BINS];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5;
   for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_hist[0][0])[k] = 0;
   __syncthreads();
   const uint64_t n = read_n(n_host, n_dev);
   const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
   const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
   const uint32_t mask = (1u << nbits) - 1u;
-  for (uint64_t t0 = beg; t0 < end; t0 += RS_TILE) {
-    uint32_t d[RS_ROUNDS];
-#pragma unroll
-    for (int r = 0; r < RS_ROUNDS; ++r) {
-      const uint64_t i = t0 + warp * (RS_ROUNDS * 32) + r * 32 + lane;
-      d[r] = i < end ? (__ldg(keys + i) >> shift) & mask : 0xffffffffu;
-    }
-#pragma unroll
-    for (int r = 0; r < RS_ROUNDS; ++r) {
-      const bool valid = d[r] != 0xffffffffu;
-      const uint32_t act = __ballot_sync(FULL, valid);
-      if (act == 0) break;
-      const uint32_t peers = match_digit(d[r], nbits, act);
-      if (valid && (peers & lanemask_lt()) == 0) s_hist[warp][d[r]] += __popc(peers);
-    }
+  uint32_t* h = s_hist[warp];
+  uint64_t i = beg + tid;
+  for (; i + 3 * RS_THREADS < end; i += 4 * RS_THREADS) {
+    const uint32_t k0 = io.key(i), k1 = io.key(i + RS_THREADS), k2 = io.key(i + 2 * RS_THREADS),
+                   k3 = io.key(i + 3 * RS_THREADS);
+    atomicAdd(h + ((k0 >> shift) & mask), 1u);
+    atomicAdd(h + ((k1 >> shift) & mask), 1u);
+    atomicAdd(h + ((k2 >> shift) & mask), 1u);
+    atomicAdd(h + ((k3 >> shift) & mask), 1u);
   }
+  for (; i < end; i += RS_THREADS) atomicAdd(h + ((io.key(i) >> shift) & mask), 1u);
   __syncthreads();
   for (int dd = tid; dd < RS_BINS; dd += RS_THREADS) {
     uint32_t s = 0;
@@ -164,14 +181,11 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* __res
   }
 }
 
-__global__ void __launch_bounds__(RS_THREADS, 4) k_rs_downsweep(const uint32_t* __restrict__ kin,
-                                                                const uint32_t* __restrict__ vin,
-                                                                uint32_t* __restrict__ kout,
-                                                                uint32_t* __restrict__ vout, uint64_t n_host,
-                                                                const uint32_t* n_dev, int shift, int nbits,
+template <class IO>
+__global__ void __launch_bounds__(RS_THREADS, 3) k_rs_downsweep(IO io, uint64_t n_host, const uint32_t* n_dev,
+                                                                int shift, int nbits,
                                                                 const uint32_t* __restrict__ hist) {
-  __shared__ uint32_t s_k[RS_TILE];
-  __shared__ uint32_t s_v[RS_TILE];
+  __shared__ uint2 s_e[RS_TILE];
   __shared__ uint32_t s_wh[RS_WARPS][RS_BINS];
   __shared__ uint32_t s_start[RS_BINS], s_gofs[RS_BINS], s_run[RS_BINS];
   using BS = cub::BlockScan<uint32_t, RS_THREADS>;
@@ -183,16 +197,17 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_downsweep(const uint32_t* 
   if (beg >= end) return;
   const uint32_t mask = (1u << nbits) - 1u;
   s_run[tid] = hist[(size_t)tid * gridDim.x + blockIdx.x];  // RS_THREADS == RS_BINS
-  for (uint64_t t0 = beg; t0 < end; t0 += RS_TILE) {
-    const int tn = (int)min((uint64_t)RS_TILE, end - t0);
-    uint32_t key[RS_ROUNDS], val[RS_ROUNDS];
+  uint2 e[RS_ROUNDS];
+  {
+    const int tn = (int)min((uint64_t)RS_TILE, end - beg);
 #pragma unroll
     for (int r = 0; r < RS_ROUNDS; ++r) {
       const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
-      const bool valid = idx < tn;
-      key[r] = valid ? __ldg(kin + t0 + idx) : 0u;
-      val[r] = valid ? __ldg(vin + t0 + idx) : 0u;
+      e[r] = idx < tn ? io.load(beg + idx) : make_uint2(0u, 0u);
     }
+  }
+  for (uint64_t t0 = beg; t0 < end; t0 += RS_TILE) {
+    const int tn = (int)min((uint64_t)RS_TILE, end - t0);
 #pragma unroll
     for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_wh[0][0])[k] = 0;
     __syncthreads();
@@ -201,7 +216,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_downsweep(const uint32_t* 
     for (int r = 0; r < RS_ROUNDS; ++r) {
       const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
       const bool valid = idx < tn;
-      const uint32_t d = (key[r] >> shift) & mask;
+      const uint32_t d = (e[r].x >> shift) & mask;
       const uint32_t act = __ballot_sync(FULL, valid);
       const uint32_t peers = match_digit(d, nbits, act);
       uint32_t basev = 0;
@@ -232,19 +247,24 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_downsweep(const uint32_t* 
     for (int r = 0; r < RS_ROUNDS; ++r) {
       const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
       if (idx < tn) {
-        const uint32_t d = (key[r] >> shift) & mask;
-        const uint32_t pos = s_start[d] + s_wh[warp][d] + pre[r];
-        s_k[pos] = key[r];
-        s_v[pos] = val[r];
+        const uint32_t d = (e[r].x >> shift) & mask;
+        s_e[s_start[d] + s_wh[warp][d] + pre[r]] = e[r];
+      }
+    }
+    {  // the next tile's elements are in flight during the write-out
+      const uint64_t t1 = t0 + RS_TILE;
+      const int tn1 = t1 < end ? (int)min((uint64_t)RS_TILE, end - t1) : 0;
+#pragma unroll
+      for (int r = 0; r < RS_ROUNDS; ++r) {
+        const int idx = warp * (RS_ROUNDS * 32) + r * 32 + lane;
+        e[r] = idx < tn1 ? io.load(t1 + idx) : make_uint2(0u, 0u);
       }
     }
     __syncthreads();
 #pragma unroll 4
     for (int i = tid; i < tn; i += RS_THREADS) {
-      const uint32_t k = s_k[i];
-      const size_t g = (size_t)(s_gofs[(k >> shift) & mask] + (uint32_t)i);
-      kout[g] = k;
-      vout[g] = s_v[i];
+      const uint2 v = s_e[i];
+      io.store((size_t)(s_gofs[(v.x >> shift) & mask] + (uint32_t)i), v);
     }
     __syncthreads();
   }
@@ -308,31 +328,38 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
         const uint32_t local = j - o_excl;
         const uint32_t ly = local / o_wd, lx = local - ly * o_wd;
         const uint32_t pos = off0 + j;
-        a.keys[pos] = o_tb + (o_y0 + ly) * o_tx + (o_x0 + lx);
+        const uint32_t key = o_tb + (o_y0 + ly) * o_tx + (o_x0 + lx);
+        uint32_t val = o_item;
         if (a.val_mode == 1) {
-          a.vals[pos] = pos;
+          val = pos;
           a.exp_item[pos] = o_item;
         } else if (a.val_mode == 2) {
-          const uint32_t e = a.ref_offsets[o_item] + local;
-          a.vals[pos] = e;
-          if (e < tot) a.entry_items[e] = o_item;
-        } else {
-          a.vals[pos] = o_item;
+          val = a.ref_offsets[o_item] + local;
+          if (val < tot) a.entry_items[val] = o_item;
         }
+        a.pairs[pos] = make_uint2(key, val);
       }
     }
   }
 }
 
-__global__ void __launch_bounds__(256) k_ranges(const uint32_t* keys, const unsigned long long* total,
+__global__ void __launch_bounds__(256) k_ranges(const uint2* pairs, const unsigned long long* total,
                                                 uint64_t capacity, uint2* ranges, uint32_t num_tiles) {
   const uint64_t n = min((uint64_t)*total, capacity);
+  const uint32_t* keys = reinterpret_cast<const uint32_t*>(pairs);  // key of pair p at 2p
   for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t t = keys[p];
+    const uint32_t t = __ldg(keys + 2 * p);
     if (t >= num_tiles) continue;
-    if (p == 0 || keys[p - 1] != t) ranges[t].x = (uint32_t)p;
-    if (p == n - 1 || keys[p + 1] != t) ranges[t].y = (uint32_t)(p + 1);
+    if (p == 0 || __ldg(keys + 2 * (p - 1)) != t) ranges[t].x = (uint32_t)p;
+    if (p == n - 1 || __ldg(keys + 2 * (p + 1)) != t) ranges[t].y = (uint32_t)(p + 1);
   }
+}
+
+__global__ void __launch_bounds__(256) k_pair_values(const uint2* src, uint32_t* dst, const unsigned long long* total,
+                                                     uint64_t capacity) {
+  const uint64_t n = min((uint64_t)*total, capacity);
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x)
+    dst[p] = src[p].y;
 }
 
 // Entry-capacity guard, run right after the entry scan: when the scene needs
@@ -386,24 +413,41 @@ int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_
   return (int)cudaGetLastError();
 }
 
-int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n_host, const uint32_t* n_dev,
-                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st) {
+template <class IO, class SWAP>
+int radix_passes(IO io, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch, int* result_in_1,
+                 cudaStream_t st, SWAP swap) {
   auto* hist = reinterpret_cast<uint32_t*>(scratch);
-  uint32_t *ki = k0, *vi = v0, *ko = k1, *vo = v1;
   int in1 = 0;
   for (int shift = 0; shift < key_bits; shift += 8) {
     const int nbits = key_bits - shift < 8 ? key_bits - shift : 8;
-    k_rs_upsweep<<<SORT_GRID, RS_THREADS, 0, st>>>(ki, n_host, n_dev, shift, nbits, hist);
+    k_rs_upsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist);
     const int e = launch_scan(hist, nullptr, hist, (uint64_t)RS_BINS * SORT_GRID, nullptr, nullptr, nullptr,
                               hist + RS_BINS * SORT_GRID, st);
     if (e) return e;
-    k_rs_downsweep<<<SORT_GRID, RS_THREADS, 0, st>>>(ki, vi, ko, vo, n_host, n_dev, shift, nbits, hist);
-    uint32_t* t = ki; ki = ko; ko = t;
-    t = vi; vi = vo; vo = t;
+    k_rs_downsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist);
+    swap(io);
     in1 ^= 1;
   }
   *result_in_1 = in1;
   return (int)cudaGetLastError();
+}
+
+int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n_host, const uint32_t* n_dev,
+                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st) {
+  SplitIO io{k0, v0, k1, v1};
+  return radix_passes(io, n_host, n_dev, key_bits, scratch, result_in_1, st, [](SplitIO& x) {
+    SplitIO y{x.kout, x.vout, const_cast<uint32_t*>(x.kin), const_cast<uint32_t*>(x.vin)};
+    x = y;
+  });
+}
+
+int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch,
+                            int* result_in_1, cudaStream_t st) {
+  PairIO io{p0, p1};
+  return radix_passes(io, n_host, n_dev, key_bits, scratch, result_in_1, st, [](PairIO& x) {
+    PairIO y{x.out, const_cast<uint2*>(x.in)};
+    x = y;
+  });
 }
 
 int launch_expand(const ExpandArgs& a, cudaStream_t st) {
@@ -412,10 +456,16 @@ int launch_expand(const ExpandArgs& a, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
-int launch_ranges(const uint32_t* sorted_keys, const unsigned long long* total, uint64_t capacity, uint2* ranges,
+int launch_ranges(const uint2* sorted_pairs, const unsigned long long* total, uint64_t capacity, uint2* ranges,
                   uint32_t num_tiles, cudaStream_t st) {
   cudaMemsetAsync(ranges, 0, sizeof(uint2) * (size_t)num_tiles, st);
-  k_ranges<<<148 * 8, 256, 0, st>>>(sorted_keys, total, capacity, ranges, num_tiles);
+  k_ranges<<<148 * 8, 256, 0, st>>>(sorted_pairs, total, capacity, ranges, num_tiles);
+  return (int)cudaGetLastError();
+}
+
+int launch_pair_values(const uint2* src, uint32_t* dst, const unsigned long long* n, uint64_t capacity,
+                       cudaStream_t st) {
+  k_pair_values<<<148 * 8, 256, 0, st>>>(src, dst, n, capacity);
   return (int)cudaGetLastError();
 }
 
