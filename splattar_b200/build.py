@@ -2,7 +2,8 @@
 
 Each translation unit compiles separately (in parallel); ``gs_project.cu`` is
 built with ``--fmad=false`` so its tile-rect and depth-key arithmetic is free
-of fused multiply-adds and matches an f32 restatement bit for bit. ptxas
+of fused multiply-adds and matches an f32 restatement bit for bit (its adjoint
+is in ``gs_project_bwd.cu``, built normally). ptxas
 resource usage of every kernel is written to ``_build/ptxas_<unit>.txt``.
 """
 from __future__ import annotations
@@ -21,13 +22,14 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 UNITS = {
     "gs_api.cu": [],
     "gs_project.cu": ["--fmad=false"],
+    "gs_project_bwd.cu": [],
     "gs_raster.cu": [],
     "gs_sort.cu": [],
     "gs_loss.cu": [],
     "gs_optim.cu": [],
     "gs_noalloc.cu": [],
 }
-HEADERS = ["gs_common.cuh", "gs_kernels.h"]
+HEADERS = ["gs_common.cuh", "gs_kernels.h", "gs_geom.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "-I", INCLUDE]
 

@@ -492,6 +492,7 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   o.sh_half = prec == 0 ? nullptr : r->sh_half;
   o.sh_half_is_bf16 = prec == 2;
   o.accum_grad_norm = r->accum_norm;
+  o.error_word = r->words + 1;
   TRY_LAUNCH(r, launch_project_bwd_adam(b, o, prec, false, st));
   mark(prof, 8, st);
   return GS_OK;
@@ -597,6 +598,10 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   } while (0)
   cudaGetDevice(&r->device);
   cudaDeviceGetAttribute(&r->num_sms, cudaDevAttrMultiProcessorCount, r->device);
+  {
+    const int pe = prepare_project_kernels();
+    if (pe) return bail((cudaError_t)pe, "kernel shared-memory opt-in");
+  }
   const size_t N = c.capacity, I = r->max_items, E = r->max_entries, P = r->max_pixels;
   ALLOC(r->positions, N); ALLOC(r->scales, N); ALLOC(r->quats, N); ALLOC(r->opacities, N);
   ALLOC(r->sh, N * SH_FLOATS);
@@ -631,7 +636,9 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   ALLOC(r->grad_sh, N * SH_FLOATS);
   ALLOC(r->grad_cam, 16 * (size_t)c.max_views);
   for (int k = 0; k < 5; ++k) {
-    ALLOC(r->raw[k], N * WIDTH[k]); ALLOC(r->mom1[k], N * WIDTH[k]); ALLOC(r->mom2[k], N * WIDTH[k]);
+    // whole multiples of 64 surfels: the fused Adam kernel copies full 32-surfel rows
+    const size_t NP = (N + 63) / 64 * 64;
+    ALLOC(r->raw[k], NP * WIDTH[k]); ALLOC(r->mom1[k], NP * WIDTH[k]); ALLOC(r->mom2[k], NP * WIDTH[k]);
   }
   ALLOC(r->accum_norm, N);
   ALLOC(r->dyn_dev, sizeof(DynParams) / sizeof(float));

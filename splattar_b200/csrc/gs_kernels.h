@@ -68,6 +68,7 @@ struct AdamFusedArgs {
   void* sh_half;          // 16-bit activated SH copy for mixed precision, or null
   int sh_half_is_bf16;
   float* accum_grad_norm; // per-surfel running sum of |dL/dpos| (densify), or null
+  uint32_t* error_word;   // sticky device error word (bounded-wait expiry)
 };
 
 struct RasterArgs {
@@ -95,6 +96,7 @@ int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det);
 
 int launch_project(const ProjectArgs& a, int prec, uint32_t n_views, cudaStream_t st);
 int launch_project_bwd(const ProjectBwdArgs& a, int prec, bool aux, cudaStream_t st);
+int prepare_project_kernels();
 int launch_project_bwd_adam(const ProjectBwdArgs& a, const AdamFusedArgs& opt, int prec, bool aux, cudaStream_t st);
 int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, int grid,
                       cudaStream_t st);

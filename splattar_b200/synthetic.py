@@ -150,6 +150,11 @@ def workload(name: str) -> Workload:
         t = make_surfels(200_000, 1, True, 3, 0.1)
         cams = ring_cameras([(1920, 1080), (1920, 1080)])
         return Workload(name, s, t, cams, "200,000 surfels in 64 clusters, SH deg 3, 2 views 1920x1080")
+    if name == "ring8_250k":  # profiling case with the 8-view rig: a quarter of the surfels
+        s = make_surfels(250_000, 0, True, 3, 0.1)
+        t = make_surfels(250_000, 1, True, 3, 0.1)
+        cams = ring_cameras(RING_RESOLUTIONS)
+        return Workload(name, s, t, cams, "250,000 surfels in 64 clusters, SH deg 3, 8 ring views 640x480..1920x1080")
     if name == "mp4x1080_3m":
         s = make_surfels(3_000_000, 0, True, 3, 0.1)
         t = make_surfels(3_000_000, 1, True, 3, 0.1)
