@@ -406,7 +406,8 @@ gs_status run_loss(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vhost
   int t16 = 0;
   for (uint32_t v = 0; v < nv; ++v) t16 += ((vhost[v].width + 15) / 16) * ((vhost[v].height + 15) / 16);
   a.total_tiles16 = t16;
-  a.img = r->out_color; a.target = r->target; a.coef = r->coef; a.dl_dcolor = r->dl_dcolor;
+  a.img = r->out_color; a.target = r->target; a.coef = r->coef; a.coef_stride = r->max_pixels;
+  a.dl_dcolor = r->dl_dcolor;
   a.loss_sums = sums;
   a.w_l1 = w_l1; a.w_ssim = w_ssim;
   TRY_LAUNCH(r, launch_ssim(a, st));

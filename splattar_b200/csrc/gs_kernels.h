@@ -168,7 +168,8 @@ struct SsimArgs {
   int total_tiles16;          // 16x16 tiles over all views
   const float4* img;
   const float4* target;
-  float* coef;                // 9 floats per pixel scratch
+  float* coef;                // 9 planes of coef_stride floats (scratch)
+  uint64_t coef_stride;       // pixels per plane (the pixel budget)
   float4* dl_dcolor;
   double* loss_sums;          // 2 per view
   float w_l1, w_ssim;

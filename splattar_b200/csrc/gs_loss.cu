@@ -6,10 +6,11 @@
 // two dispatches each, partials, combine) through ~17 image-sized buffers.
 // Here two tiled kernels cover every view of a step:
 //   k_ssim_moments: per 16×16 tile, stage x and y with a 5-pixel halo in
-//     shared memory, blur the five moments (μx, μy, x², y², xy) separably,
-//     form SSIM and the three coefficient maps Cμ, Cx², Cxy per channel
-//     (ssim.wgsl:94-126), and accumulate the per-view loss sums.
-//   k_ssim_grad: stage the nine coefficient maps with a halo, blur them
+//     shared memory, blur the five moments (μx, μy, x², y², xy) of the three
+//     channels separably, form SSIM and the three coefficient maps Cμ, Cx²,
+//     Cxy per channel (ssim.wgsl:94-126), stored as nine planes, and
+//     accumulate the per-view loss sums.
+//   k_ssim_grad: stage the nine coefficient planes with a halo, blur them
 //     (the zero-padded symmetric window is self-adjoint) and combine with the
 //     L1 term into dL/dx (ssim.wgsl:130-143).
 // L = w_l1·mean|x−y| + w_ssim·mean(1−S) over pixels × rgb of each view.
@@ -19,7 +20,22 @@
 namespace gs {
 namespace {
 
+// Output tiles of 16×16 pixels, inputs staged with a 5-pixel halo (26×26).
+// Separable 11-tap blurs run as sliding windows in registers: a horizontal
+// pass where each thread owns one (row, map) and slides along x, then a
+// vertical pass where each thread owns one (column, map) and slides along y,
+// so every staged value is read from shared memory once per pass.
 constexpr int T16 = 16, HALO = 5, EXT = T16 + 2 * HALO;  // 26
+constexpr int TAPS = 2 * HALO + 1;                       // 11
+// Shared-memory strides chosen against bank conflicts: staged planes use an
+// odd row pitch (rows are read by consecutive lanes); horizontal results use
+// an odd row pitch (written by lanes holding consecutive rows) and a plane
+// stride ≡ 16 (mod 32) words (read by two half-warps of different planes);
+// vertical results use a plane stride ≡ 16 (mod 32) for the same reason.
+constexpr int IN_PITCH = EXT + 1;                        // 27
+constexpr int H_ROW = T16 + 1;                           // 17
+constexpr int H_PLANE = 464;                             // ≥ EXT·H_ROW = 442, ≡ 16 mod 32
+constexpr int V_PLANE = T16 * T16 + 16;                  // 272
 
 struct TileLoc {
   int v, x0, y0, W, H;
@@ -45,10 +61,33 @@ __device__ __forceinline__ TileLoc locate(const SsimArgs& a, int t) {
   }
 }
 
+// Slides an 11-tap window along `n_out` outputs: out[o] = Σ_d w[|d−5|]·in(o+d).
+// `in(i)` produces input i (0 ≤ i < n_out + 10), `out(o, value)` consumes.
+template <int N_OUT, class In, class Out>
+__device__ __forceinline__ void slide11(const float (&w)[6], In in, Out out) {
+  float win[TAPS];
+#pragma unroll
+  for (int i = 0; i < TAPS - 1; ++i) win[i] = in(i);
+#pragma unroll
+  for (int o = 0; o < N_OUT; ++o) {
+    win[TAPS - 1] = in(o + TAPS - 1);
+    float acc = w[0] * win[HALO];  // w[k] is the weight at offset ±k
+#pragma unroll
+    for (int d = 0; d < HALO; ++d) acc += w[HALO - d] * (win[d] + win[TAPS - 1 - d]);
+    out(o, acc);
+#pragma unroll
+    for (int i = 0; i < TAPS - 1; ++i) win[i] = win[i + 1];
+  }
+}
+
+// Moments → SSIM, its coefficient maps and the per-view loss sums.
+// Horizontal maps per channel: μx, μy, x², y², xy (15 in all).
 __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
-  __shared__ float s_x[3][EXT][EXT], s_y[3][EXT][EXT];
-  __shared__ float s_h[5][EXT][T16];
+  __shared__ float s_in[6][EXT][IN_PITCH];   // x rgb, y rgb with halo
+  __shared__ float s_h[15 * H_PLANE];        // horizontal results [map][row][col]
   __shared__ double s_red[2][8];
+  float* s_v = &s_in[0][0][0];  // vertical results [map][row][col], reusing s_in after pass 1
+  static_assert(15 * V_PLANE <= 6 * EXT * IN_PITCH, "s_v fits in s_in");
   const int tid = threadIdx.x;
   const TileLoc L = locate(a, blockIdx.x);
   for (int k = tid; k < EXT * EXT; k += 256) {
@@ -60,53 +99,74 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
       xv = a.img[p];
       yv = a.target[p];
     }
-    s_x[0][ly][lx] = xv.x; s_x[1][ly][lx] = xv.y; s_x[2][ly][lx] = xv.z;
-    s_y[0][ly][lx] = yv.x; s_y[1][ly][lx] = yv.y; s_y[2][ly][lx] = yv.z;
+    s_in[0][ly][lx] = xv.x; s_in[1][ly][lx] = xv.y; s_in[2][ly][lx] = xv.z;
+    s_in[3][ly][lx] = yv.x; s_in[4][ly][lx] = yv.y; s_in[5][ly][lx] = yv.z;
   }
+  float w[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) w[k] = a.w[k];
+  __syncthreads();
+  // Horizontal: item = (map mc, row r); map mc = 5·channel + moment.
+  for (int it = tid; it < 15 * EXT; it += 256) {
+    const int mc = it / EXT, r = it - mc * EXT;
+    const int ch = mc / 5, m = mc - ch * 5;
+    const float* X = &s_in[ch][r][0];
+    const float* Y = &s_in[3 + ch][r][0];
+    float* O = s_h + mc * H_PLANE + r * H_ROW;
+    auto put = [&](int o, float v) { O[o] = v; };
+    switch (m) {
+      case 0: slide11<T16>(w, [&](int i) { return X[i]; }, put); break;
+      case 1: slide11<T16>(w, [&](int i) { return Y[i]; }, put); break;
+      case 2: slide11<T16>(w, [&](int i) { const float x = X[i]; return x * x; }, put); break;
+      case 3: slide11<T16>(w, [&](int i) { const float y = Y[i]; return y * y; }, put); break;
+      default: slide11<T16>(w, [&](int i) { return X[i] * Y[i]; }, put); break;
+    }
+  }
+  // L1 of this thread's pixel, read before s_in is reused.
   const int ox = tid & 15, oy = tid >> 4;
   const int gx = L.x0 + ox, gy = L.y0 + oy;
   const bool inside = gx < L.W && gy < L.H;
-  const long long pix = L.pix_base + (long long)gy * L.W + gx;
-  const float C1 = 1e-4f, C2 = 9e-4f;
-  float l1 = 0.f, ss = 0.f;
+  float l1 = 0.f;
+  float xs[3], ys[3];
+#pragma unroll
   for (int ch = 0; ch < 3; ++ch) {
-    __syncthreads();
-    for (int k = tid; k < EXT * T16; k += 256) {
-      const int r = k / T16, c = k % T16;
-      float m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0;
+    xs[ch] = s_in[ch][oy + HALO][ox + HALO];
+    ys[ch] = s_in[3 + ch][oy + HALO][ox + HALO];
+    if (inside) l1 += fabsf(xs[ch] - ys[ch]);
+  }
+  __syncthreads();
+  // Vertical: item = (map mc, column c).
+  if (tid < 15 * T16) {
+    const int mc = tid / T16, c = tid - mc * T16;
+    const float* I = s_h + mc * H_PLANE + c;
+    float* O = s_v + mc * V_PLANE + c;
+    slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+  }
+  __syncthreads();
+  float ss = 0.f;
+  if (inside) {
+    const long long pix = L.pix_base + (long long)gy * L.W + gx;
+    const float inv_n3 = 1.0f / (3.0f * (float)L.W * (float)L.H);
+    const float C1 = 1e-4f, C2 = 9e-4f;
+    const float dw = -a.w_ssim * inv_n3;
 #pragma unroll
-      for (int d = -HALO; d <= HALO; ++d) {
-        const float w = a.w[d < 0 ? -d : d];
-        const float xv = s_x[ch][r][c + HALO + d], yv = s_y[ch][r][c + HALO + d];
-        m0 += w * xv; m1 += w * yv; m2 += w * xv * xv; m3 += w * yv * yv; m4 += w * xv * yv;
-      }
-      s_h[0][r][c] = m0; s_h[1][r][c] = m1; s_h[2][r][c] = m2; s_h[3][r][c] = m3; s_h[4][r][c] = m4;
-    }
-    __syncthreads();
-    float mu_x = 0, mu_y = 0, bx2 = 0, by2 = 0, bxy = 0;
-#pragma unroll
-    for (int d = -HALO; d <= HALO; ++d) {
-      const float w = a.w[d < 0 ? -d : d];
-      const int r = oy + HALO + d;
-      mu_x += w * s_h[0][r][ox]; mu_y += w * s_h[1][r][ox]; bx2 += w * s_h[2][r][ox];
-      by2 += w * s_h[3][r][ox]; bxy += w * s_h[4][r][ox];
-    }
-    if (inside) {
-      const float inv_n3 = 1.0f / (3.0f * (float)L.W * (float)L.H);
+    for (int ch = 0; ch < 3; ++ch) {
+      const float* V = s_v + oy * T16 + ox;
+      const float mu_x = V[(5 * ch) * V_PLANE], mu_y = V[(5 * ch + 1) * V_PLANE];
+      const float bx2 = V[(5 * ch + 2) * V_PLANE], by2 = V[(5 * ch + 3) * V_PLANE], bxy = V[(5 * ch + 4) * V_PLANE];
       const float sx2 = bx2 - mu_x * mu_x, sy2 = by2 - mu_y * mu_y, sxy = bxy - mu_x * mu_y;
       const float p = mu_x * mu_x + mu_y * mu_y + C1;
       const float q = sx2 + sy2 + C2;
       const float l = (2.0f * mu_x * mu_y + C1) / p;
       const float cs = (2.0f * sxy + C2) / q;
       const float S = l * cs;
-      const float dw = -a.w_ssim * inv_n3;
       const float ds_dmux = cs * (2.0f * mu_y - 2.0f * mu_x * l) / p + l * (-2.0f * mu_y + 2.0f * mu_x * cs) / q;
       const float ds_dbx2 = -l * cs / q;
       const float ds_dbxy = 2.0f * l / q;
-      float* cf = a.coef + (size_t)pix * 9 + ch * 3;
-      cf[0] = ds_dmux * dw; cf[1] = ds_dbx2 * dw; cf[2] = ds_dbxy * dw;
+      a.coef[(size_t)(3 * ch) * a.coef_stride + pix] = ds_dmux * dw;
+      a.coef[(size_t)(3 * ch + 1) * a.coef_stride + pix] = ds_dbx2 * dw;
+      a.coef[(size_t)(3 * ch + 2) * a.coef_stride + pix] = ds_dbxy * dw;
       ss += S;
-      l1 += fabsf(s_x[ch][oy + HALO][ox + HALO] - s_y[ch][oy + HALO][ox + HALO]);
     }
   }
   // Per-view loss sums: warp, then block, then one double atomic each.
@@ -115,58 +175,50 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
   __syncthreads();
   if (tid == 0) {
     double t0 = 0, t1 = 0;
-    for (int w = 0; w < 8; ++w) { t0 += s_red[0][w]; t1 += s_red[1][w]; }
+    for (int k = 0; k < 8; ++k) { t0 += s_red[0][k]; t1 += s_red[1][k]; }
     atomicAdd(a.loss_sums + 2 * L.v, t0);
     atomicAdd(a.loss_sums + 2 * L.v + 1, t1);
   }
 }
 
+// Blur of the nine coefficient maps (the zero-padded symmetric window is
+// self-adjoint) combined with the L1 term into dL/dx.
 __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
-  __shared__ float s_c[9][EXT][EXT];
-  __shared__ float s_h[9][EXT][T16];
+  __shared__ float s_c[9][EXT][IN_PITCH];
+  __shared__ float s_h[9 * H_PLANE];
+  float* s_v = &s_c[0][0][0];  // vertical results [map][row][col], reusing s_c after pass 1
+  static_assert(9 * V_PLANE <= 9 * EXT * IN_PITCH, "s_v fits in s_c");
   const int tid = threadIdx.x;
   const TileLoc L = locate(a, blockIdx.x);
   for (int k = tid; k < EXT * EXT; k += 256) {
     const int ly = k / EXT, lx = k % EXT;
     const int gx = L.x0 + lx - HALO, gy = L.y0 + ly - HALO;
     const bool in = gx >= 0 && gy >= 0 && gx < L.W && gy < L.H;
-    if (in) {
-      const float* cf = a.coef + (size_t)(L.pix_base + (long long)gy * L.W + gx) * 9;
+    const size_t p = in ? (size_t)(L.pix_base + (long long)gy * L.W + gx) : 0;
 #pragma unroll
-      for (int m = 0; m < 9; ++m) s_c[m][ly][lx] = cf[m];
-    } else {
+    for (int m = 0; m < 9; ++m) s_c[m][ly][lx] = in ? __ldg(a.coef + (size_t)m * a.coef_stride + p) : 0.f;
+  }
+  float w[6];
 #pragma unroll
-      for (int m = 0; m < 9; ++m) s_c[m][ly][lx] = 0.f;
-    }
+  for (int k = 0; k < 6; ++k) w[k] = a.w[k];
+  __syncthreads();
+  for (int it = tid; it < 9 * EXT; it += 256) {
+    const int m = it / EXT, r = it - m * EXT;
+    const float* X = &s_c[m][r][0];
+    float* O = s_h + m * H_PLANE + r * H_ROW;
+    slide11<T16>(w, [&](int i) { return X[i]; }, [&](int o, float v) { O[o] = v; });
   }
   __syncthreads();
-  for (int k = tid; k < EXT * T16; k += 256) {
-    const int r = k / T16, c = k % T16;
-    float acc[9];
-#pragma unroll
-    for (int m = 0; m < 9; ++m) acc[m] = 0.f;
-#pragma unroll
-    for (int d = -HALO; d <= HALO; ++d) {
-      const float w = a.w[d < 0 ? -d : d];
-#pragma unroll
-      for (int m = 0; m < 9; ++m) acc[m] += w * s_c[m][r][c + HALO + d];
-    }
-#pragma unroll
-    for (int m = 0; m < 9; ++m) s_h[m][r][c] = acc[m];
+  if (tid < 9 * T16) {
+    const int m = tid / T16, c = tid - m * T16;
+    const float* I = s_h + m * H_PLANE + c;
+    float* O = s_v + m * V_PLANE + c;
+    slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
   }
   __syncthreads();
   const int ox = tid & 15, oy = tid >> 4;
   const int gx = L.x0 + ox, gy = L.y0 + oy;
   if (gx >= L.W || gy >= L.H) return;
-  float acc[9];
-#pragma unroll
-  for (int m = 0; m < 9; ++m) acc[m] = 0.f;
-#pragma unroll
-  for (int d = -HALO; d <= HALO; ++d) {
-    const float w = a.w[d < 0 ? -d : d];
-#pragma unroll
-    for (int m = 0; m < 9; ++m) acc[m] += w * s_h[m][oy + HALO + d][ox];
-  }
   const long long pix = L.pix_base + (long long)gy * L.W + gx;
   const float4 x = a.img[pix], y = a.target[pix];
   const float k1 = a.w_l1 / (3.0f * (float)L.W * (float)L.H);
@@ -176,7 +228,9 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
   for (int ch = 0; ch < 3; ++ch) {
     const float diff = xs[ch] - ys[ch];
     const float sg = diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f);
-    out[ch] = sg * k1 + acc[3 * ch] + 2.0f * xs[ch] * acc[3 * ch + 1] + ys[ch] * acc[3 * ch + 2];
+    const float* V = s_v + oy * T16 + ox;
+    out[ch] = sg * k1 + V[(3 * ch) * V_PLANE] + 2.0f * xs[ch] * V[(3 * ch + 1) * V_PLANE] +
+              ys[ch] * V[(3 * ch + 2) * V_PLANE];
   }
   a.dl_dcolor[pix] = make_float4(out[0], out[1], out[2], 0.f);
 }
