@@ -37,7 +37,7 @@ METRIC = "fwd+bwd+Adam steps/s, 1M surfels 1080p: chosen vs plain form; HBM roof
 FALLBACK_HBM_GBS = 6650.0
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=10)
@@ -48,7 +48,12 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU-baseline sample time")
-    return p.parse_args()
+    p.add_argument("--densify-every", type=int, default=0,
+                   help="densify/prune cycle: clone/prune every K timed steps (grad 2e-4, opacity 0.005)")
+    p.add_argument("--deterministic", action="store_true", help="ordered gradient reduction (densify cycle)")
+    p.add_argument("--capacity-factor", type=float, default=1.25, help="densify cycle: capacity / initial surfels")
+    p.add_argument("--entries-per-item", type=float, default=12.0, help="densify cycle: tile-entry budget per item")
+    return p.parse_args(argv)
 
 
 def dist_env():
@@ -280,6 +285,69 @@ def run_ours(args, ws, rank, local):
     return result
 
 
+def run_densify_cycle(args, ws, rank, local):
+    """Training with the densify/prune cycle: `steps` chosen-form steps, a
+    densify/prune compaction after every `densify_every` of them (clone where
+    the mean |dL/dpos| exceeds 2e-4, prune activated opacity below 0.005),
+    all inside the timed region (the compaction synchronises with the host to
+    learn the new surfel count)."""
+    import torch
+    torch.cuda.set_device(local)
+    from splattar_b200 import Rasterizer, StepSettings
+    from splattar_b200.rasterizer import AdamSettings
+    from splattar_b200.synthetic import workload
+
+    wl = workload(args.workload)
+    cams = wl.cameras
+    n, nv, P = wl.surfels.n, len(cams), wl.pixels
+    cap = int(n * args.capacity_factor)
+    max_entries = int(min(4.2e9, args.entries_per_item * cap * nv))
+    free0, total = torch.cuda.mem_get_info()
+    rast = Rasterizer(cap, 0, 0, max_entries, max_views=nv, max_pixels=P, precision=args.precision, color_only=True,
+                      deterministic=args.deterministic, tight=True)
+    free1, _ = torch.cuda.mem_get_info()
+    rast.upload_scene(wl.target_surfels.scene_input())
+    rast.forward(cams, n)
+    rast.check()
+    rast.write("target", rast.read("out_color", 4 * P))
+    rast.upload_scene(wl.surfels.scene_input())
+    rast.optimizer_init(n)
+    step = StepSettings(0.8, 0.2, AdamSettings(eps=1e-15), "chosen")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    for _ in range(args.warmup):
+        rast.train_step(cams, n, step, sp)
+    rast.check(sp)
+    counts = [n]
+    entries = []
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        rast.train_step(cams, n, step, sp)
+        if args.densify_every and (k + 1) % args.densify_every == 0:
+            entries.append(rast.entry_count())
+            n = rast.densify_prune(2e-4, 0.005, n, sp)
+            counts.append(n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    rast.check(sp)
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, ws)
+    rast.close()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": METRIC, "value": round(aggregate_steps_per_s(ms, ws), 4), "unit": "steps/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "views": nv, "pixels_per_step": P, "capacity": cap,
+                   "densify_every": args.densify_every, "mode": "deterministic" if args.deterministic else "atomic",
+                   "surfels_after_each_densify": counts, "tile_entries_before_each_densify": entries,
+                   "device_bytes_of_handle": int(free0 - free1), "device_bytes_total": int(total),
+                   "note": "densify/prune cycle inside the timed region"},
+    }))
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -291,6 +359,13 @@ def main():
         import datetime
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.densify_every or args.deterministic:
+        run_densify_cycle(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     r = run_ours(args, ws, rank, local)
     if ws > 1:
         import torch.distributed as dist

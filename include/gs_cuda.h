@@ -132,7 +132,19 @@ typedef enum {
   GS_BUF_RAW_SH = 26,
   GS_BUF_RECTS = 27,      /* uint4 tile rect per item (x0,y0,x1,y1 inclusive; culled or off-screen = 1,1,0,0) */
   GS_BUF_DEPTH_KEYS = 28, /* u32 per item after the depth sort: f32 bits of the centre depth, ascending */
-  GS_BUF_DEPTH_ORDER = 29 /* u32 per item after the depth sort: item index (stable, ties by index) */
+  GS_BUF_DEPTH_ORDER = 29,/* u32 per item after the depth sort: item index (stable, ties by index) */
+  GS_BUF_GRAD_NORM_SUM = 30,/* float per surfel: sum over optimizer steps since the last densify (or init) of
+                               |dL/dpos|, the densify statistic */
+  GS_BUF_M_POS = 31,      /* Adam first moments (Optimizer ParamClass::m), layout of the raw buffers */
+  GS_BUF_M_SCALES = 32,
+  GS_BUF_M_QUAT = 33,
+  GS_BUF_M_OPACITY = 34,
+  GS_BUF_M_SH = 35,
+  GS_BUF_V_POS = 36,      /* Adam second moments (Optimizer ParamClass::v) */
+  GS_BUF_V_SCALES = 37,
+  GS_BUF_V_QUAT = 38,
+  GS_BUF_V_OPACITY = 39,
+  GS_BUF_V_SH = 40
 } gs_buffer_id;
 
 typedef struct gs_rasterizer gs_rasterizer;

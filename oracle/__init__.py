@@ -303,3 +303,30 @@ def cpu_step_timed(scene: Scene, cam: Camera, target_rgba, tile=16, tile_stride=
     s, c = scene.c(), cam.c()
     lib().orc_cpu_step_timed(C.byref(s), C.byref(c), tile, tile_stride, threads, _p(tgt), _p(times))
     return times
+
+
+def densify(arrays: dict, widths: dict, moments: set, grad_norm_sum, steps: int, opacity_act,
+            grad_threshold: float, opacity_threshold: float, capacity: int):
+    """Clone/prune compaction restated in numpy (the reference has no such
+    pass; it relocates at a fixed budget, first_attempt/crates/gs-train/src/
+    trainer.rs:1558-1689). A surfel is kept when its activated opacity is at
+    least `opacity_threshold`; a kept surfel is cloned when its mean
+    |dL/dpos| over the accumulated steps exceeds `grad_threshold`. Survivors
+    keep their order, clones follow in the order of their sources, and clones
+    past `capacity` are dropped. Clones copy every array except the moment
+    arrays (names in `moments`), which start at zero. Returns (new arrays,
+    new count)."""
+    n = len(opacity_act)
+    keep = np.asarray(opacity_act, np.float32) >= np.float32(opacity_threshold)
+    inv = np.float32(1.0 / steps) if steps else np.float32(0.0)
+    mean = np.asarray(grad_norm_sum, np.float32) * inv
+    clone = keep & (mean > np.float32(grad_threshold))
+    kept_idx = np.nonzero(keep)[0]
+    clone_idx = np.nonzero(clone)[0][:max(0, capacity - len(kept_idx))]
+    out = {}
+    for name, a in arrays.items():
+        w = widths[name]
+        rows = np.asarray(a).reshape(-1, w)[:n]
+        cl = np.zeros((len(clone_idx), w), rows.dtype) if name in moments else rows[clone_idx]
+        out[name] = np.concatenate([rows[kept_idx], cl], axis=0)
+    return out, len(kept_idx) + len(clone_idx)

@@ -27,6 +27,8 @@ BUF = {
     "grad_quat": 13, "grad_opacity": 14, "grad_sh": 15, "grad_cam": 16, "target": 17, "ranges": 18,
     "sorted_items": 19, "entry_count": 20, "loss": 21, "raw_pos": 22, "raw_scales": 23, "raw_quat": 24,
     "raw_opacity": 25, "raw_sh": 26, "rects": 27, "depth_keys": 28, "depth_order": 29,
+    "grad_norm_sum": 30, "m_pos": 31, "m_scales": 32, "m_quat": 33, "m_opacity": 34, "m_sh": 35, "v_pos": 36,
+    "v_scales": 37, "v_quat": 38, "v_opacity": 39, "v_sh": 40,
 }
 
 

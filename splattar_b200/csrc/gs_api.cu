@@ -451,6 +451,10 @@ void bias_corrections(float b1, float b2, uint32_t t, float& bc1, float& bc2) {
 }
 
 gs_status adam_plain(gs_rasterizer* r, const gs_adam_config* c, uint32_t n, cudaStream_t st) {
+  // Densify statistic: running sum of |dL/dpos| per surfel (the fused chosen
+  // form adds it inside its kernel).
+  TRY_LAUNCH(r, launch_accum_norm(r->grad_pos, r->accum_norm, n, st));
+  r->accum_steps += 1;
   r->t += 1;
   float bc1, bc2;
   bias_corrections(c->beta1, c->beta2, r->t, bc1, bc2);
@@ -521,7 +525,6 @@ gs_status plain_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_co
     if (s) return s;
     mark(prof, 8, st);
   }
-  r->accum_steps += 1;
   s = adam_plain(r, &cfg->adam, n, st);
   mark(prof, 8, st);
   return s;
@@ -778,6 +781,17 @@ static gs_status buffer_info(gs_rasterizer* r, gs_buffer_id id, void** p, size_t
     case GS_BUF_RECTS: *p = r->rects; *bytes = 16 * I; break;
     case GS_BUF_DEPTH_KEYS: *p = r->item_keys[0]; *bytes = 4 * I; break;
     case GS_BUF_DEPTH_ORDER: *p = r->item_vals[0]; *bytes = 4 * I; break;
+    case GS_BUF_GRAD_NORM_SUM: *p = r->accum_norm; *bytes = 4 * N; break;
+    case GS_BUF_M_POS: case GS_BUF_M_SCALES: case GS_BUF_M_QUAT: case GS_BUF_M_OPACITY: case GS_BUF_M_SH: {
+      const int k = (int)id - (int)GS_BUF_M_POS;
+      *p = r->mom1[k]; *bytes = 4 * N * WIDTH[k];
+      break;
+    }
+    case GS_BUF_V_POS: case GS_BUF_V_SCALES: case GS_BUF_V_QUAT: case GS_BUF_V_OPACITY: case GS_BUF_V_SH: {
+      const int k = (int)id - (int)GS_BUF_V_POS;
+      *p = r->mom2[k]; *bytes = 4 * N * WIDTH[k];
+      break;
+    }
     default: return fail(r, GS_ERR_INVALID_ARG, "unknown buffer id");
   }
   return GS_OK;

@@ -179,6 +179,7 @@ int launch_ssim(const SsimArgs& a, cudaStream_t st);
 
 int launch_adam_grad(const AdamClass& c, const float* grad, uint64_t n, int activation, float beta1, float beta2,
                      float eps, float bc1_inv, float bc2_inv, cudaStream_t st);
+int launch_accum_norm(const float4* grad_pos, float* accum, uint32_t n, cudaStream_t st);
 int launch_activate_init(const AdamClass& c, uint64_t n, int activation, cudaStream_t st);
 int launch_to_half(const float* src, void* dst, uint64_t n, bool bf16, cudaStream_t st);
 

@@ -126,7 +126,20 @@ __global__ void k_densify_count(const uint32_t* n_keep, const uint32_t* n_clone,
   *n_out = t > capacity ? capacity : (uint32_t)t;
 }
 
+__global__ void __launch_bounds__(256) k_accum_norm(const float4* grad_pos, float* accum, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 g = grad_pos[i];
+    accum[i] += sqrtf(g.x * g.x + g.y * g.y + g.z * g.z);
+  }
+}
+
 }  // namespace
+
+int launch_accum_norm(const float4* grad_pos, float* accum, uint32_t n, cudaStream_t st) {
+  if (n == 0) return 0;
+  k_accum_norm<<<grid_of(n), 256, 0, st>>>(grad_pos, accum, n);
+  return (int)cudaGetLastError();
+}
 
 int launch_adam_grad(const AdamClass& c, const float* grad, uint64_t n, int activation, float beta1, float beta2,
                      float eps, float bc1_inv, float bc2_inv, cudaStream_t st) {

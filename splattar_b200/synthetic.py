@@ -160,6 +160,13 @@ def workload(name: str) -> Workload:
         t = make_surfels(3_000_000, 1, True, 3, 0.1)
         cams = ring_cameras([(1920, 1080)] * 4)
         return Workload(name, s, t, cams, "3,000,000 surfels in 64 clusters, SH deg 3, 4 views 1920x1080")
+    if name == "full16_3m":  # the 16-view rig at half the surfels (deterministic-mode memory)
+        s = make_surfels(3_000_000, 0, True, 3, 0.1)
+        t = make_surfels(3_000_000, 1, True, 3, 0.1)
+        rng = np.random.default_rng(7)
+        res = [RING_RESOLUTIONS[i] for i in rng.integers(0, len(RING_RESOLUTIONS), 16)]
+        cams = ring_cameras(res)
+        return Workload(name, s, t, cams, "3,000,000 surfels in 64 clusters, SH deg 3, 16 views per step")
     if name == "full16_6m":
         s = make_surfels(6_000_000, 0, True, 3, 0.1)
         t = make_surfels(6_000_000, 1, True, 3, 0.1)

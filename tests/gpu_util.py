@@ -57,10 +57,17 @@ def backward(rast, scene, dl_dcolor4, dl_dnormal4=None):
 
 
 class GradCheck:
-    """raster_parity.rs:83-114: err ≤ 1e-5 + rel_tol·max(|gpu|, |cpu|)."""
+    """raster_parity.rs:83-114: err ≤ 1e-5 + rel_tol·max(|gpu|, |cpu|).
 
-    def __init__(self, rel_tol):
+    With `outliers` > 0, up to that fraction of the entries may exceed the
+    tolerance, none by more than `outlier_rel` of the array's largest
+    gradient (f32 against f64 on scenes dense enough to hold near-grazing
+    surfels, whose ray-branch gradients scale with 1/det and amplify f32
+    rounding)."""
+
+    def __init__(self, rel_tol, outliers=0.0, outlier_rel=2e-2):
         self.rel_tol = rel_tol
+        self.outliers, self.outlier_rel = outliers, outlier_rel
         self.worst, self.label = 0.0, ""
 
     def check(self, label, gpu, cpu):
@@ -73,5 +80,12 @@ class GradCheck:
         if sel.any() and rel[sel].max() > self.worst:
             self.worst, self.label = float(rel[sel].max()), f"{label}[{int(np.argmax(np.where(sel, rel, 0)))}]"
         bad = err > 1e-5 + self.rel_tol * denom
+        if self.outliers > 0:
+            far = err > 1e-5 + self.outlier_rel * float(np.abs(cpu).max(initial=0.0))
+            assert not far.any(), (f"{label}: {int(far.sum())} beyond {self.outlier_rel}, first at "
+                                   f"{int(np.argmax(far))}: gpu {gpu[far][0]:.6e} vs cpu {cpu[far][0]:.6e}")
+            assert bad.sum() <= self.outliers * bad.size, (f"{label}: {int(bad.sum())} of {bad.size} beyond "
+                                                           f"{self.rel_tol}")
+            return
         assert not bad.any(), (f"{label}: {int(bad.sum())} mismatches, first at {int(np.argmax(bad))}: gpu "
                                f"{gpu[bad][0]:.6e} vs cpu {cpu[bad][0]:.6e}")
