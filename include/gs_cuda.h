@@ -38,7 +38,9 @@ typedef enum {
   GS_ERR_CUDA = 3,           /* a CUDA runtime call failed */
   GS_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait expired */
   GS_ERR_NONFINITE = 5,
-  GS_ERR_STATE = 6           /* call out of order (e.g. backward before forward) */
+  GS_ERR_STATE = 6,          /* call out of order (e.g. backward before forward) */
+  GS_ERR_IO = 7,             /* a file could not be opened, read or written */
+  GS_ERR_FORMAT = 8          /* a file is not in a supported format (text in gs_last_error(NULL)) */
 } gs_status;
 
 /* Storage precision of the renderer-facing copies (projected records, SH). */
@@ -304,6 +306,31 @@ gs_status gs_exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, u
  * streams, or different host threads) race and corrupt each other's
  * results. Stream-ordered, does not synchronise. */
 gs_status gs_radix_sort_pairs_noalloc(uint32_t* keys, uint32_t* vals, uint64_t n, uint32_t key_bits, void* stream);
+
+/* ---- Surfel PLY files (first_attempt/crates/gs-io/src/ply) ---------------
+ * The 3DGS binary little-endian layout: x y z | f_dc_0..2 | f_rest_0..44
+ * (channel-major) | opacity (logit) | scale_0..2 (log) | rot_0..3 (w first).
+ * gs_ply_write is write_3dgs_ply (ply/writer.rs): activated inputs
+ * (positions 4 floats per surfel, scales 2, quats xyzw, opacities, SH 48
+ * coefficient-major); the third log-scale is written as -10 (flattened).
+ * gs_ply_info / gs_ply_read are load_ply for splat files (ply/reader.rs):
+ * properties located by name, f_rest counts 0/9/24/45, activated outputs
+ * (positions 3, scales 3 = exp, quats xyzw normalised or identity when
+ * degenerate, opacities = sigmoid, SH sh_coeffs*3 coefficient-major).
+ * Errors: GS_ERR_IO (open/read/write), GS_ERR_FORMAT (not a ply, not
+ * binary_little_endian 1.0, unknown layout, non-float property, wrong f_rest
+ * count, payload shorter than the header's count, more surfels than
+ * capacity); the text is in gs_last_error(NULL). Host-only. */
+gs_status gs_ply_write(const char* path, uint32_t count, const float* positions4, const float* scales2,
+                       const float* quats4, const float* opacities, const float* sh48);
+gs_status gs_ply_info(const char* path, uint32_t* count, uint32_t* sh_coeffs);
+gs_status gs_ply_read(const char* path, uint32_t capacity, float* positions3, float* scales3, float* quats4,
+                      float* opacities, float* sh, uint32_t* count);
+/* The handle's activated surfels [0, num_surfels) to a PLY file (blocking). */
+gs_status gs_rasterizer_save_ply(gs_rasterizer* r, const char* path, uint32_t num_surfels, void* stream);
+/* A splat PLY file into the handle (gs_rasterizer_upload_scene of its
+ * activated values; the third scale is dropped). *num_surfels = its count. */
+gs_status gs_rasterizer_load_ply(gs_rasterizer* r, const char* path, uint32_t* num_surfels, void* stream);
 
 /* Camera-to-world rotation (column-major 3x3) exactly as the forward computes
  * it from gs_camera.quat (glam Mat3::from_quat of the normalised quaternion,

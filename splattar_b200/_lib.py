@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libgs_cuda.so")
 
 GS_OK = 0
 STATUS = {0: "GS_OK", 1: "GS_ERR_INVALID_ARG", 2: "GS_ERR_CAPACITY", 3: "GS_ERR_CUDA", 4: "GS_ERR_DEVICE_TIMEOUT",
-          5: "GS_ERR_NONFINITE", 6: "GS_ERR_STATE"}
+          5: "GS_ERR_NONFINITE", 6: "GS_ERR_STATE", 7: "GS_ERR_IO", 8: "GS_ERR_FORMAT"}
 
 PREC = {"f32": 0, "f16": 1, "bf16": 2}
 FLAG_DETERMINISTIC = 1
@@ -112,6 +112,11 @@ def lib():
         "gs_radix_sort_pairs_noalloc": [vp, vp, u64, u32, vp],
         "gs_exclusive_scan_u32": [vp, vp, u64, vp, vp],
         "gs_camera_rotation": [C.POINTER(Camera), C.POINTER(C.c_float)],
+        "gs_ply_write": [C.c_char_p, u32, vp, vp, vp, vp, vp],
+        "gs_ply_info": [C.c_char_p, C.POINTER(u32), C.POINTER(u32)],
+        "gs_ply_read": [C.c_char_p, u32, vp, vp, vp, vp, vp, C.POINTER(u32)],
+        "gs_rasterizer_save_ply": [vp, C.c_char_p, u32, vp],
+        "gs_rasterizer_load_ply": [vp, C.c_char_p, C.POINTER(u32), vp],
         "gs_shutdown": [],
     }
     for name, args in sigs.items():
@@ -146,4 +151,5 @@ def exported_symbols() -> list[str]:
         "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_set_launch_shapes", "gs_binner_create",
         "gs_binner_destroy", "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_radix_sort_pairs_noalloc",
         "gs_exclusive_scan_u32",
-        "gs_camera_rotation", "gs_shutdown"]
+        "gs_camera_rotation", "gs_shutdown", "gs_ply_write", "gs_ply_info", "gs_ply_read", "gs_rasterizer_save_ply",
+        "gs_rasterizer_load_ply"]

@@ -28,6 +28,7 @@ UNITS = {
     "gs_loss.cu": [],
     "gs_optim.cu": [],
     "gs_noalloc.cu": [],
+    "gs_ply.cpp": [],
 }
 HEADERS = ["gs_common.cuh", "gs_kernels.h", "gs_geom.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,12 +49,12 @@ def _deps_mtime() -> float:
 
 def _compile(unit: str, extra: list[str], force: bool) -> str:
     src = os.path.join(CSRC, unit)
-    obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+    obj = os.path.join(BUILD, os.path.splitext(unit)[0] + ".o")
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), _deps_mtime()):
         return obj
     cmd = [_nvcc(), *FLAGS, *extra, "-c", src, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
-    with open(os.path.join(BUILD, "ptxas_" + unit.replace(".cu", ".txt")), "w") as f:
+    with open(os.path.join(BUILD, "ptxas_" + os.path.splitext(unit)[0] + ".txt"), "w") as f:
         f.write(" ".join(cmd) + "\n" + res.stdout + res.stderr)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed for {unit}:\n{res.stderr[-6000:]}")

@@ -1129,6 +1129,42 @@ gs_status gs_densify_prune(gs_rasterizer* r, const gs_densify_config* c, uint32_
   return GS_OK;
 }
 
+// ------------------------------------------------------------------- PLY
+gs_status gs_rasterizer_save_ply(gs_rasterizer* r, const char* path, uint32_t n, void* stream) {
+  if (!r || !path) return GS_ERR_INVALID_ARG;
+  if (n > r->cap) return fail(r, GS_ERR_CAPACITY, "num_surfels exceeds capacity");
+  cudaStream_t st = S(stream);
+  std::vector<float> pos(4 * (size_t)n), sc(2 * (size_t)n), q(4 * (size_t)n), op(n), sh(SH_FLOATS * (size_t)n);
+  TRY_CUDA(r, cudaMemcpyAsync(pos.data(), r->positions, pos.size() * 4, cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaMemcpyAsync(sc.data(), r->scales, sc.size() * 4, cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaMemcpyAsync(q.data(), r->quats, q.size() * 4, cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaMemcpyAsync(op.data(), r->opacities, op.size() * 4, cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaMemcpyAsync(sh.data(), r->sh, sh.size() * 4, cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaStreamSynchronize(st));
+  const gs_status s = gs_ply_write(path, n, pos.data(), sc.data(), q.data(), op.data(), sh.data());
+  if (s) r->err = g_last_error;
+  return s;
+}
+
+gs_status gs_rasterizer_load_ply(gs_rasterizer* r, const char* path, uint32_t* n_out, void* stream) {
+  if (!r || !path || !n_out) return GS_ERR_INVALID_ARG;
+  uint32_t n = 0, nc = 0;
+  gs_status s = gs_ply_info(path, &n, &nc);
+  if (!s && n > r->cap) s = fail(nullptr, GS_ERR_CAPACITY, "ply holds more surfels than the capacity");
+  std::vector<float> pos3(3 * (size_t)n), sc3(3 * (size_t)n), q(4 * (size_t)n), op(n), sh(3 * (size_t)nc * n);
+  if (!s) s = gs_ply_read(path, r->cap, pos3.data(), sc3.data(), q.data(), op.data(), sh.data(), &n);
+  if (s) {
+    r->err = g_last_error;
+    return s;
+  }
+  std::vector<float> sc2(2 * (size_t)n);
+  for (size_t i = 0; i < n; ++i) { sc2[2 * i] = sc3[3 * i]; sc2[2 * i + 1] = sc3[3 * i + 1]; }
+  gs_scene_input in{pos3.data(), sc2.data(), q.data(), op.data(), sh.data(), nc, n};
+  s = gs_rasterizer_upload_scene(r, &in, stream);
+  if (!s) *n_out = n;
+  return s;
+}
+
 // ---------------------------------------------------------------- binner
 gs_status gs_binner_create(uint32_t max_items, uint64_t max_entries, uint32_t num_tiles, gs_binner** out) {
   if (!out || max_items == 0 || num_tiles == 0 || max_entries >= 0xffffffffull)

@@ -12,6 +12,7 @@ Where the reference panics on a violated assert, these raise ``GsError``.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -231,6 +232,16 @@ class Rasterizer:
         arr = (C.c_uint32 * 4)(fwd_batch, fwd_pixels_per_thread, bwd_batch, bwd_pixels_per_thread)
         self._chk(lib().gs_set_launch_shapes(self._h, arr))
 
+    def save_ply(self, path: str, num_surfels: int, stream: int = 0):
+        """The activated surfels [0, num_surfels) to a 3DGS-layout PLY file."""
+        self._chk(lib().gs_rasterizer_save_ply(self._h, os.fsencode(path), num_surfels, stream))
+
+    def load_ply(self, path: str, stream: int = 0) -> int:
+        """A splat PLY file into the handle; returns its surfel count."""
+        n = C.c_uint32()
+        self._chk(lib().gs_rasterizer_load_ply(self._h, os.fsencode(path), C.byref(n), stream))
+        return n.value
+
     def densify_prune(self, grad_threshold: float, opacity_threshold: float, num_surfels: int,
                       stream: int = 0) -> int:
         cfg = DensifyConfig(grad_threshold, opacity_threshold)
@@ -304,6 +315,32 @@ class TileBinner:
         p, n = C.c_void_p(), C.c_size_t()
         check(lib().gs_binner_buffer(self._h, idx, C.byref(p), C.byref(n)))
         return p.value, n.value
+
+
+def write_ply(path: str, positions4, scales2, quats4, opacities, sh48):
+    """write_3dgs_ply (first_attempt/crates/gs-io/src/ply/writer.rs) from host
+    arrays of activated values: positions (n,4), scales (n,2), quats xyzw
+    (n,4), opacities (n,), SH (n,48) coefficient-major."""
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (positions4, scales2, quats4, opacities, sh48)]
+    n = arrs[3].shape[0]
+    check(lib().gs_ply_write(os.fsencode(path), n, *[a.ctypes.data for a in arrs]))
+
+
+def read_ply(path: str) -> dict:
+    """load_ply of a splat file (ply/reader.rs): activated positions (n,3),
+    scales (n,3), quats xyzw (n,4), opacities (n,), SH (n, coeffs*3)."""
+    n, nc = C.c_uint32(), C.c_uint32()
+    check(lib().gs_ply_info(os.fsencode(path), C.byref(n), C.byref(nc)))
+    k = n.value
+    out = {"positions": np.zeros((k, 3), np.float32), "scales": np.zeros((k, 3), np.float32),
+           "quats": np.zeros((k, 4), np.float32), "opacities": np.zeros(k, np.float32),
+           "sh": np.zeros((k, 3 * nc.value), np.float32)}
+    got = C.c_uint32()
+    check(lib().gs_ply_read(os.fsencode(path), k, out["positions"].ctypes.data, out["scales"].ctypes.data,
+                            out["quats"].ctypes.data, out["opacities"].ctypes.data, out["sh"].ctypes.data,
+                            C.byref(got)))
+    out["sh_coeffs"] = nc.value
+    return out
 
 
 def radix_sort_pairs(keys_ptr: int, vals_ptr: int, n: int, key_bits: int = 32, stream: int = 0):
