@@ -271,6 +271,33 @@ typedef struct {
 gs_status gs_densify_prune(gs_rasterizer* r, const gs_densify_config* cfg, uint32_t num_surfels,
                            uint32_t* num_out, void* stream);
 
+/* ---- MCMC relocation (first_attempt/crates/gs-train/src/trainer.rs:1558-1689,
+ * shaders/relocate.wgsl, shaders/mcmc.wgsl) -------------------------------
+ * Dead surfels (activated opacity below dead_threshold) move onto alive
+ * surfels sampled in proportion to opacity (one xorshift64 draw per dead
+ * surfel in index order; a target already taken by a lower-indexed dead
+ * surfel defers this one); with split_ratio > 0, leftover dead slots then
+ * split the alive surfels larger than split_ratio x the median alive size
+ * (largest first). Both surfels of a pair get the opacity 1 - sqrt(1 - a),
+ * shrunk scales (x0.85, or x0.6 and +-0.6 sigma offsets for splits) and zero
+ * Adam moments. The same choices as the reference's host sampler for the same
+ * generator state, computed on the device without a readback; the generator
+ * state lives on the device and advances by one step per dead surfel.
+ * Requires gs_optimizer_init. Stream-ordered. */
+typedef struct {
+  float dead_threshold; /* 0.005 in the reference trainer (trainer.rs:487) */
+  float split_ratio;    /* 8.0 (trainer.rs:488); 0 disables splits */
+} gs_mcmc_config;
+gs_status gs_mcmc_seed(gs_rasterizer* r, uint64_t xorshift_state, void* stream);  /* nonzero; blocking */
+gs_status gs_mcmc_relocate(gs_rasterizer* r, const gs_mcmc_config* cfg, uint32_t num_surfels, void* stream);
+/* Blocking: out = {dead, relocated, split, deferred} of the last relocation, and the generator state. */
+gs_status gs_mcmc_stats(gs_rasterizer* r, uint32_t out[4], uint64_t* xorshift_state, void* stream);
+/* Exploration noise on positions (mcmc.wgsl:39-58): each coordinate moves by
+ * sigma * mean(scale) * exp(-opacity_k * opacity) * (sum of 4 uniforms - 2),
+ * uniforms from a PCG hash of (index ^ seed); the activated positions follow. */
+gs_status gs_mcmc_noise(gs_rasterizer* r, uint32_t num_surfels, uint32_t seed, float sigma, float opacity_k,
+                        void* stream);
+
 /* ---- TileBinner (crates/gs-kernels/src/binning.rs:22-238) ---------------
  * Items are tile-space AABBs (uint4 min_x, min_y, max_x, max_y inclusive;
  * max < min = culled) with u32 depth keys. After encode, sorted_entries holds

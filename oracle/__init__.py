@@ -330,3 +330,107 @@ def densify(arrays: dict, widths: dict, moments: set, grad_norm_sum, steps: int,
         cl = np.zeros((len(clone_idx), w), rows.dtype) if name in moments else rows[clone_idx]
         out[name] = np.concatenate([rows[kept_idx], cl], axis=0)
     return out, len(kept_idx) + len(clone_idx)
+
+
+_M64 = (1 << 64) - 1
+
+
+def _xorshift(x: int) -> int:
+    x ^= (x << 13) & _M64
+    x ^= x >> 7
+    x ^= (x << 17) & _M64
+    return x
+
+
+def mcmc_pairs(opacity_act, scales_act, rng_state: int, dead_threshold=0.005, split_ratio=8.0):
+    """Restatement of the reference's host sampler (first_attempt/crates/
+    gs-train/src/trainer.rs:1558-1647): dead = activated opacity below the
+    threshold; per dead surfel in index order one xorshift64 draw r·total
+    picks the first alive surfel whose cumulative (f64) opacity reaches it; a
+    pick equal to the dead index or already used defers the dead surfel;
+    leftover dead slots then split unused alive surfels larger than
+    split_ratio × the median alive size, largest first. Returns
+    (pairs [(dead, alive, mode)], new generator state)."""
+    op = np.asarray(opacity_act, np.float32)
+    n = len(op)
+    thr = np.float32(dead_threshold)
+    dead = [i for i in range(n) if op[i] < thr]
+    if not dead:
+        return [], rng_state
+    cum = []
+    total = 0.0
+    for o in op:
+        if o >= thr:
+            total += float(o)
+        cum.append(total)
+    if total <= 0.0:
+        return [], rng_state
+    cum = np.array(cum)
+    used = np.zeros(n, bool)
+    spent = np.zeros(len(dead), bool)
+    pairs = []
+    x = rng_state
+    for di, d in enumerate(dead):
+        x = _xorshift(x)
+        r = float(x >> 11) / float(1 << 53) * total
+        a = min(int(np.searchsorted(cum, r, side="left")), n - 1)
+        if a == d or used[a]:
+            continue
+        used[a] = True
+        spent[di] = True
+        pairs.append((d, a, 0))
+    if split_ratio > 0.0:
+        sc = np.asarray(scales_act, np.float32).reshape(n, 2)
+        size = np.maximum(sc[:, 0], sc[:, 1])
+        alive = op >= thr
+        alive_sizes = np.sort(size[alive], kind="stable")
+        if len(alive_sizes) >= 16:
+            med = alive_sizes[len(alive_sizes) // 2]
+            cap = np.float32(split_ratio) * med
+            over = [i for i in range(n) if alive[i] and size[i] > cap and not used[i]]
+            over.sort(key=lambda i: -size[i])  # stable: ties keep index order
+            left = [d for di, d in enumerate(dead) if not spent[di]]
+            for big, slot in zip(over, left):
+                used[big] = True
+                pairs.append((slot, big, 1))
+    return pairs, x
+
+
+def mcmc_apply(raw: dict, opacity_act, pairs):
+    """relocate.wgsl relocate_params/relocate_moments on numpy float32 copies:
+    raw = {"pos" (n,4), "scales" (n,2), "quat" (n,4), "opacity" (n,), "sh" (n,48),
+    "m_*"/"v_*" moments}. Returns the updated dict."""
+    out = {k: np.array(v, np.float32, copy=True) for k, v in raw.items()}
+    op = np.asarray(opacity_act, np.float32)
+    f = np.float32
+    for d, a, mode in pairs:
+        alpha = np.clip(op[a], f(1e-4), f(0.999))
+        an = np.clip(f(1.0) - np.sqrt(f(1.0) - alpha), f(1e-4), f(0.999))
+        logit = np.log(an / (f(1.0) - an))
+        out["opacity"][d] = logit
+        out["opacity"][a] = logit
+        q = out["quat"][a].copy()
+        out["quat"][d] = q
+        s = out["scales"][a].copy()
+        if mode == 1:
+            qn = q / np.sqrt((q * q).sum(dtype=np.float32))
+            x, y, z, w = qn
+            col0 = np.array([1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y)], np.float32)
+            col1 = np.array([2 * (x * y - w * z), 1 - 2 * (x * x + z * z), 2 * (y * z + w * x)], np.float32)
+            sw = np.exp(s)
+            axis = col0 * sw[0] if not sw[1] > sw[0] else col1 * sw[1]
+            c = out["pos"][a].copy()
+            out["pos"][d] = c + np.append(f(0.6) * axis, f(0.0))
+            out["pos"][a] = c - np.append(f(0.6) * axis, f(0.0))
+            s = s - f(0.51)
+        else:
+            out["pos"][d] = out["pos"][a]
+            s = s - f(0.16)
+        out["scales"][a] = s
+        out["scales"][d] = s
+        out["sh"][d] = out["sh"][a]
+        for k in list(out):
+            if k.startswith(("m_", "v_")):
+                out[k][d] = 0
+                out[k][a] = 0
+    return out

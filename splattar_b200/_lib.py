@@ -55,6 +55,10 @@ class SceneInputC(C.Structure):
                 ("sh", C.c_void_p), ("sh_coeffs", C.c_uint32), ("n", C.c_uint32)]
 
 
+class McmcConfig(C.Structure):
+    _fields_ = [("dead_threshold", C.c_float), ("split_ratio", C.c_float)]
+
+
 class AdamConfig(C.Structure):
     _fields_ = [("lr", C.c_float * 5), ("reg", C.c_float * 5), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("eps", C.c_float)]
@@ -112,6 +116,10 @@ def lib():
         "gs_radix_sort_pairs_noalloc": [vp, vp, u64, u32, vp],
         "gs_exclusive_scan_u32": [vp, vp, u64, vp, vp],
         "gs_camera_rotation": [C.POINTER(Camera), C.POINTER(C.c_float)],
+        "gs_mcmc_seed": [vp, u64, vp],
+        "gs_mcmc_relocate": [vp, C.POINTER(McmcConfig), u32, vp],
+        "gs_mcmc_stats": [vp, C.POINTER(u32), C.POINTER(u64), vp],
+        "gs_mcmc_noise": [vp, u32, u32, f32, f32, vp],
         "gs_ply_write": [C.c_char_p, u32, vp, vp, vp, vp, vp],
         "gs_ply_info": [C.c_char_p, C.POINTER(u32), C.POINTER(u32)],
         "gs_ply_read": [C.c_char_p, u32, vp, vp, vp, vp, vp, C.POINTER(u32)],
@@ -151,5 +159,6 @@ def exported_symbols() -> list[str]:
         "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_set_launch_shapes", "gs_binner_create",
         "gs_binner_destroy", "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_radix_sort_pairs_noalloc",
         "gs_exclusive_scan_u32",
-        "gs_camera_rotation", "gs_shutdown", "gs_ply_write", "gs_ply_info", "gs_ply_read", "gs_rasterizer_save_ply",
+        "gs_camera_rotation", "gs_shutdown", "gs_mcmc_seed", "gs_mcmc_relocate", "gs_mcmc_stats", "gs_mcmc_noise",
+        "gs_ply_write", "gs_ply_info", "gs_ply_read", "gs_rasterizer_save_ply",
         "gs_rasterizer_load_ply"]

@@ -28,6 +28,7 @@ UNITS = {
     "gs_loss.cu": [],
     "gs_optim.cu": [],
     "gs_noalloc.cu": [],
+    "gs_mcmc.cu": [],
     "gs_ply.cpp": [],
 }
 HEADERS = ["gs_common.cuh", "gs_kernels.h", "gs_geom.cuh"]

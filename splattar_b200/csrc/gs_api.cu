@@ -127,6 +127,12 @@ struct gs_rasterizer {
   float* dyn_dev = nullptr;
 
   // densify scratch
+  // MCMC relocation: scratch (allocated on first use) and device generator state
+  uint32_t* mcmc_u32 = nullptr;           // 19 arrays of capacity u32
+  unsigned long long* mcmc_u64 = nullptr;  // weight, cum (capacity each) + total
+  uint64_t* mcmc_jump = nullptr;           // MCMC_JUMP_LEVELS x 64 rows
+  uint64_t* mcmc_rng = nullptr;
+  uint32_t* mcmc_counters = nullptr;
   uint32_t* dens_flags = nullptr;
   uint32_t* dens_slots = nullptr;
   float* dens_tmp = nullptr;
@@ -676,6 +682,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->dl_dcolor, r->dl_dnormal, r->target, r->out_nc, r->coef, r->loss_sums, r->grad_geom,
                   r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
                   r->accum_norm, r->dyn_dev, r->dens_flags, r->dens_slots, r->dens_tmp, r->views_dev,
+                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters,
                   r->scan_scratch, r->sort_scratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1126,6 +1133,87 @@ gs_status gs_densify_prune(gs_rasterizer* r, const gs_densify_config* c, uint32_
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
   r->n_uploaded = out;
   *n_out = out;
+  return GS_OK;
+}
+
+// ------------------------------------------------------------------ MCMC
+static gs_status mcmc_ready(gs_rasterizer* r, cudaStream_t st) {
+  if (r->mcmc_u32) return GS_OK;
+  const size_t N = r->cap;
+  TRY_CUDA(r, dalloc(r->mcmc_u32, 19 * N));
+  TRY_CUDA(r, dalloc(r->mcmc_u64, 2 * N + 1));
+  TRY_CUDA(r, dalloc(r->mcmc_jump, 64 * (size_t)MCMC_JUMP_LEVELS));
+  TRY_CUDA(r, dalloc(r->mcmc_rng, 1));
+  TRY_CUDA(r, dalloc(r->mcmc_counters, 8));
+  std::vector<uint64_t> jump(64 * (size_t)MCMC_JUMP_LEVELS);
+  mcmc_jump_tables(jump.data());
+  TRY_CUDA(r, cudaMemcpyAsync(r->mcmc_jump, jump.data(), jump.size() * 8, cudaMemcpyHostToDevice, st));
+  const uint64_t seed = 0x853c49e6748fea9bull;
+  TRY_CUDA(r, cudaMemcpyAsync(r->mcmc_rng, &seed, 8, cudaMemcpyHostToDevice, st));
+  TRY_CUDA(r, cudaStreamSynchronize(st));  // the host sources above are stack/heap temporaries
+  return GS_OK;
+}
+
+gs_status gs_mcmc_seed(gs_rasterizer* r, uint64_t state, void* stream) {
+  if (!r || state == 0) return fail(r, GS_ERR_INVALID_ARG, "xorshift64 state must be nonzero");
+  cudaStream_t st = S(stream);
+  gs_status s = mcmc_ready(r, st);
+  if (s) return s;
+  TRY_CUDA(r, cudaMemcpyAsync(r->mcmc_rng, &state, 8, cudaMemcpyHostToDevice, st));
+  TRY_CUDA(r, cudaStreamSynchronize(st));
+  return GS_OK;
+}
+
+gs_status gs_mcmc_relocate(gs_rasterizer* r, const gs_mcmc_config* c, uint32_t n, void* stream) {
+  if (!r || !c) return GS_ERR_INVALID_ARG;
+  if (!r->optim_ready) return fail(r, GS_ERR_STATE, "gs_optimizer_init first");
+  if (n > r->cap) return fail(r, GS_ERR_CAPACITY, "num_surfels exceeds capacity");
+  if (n == 0) return GS_OK;
+  cudaStream_t st = S(stream);
+  gs_status s = mcmc_ready(r, st);
+  if (s) return s;
+  const size_t N = r->cap;
+  McmcArgs a{};
+  a.n = n; a.dead_threshold = c->dead_threshold; a.split_ratio = c->split_ratio;
+  a.jump = r->mcmc_jump; a.rng_state = r->mcmc_rng; a.counters = r->mcmc_counters;
+  uint32_t* u = r->mcmc_u32;
+  uint32_t** fields[] = {&a.dead, &a.dead_rank, &a.dead_idx, &a.owner, &a.used, &a.pick, &a.leftover_flag,
+                         &a.left_rank, &a.left_idx, &a.size_key, &a.size_val, &a.key2, &a.val2, &a.over_flag,
+                         &a.over_rank, &a.over_key, &a.over_val};
+  for (size_t k = 0; k < sizeof(fields) / sizeof(fields[0]); ++k) *fields[k] = u + k * N;
+  a.weight = r->mcmc_u64; a.cum = r->mcmc_u64 + N; a.total_weight = r->mcmc_u64 + 2 * N;
+  a.opac_act = r->opacities; a.scales_act = r->scales;
+  a.pos_raw = reinterpret_cast<float4*>(r->raw[0]); a.scales_raw = reinterpret_cast<float2*>(r->raw[1]);
+  a.quat_raw = reinterpret_cast<float4*>(r->raw[2]); a.opac_raw = r->raw[3]; a.sh_raw = r->raw[4];
+  a.pos_act = r->positions; a.scales_act_w = r->scales; a.quat_act = r->quats; a.opac_act_w = r->opacities;
+  a.sh_act = r->sh;
+  a.sh_half = r->cfg.precision == GS_PREC_F32 ? nullptr : r->sh_half;
+  for (int k = 0; k < 5; ++k) { a.m[k] = r->mom1[k]; a.v[k] = r->mom2[k]; }
+  TRY_LAUNCH(r, launch_mcmc_relocate(a, (int)r->cfg.precision, r->scan_scratch, r->sort_scratch, st));
+  return GS_OK;
+}
+
+gs_status gs_mcmc_stats(gs_rasterizer* r, uint32_t out[4], uint64_t* rng_state, void* stream) {
+  if (!r || !out) return GS_ERR_INVALID_ARG;
+  cudaStream_t st = S(stream);
+  gs_status s = mcmc_ready(r, st);
+  if (s) return s;
+  uint32_t c[8];
+  uint64_t x = 0;
+  TRY_CUDA(r, cudaMemcpyAsync(c, r->mcmc_counters, sizeof(c), cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaMemcpyAsync(&x, r->mcmc_rng, 8, cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaStreamSynchronize(st));
+  out[0] = c[0]; out[1] = c[1]; out[2] = c[2]; out[3] = c[3];
+  if (rng_state) *rng_state = x;
+  return GS_OK;
+}
+
+gs_status gs_mcmc_noise(gs_rasterizer* r, uint32_t n, uint32_t seed, float sigma, float opacity_k, void* stream) {
+  if (!r) return GS_ERR_INVALID_ARG;
+  if (!r->optim_ready) return fail(r, GS_ERR_STATE, "gs_optimizer_init first");
+  if (n > r->cap) return fail(r, GS_ERR_CAPACITY, "num_surfels exceeds capacity");
+  TRY_LAUNCH(r, launch_mcmc_noise(reinterpret_cast<float4*>(r->raw[0]), r->positions, r->scales, r->opacities, n,
+                                  seed, sigma, opacity_k, S(stream)));
   return GS_OK;
 }
 

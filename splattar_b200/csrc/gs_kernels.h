@@ -200,4 +200,33 @@ struct DensifyArgs {
 };
 int launch_densify(DensifyArgs& a, void* scan_scratch, cudaStream_t st);
 
+// ---- MCMC relocation and noise (gs_mcmc.cu) ----
+constexpr int MCMC_JUMP_LEVELS = 33;  // powers M^(2^j) of the xorshift64 step, j < 33
+struct McmcArgs {
+  uint32_t n;
+  float dead_threshold, split_ratio;
+  const uint64_t* jump;          // MCMC_JUMP_LEVELS × 64 rows
+  uint64_t* rng_state;           // device xorshift64 state, advanced by one step per dead surfel
+  uint32_t* counters;            // [0] dead [1] relocated [2] split [3] deferred [5] oversized [6] leftover
+  unsigned long long* total_weight;
+  // per-surfel scratch (capacity entries each)
+  uint32_t *dead, *dead_rank, *dead_idx, *owner, *used, *pick, *leftover_flag, *left_rank, *left_idx;
+  unsigned long long *weight, *cum;
+  uint32_t *size_key, *size_val, *key2, *val2, *over_flag, *over_rank, *over_key, *over_val;
+  const uint32_t* sorted_size_key;
+  const uint32_t* over_sorted_val;
+  // parameters
+  const float* opac_act;         // read for sampling
+  const float2* scales_act;
+  float4* pos_raw; float2* scales_raw; float4* quat_raw; float* opac_raw; float* sh_raw;
+  float4* pos_act; float2* scales_act_w; float4* quat_act; float* opac_act_w; float* sh_act;
+  void* sh_half;
+  float* m[5];
+  float* v[5];
+};
+void mcmc_jump_tables(uint64_t* out);
+int launch_mcmc_relocate(McmcArgs& a, int prec, void* scan_scratch, void* sort_scratch, cudaStream_t st);
+int launch_mcmc_noise(float4* pos_raw, float4* pos_act, const float2* scales_act, const float* opac_act, uint32_t n,
+                      uint32_t seed, float sigma, float opacity_k, cudaStream_t st);
+
 }  // namespace gs

@@ -18,7 +18,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._lib import (BUF, FLAG_COLOR_ONLY, FLAG_DETERMINISTIC, FLAG_PERSISTENT, FLAG_TIGHT_BINNING, PREC, AdamConfig, Camera,
-                   DensifyConfig, GsError, RasterConfig, SceneInputC, StepConfig, check, lib)
+                   DensifyConfig, GsError, McmcConfig, RasterConfig, SceneInputC, StepConfig, check, lib)
 
 SH_FLOATS = 48
 TILE = 16
@@ -231,6 +231,24 @@ class Rasterizer:
         """Apply raster launch shapes (e.g. a stored autotune result) without timing."""
         arr = (C.c_uint32 * 4)(fwd_batch, fwd_pixels_per_thread, bwd_batch, bwd_pixels_per_thread)
         self._chk(lib().gs_set_launch_shapes(self._h, arr))
+
+    def mcmc_seed(self, xorshift_state: int, stream: int = 0):
+        self._chk(lib().gs_mcmc_seed(self._h, xorshift_state, stream))
+
+    def mcmc_relocate(self, num_surfels: int, dead_threshold: float = 0.005, split_ratio: float = 8.0,
+                      stream: int = 0):
+        """Trainer::mcmc_relocate on the device (no readback)."""
+        cfg = McmcConfig(dead_threshold, split_ratio)
+        self._chk(lib().gs_mcmc_relocate(self._h, C.byref(cfg), num_surfels, stream))
+
+    def mcmc_stats(self, stream: int = 0) -> dict:
+        out = (C.c_uint32 * 4)()
+        st = C.c_uint64()
+        self._chk(lib().gs_mcmc_stats(self._h, out, C.byref(st), stream))
+        return {"dead": out[0], "relocated": out[1], "split": out[2], "deferred": out[3], "rng_state": st.value}
+
+    def mcmc_noise(self, num_surfels: int, seed: int, sigma: float, opacity_k: float = 5.0, stream: int = 0):
+        self._chk(lib().gs_mcmc_noise(self._h, num_surfels, seed, sigma, opacity_k, stream))
 
     def save_ply(self, path: str, num_surfels: int, stream: int = 0):
         """The activated surfels [0, num_surfels) to a 3DGS-layout PLY file."""
