@@ -49,7 +49,9 @@ typedef enum { GS_PREC_F32 = 0, GS_PREC_F16 = 1, GS_PREC_BF16 = 2 } gs_precision
 enum {
   GS_FLAG_DETERMINISTIC = 1u << 0, /* ordered per-entry gradient reduction, no float atomics */
   GS_FLAG_PERSISTENT = 1u << 1,    /* persistent raster kernels over a global tile queue */
-  GS_FLAG_COLOR_ONLY = 1u << 2,    /* backward ignores dl_dcolor.w, dl_dnormal and lambda_dist */
+  GS_FLAG_COLOR_ONLY = 1u << 2,    /* backward ignores dl_dcolor.w, dl_dnormal and lambda_dist; the chosen-form
+                                      training step's forward writes colour, alpha and final T only (OUT_NORMAL and
+                                      the depth in OUT_AUX.y are left as they were) */
   GS_FLAG_TIGHT_BINNING = 1u << 3  /* bin a surfel only into the tiles its alpha >= 1/255 box overlaps: images and
                                       gradients are unchanged; tile lists, ranges and OUT_NCONTRIB then refer to the
                                       shorter lists instead of the reference's conservative rects */

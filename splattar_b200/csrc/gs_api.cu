@@ -285,7 +285,8 @@ const void* sh_for(gs_rasterizer* r, int prec) { return prec == 0 ? (const void*
 // Projection + binning + forward raster for `nv` views starting at views_dev
 // (already uploaded), `tiles` tiles in total, storage precision `prec`.
 gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vhost, uint32_t nv, int tiles, uint32_t n,
-                      int prec, bool persistent, bool tight, cudaStream_t st, Prof* prof = nullptr) {
+                      int prec, bool persistent, bool tight, cudaStream_t st, Prof* prof = nullptr,
+                      bool color = false) {
   const uint32_t items = nv * n;
   mark(prof, -1, st);
   ProjectArgs pa{};
@@ -333,9 +334,9 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   int grid = tiles;
   if (persistent) {
     TRY_CUDA(r, cudaMemsetAsync(r->words + 2, 0, sizeof(uint32_t), st));
-    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(prec, batch, ppt, r->det));
+    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(prec, batch, ppt, r->det, color));
   }
-  TRY_LAUNCH(r, launch_raster_fwd(ra, prec, batch, ppt, r->det, persistent, grid, st));
+  TRY_LAUNCH(r, launch_raster_fwd(ra, prec, batch, ppt, r->det, persistent, color && persistent, grid, st));
   mark(prof, 5, st);
   r->last_nv = nv; r->last_n = n; r->last_tiles = tiles; r->last_views_dev = vdev; r->last_views_host = vhost;
   r->have_forward = true;
@@ -485,7 +486,8 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   const ViewInfo* vdev = r->views_dev;
   int tiles = 0;
   for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
-  gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, prof);
+  // With GS_FLAG_COLOR_ONLY the step's forward leaves depth and normal unwritten (nothing reads them).
+  gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, prof, r->color_only);
   if (s) return s;
   TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
   s = run_loss(r, vdev, r->views_batched.data(), nv, cfg->w_l1, cfg->w_ssim, r->loss_sums, st);
@@ -1062,7 +1064,7 @@ gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint
     r->fwd_ppt = fshape[k][1];
     gs_status fs = GS_OK;
     const float ms = time_it([&] { fs = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true,
-                                                    true, st); });
+                                                    true, st, nullptr, r->color_only); });
     if (fs) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fs; }
     if (ms < best) { best = ms; bf = k; }
   }

@@ -91,14 +91,14 @@ struct RasterArgs {
   uint32_t* tile_counter;       // persistent kernels: zeroed before each launch
 };
 // Blocks per SM the raster kernels sustain (for persistent grids).
-int raster_fwd_occupancy(int prec, int batch, int ppt, bool det);
+int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color);
 int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det);
 
 int launch_project(const ProjectArgs& a, int prec, uint32_t n_views, cudaStream_t st);
 int launch_project_bwd(const ProjectBwdArgs& a, int prec, bool aux, cudaStream_t st);
 int prepare_project_kernels();
 int launch_project_bwd_adam(const ProjectBwdArgs& a, const AdamFusedArgs& opt, int prec, bool aux, cudaStream_t st);
-int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, int grid,
+int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, bool color, int grid,
                       cudaStream_t st);
 int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, int ppt, int batch, bool det, bool persistent, int grid,
                       cudaStream_t st);

@@ -139,11 +139,15 @@ __device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept)
   return off + __popc(bal & lanemask_lt());
 }
 
-template <int BATCH, int PREC, bool DET, bool PERSIST, int PPT>
+// COLOR: colour, alpha and final transmittance only (the training step's
+// loss reads nothing else); depth and normal are neither accumulated nor
+// written.
+template <int BATCH, int PREC, bool DET, bool PERSIST, int PPT, bool COLOR = false>
 __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
   constexpr int NT = 256 / PPT, NW = NT / 32;
   static_assert(BATCH <= NT, "one staging pass per batch");
-  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_r4[BATCH], s_bb[BATCH];
+  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
+  __shared__ float4 s_r4[COLOR ? 1 : BATCH];
   __shared__ int s_j[BATCH];
   __shared__ int s_wcount[NW];
   __shared__ int s_tile;
@@ -186,7 +190,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
       if (keep) {
         float4 r0, r1, r2, r3, r4;
         load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
-        s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3; s_r4[slot] = r4;
+        s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
+        if (!COLOR) s_r4[slot] = r4;
         s_bb[slot] = bb;
         s_j[slot] = tid;
       }
@@ -196,7 +201,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
           const float4 bbk = s_bb[k];
           if (g.pxc < bbk.x || g.pxc > bbk.y) continue;
           const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
-          const float4 r3 = s_r3[k], r4 = s_r4[k];
+          const float4 r3 = s_r3[k];
+          const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
           const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
 #pragma unroll
           for (int p = 0; p < PPT; ++p) {
@@ -207,8 +213,10 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
             const float w = T[p] * alpha;
             cr[p] += r3.x * w; cg[p] += r3.y * w; cb[p] += r3.z * w;
             aa[p] += w;
-            ad[p] += h.t * w;
-            nx[p] += r4.x * w; ny[p] += r4.y * w; nz[p] += r4.z * w;
+            if (!COLOR) {
+              ad[p] += h.t * w;
+              nx[p] += r4.x * w; ny[p] += r4.y * w; nz[p] += r4.z * w;
+            }
             T[p] = __fmul_rn(T[p], 1.0f - alpha);
             nc[p] = idx1;
             if (T[p] < T_TERMINATE) done[p] = true;
@@ -225,8 +233,12 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
       if (!g.inside[p]) continue;
       const long long pix = g.row0 + (long long)p * g.W;
       a.out_color[pix] = make_float4(cr[p], cg[p], cb[p], aa[p]);
-      a.out_aux[pix] = make_float4(T[p], ad[p], 0.f, 0.f);
-      a.out_normal[pix] = make_float4(nx[p], ny[p], nz[p], 0.f);
+      if (COLOR) {
+        a.out_aux[pix].x = T[p];
+      } else {
+        a.out_aux[pix] = make_float4(T[p], ad[p], 0.f, 0.f);
+        a.out_normal[pix] = make_float4(nx[p], ny[p], nz[p], 0.f);
+      }
       a.out_nc[pix] = nc[p];
     }
     if (!PERSIST) return;
@@ -469,17 +481,17 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
 // Backward: two pixels per thread and 128-entry batches without aux
 // losses; one pixel per thread and 32-entry batches with aux losses (the
 // per-warp partial buffer is NW·BATCH·NG floats of static shared memory).
-template <int PREC, bool DET, bool PERSIST>
+template <int PREC, bool DET, bool PERSIST, bool COLOR = false>
 void fwd_dispatch(const RasterArgs& a, int batch, int ppt, int grid, cudaStream_t st) {
   if (ppt == 4) {
-    k_raster_fwd<64, PREC, DET, PERSIST, 4><<<grid, 64, 0, st>>>(a);
+    k_raster_fwd<64, PREC, DET, PERSIST, 4, COLOR><<<grid, 64, 0, st>>>(a);
   } else if (ppt == 2) {
-    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
-    else k_raster_fwd<128, PREC, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
+    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 2, COLOR><<<grid, 128, 0, st>>>(a);
+    else k_raster_fwd<128, PREC, DET, PERSIST, 2, COLOR><<<grid, 128, 0, st>>>(a);
   } else {
-    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
-    else if (batch == 256) k_raster_fwd<256, PREC, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
-    else k_raster_fwd<128, PREC, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
+    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 1, COLOR><<<grid, 256, 0, st>>>(a);
+    else if (batch == 256) k_raster_fwd<256, PREC, DET, PERSIST, 1, COLOR><<<grid, 256, 0, st>>>(a);
+    else k_raster_fwd<128, PREC, DET, PERSIST, 1, COLOR><<<grid, 256, 0, st>>>(a);
   }
 }
 
@@ -506,10 +518,12 @@ int occ(K kernel, int threads) {
 
 }  // namespace
 
-int raster_fwd_occupancy(int prec, int batch, int ppt, bool det) {
-#define GS_O1(B, P) (det ? occ(k_raster_fwd<B, P, true, true, 1>, 256) : occ(k_raster_fwd<B, P, false, true, 1>, 256))
-#define GS_O2(B, P) (det ? occ(k_raster_fwd<B, P, true, true, 2>, 128) : occ(k_raster_fwd<B, P, false, true, 2>, 128))
-#define GS_O4(P) (det ? occ(k_raster_fwd<64, P, true, true, 4>, 64) : occ(k_raster_fwd<64, P, false, true, 4>, 64))
+int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color) {
+#define GS_OC(B, P, D, PPT, NT) (color ? occ(k_raster_fwd<B, P, D, true, PPT, true>, NT) \
+                                       : occ(k_raster_fwd<B, P, D, true, PPT, false>, NT))
+#define GS_O1(B, P) (det ? GS_OC(B, P, true, 1, 256) : GS_OC(B, P, false, 1, 256))
+#define GS_O2(B, P) (det ? GS_OC(B, P, true, 2, 128) : GS_OC(B, P, false, 2, 128))
+#define GS_O4(P) (det ? GS_OC(64, P, true, 4, 64) : GS_OC(64, P, false, 4, 64))
 #define GS_OB(P) (ppt == 4 ? GS_O4(P) : ppt == 2 ? (batch == 64 ? GS_O2(64, P) : GS_O2(128, P)) \
                            : (batch == 64 ? GS_O1(64, P) : (batch == 256 ? GS_O1(256, P) : GS_O1(128, P))))
   return prec == 0 ? GS_OB(0) : (prec == 1 ? GS_OB(1) : GS_OB(2));
@@ -517,6 +531,7 @@ int raster_fwd_occupancy(int prec, int batch, int ppt, bool det) {
 #undef GS_O4
 #undef GS_O2
 #undef GS_O1
+#undef GS_OC
 }
 
 int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det) {
@@ -531,13 +546,16 @@ int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det) {
 #undef GS_OV
 }
 
-int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, int grid,
-                      cudaStream_t st) {
+int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, bool color,
+                      int grid, cudaStream_t st) {
   if (a.total_tiles == 0) return 0;
+  if (color && !persistent) return (int)cudaErrorInvalidValue;  // the colour-only variant is persistent
 #define GS_F(P, D, S) fwd_dispatch<P, D, S>(a, batch, ppt, grid, st)
 #define GS_F2(P)                                   \
-  if (det) { if (persistent) GS_F(P, true, true); else GS_F(P, true, false); } \
-  else { if (persistent) GS_F(P, false, true); else GS_F(P, false, false); }
+  if (det) { if (color) fwd_dispatch<P, true, true, true>(a, batch, ppt, grid, st); \
+             else if (persistent) GS_F(P, true, true); else GS_F(P, true, false); } \
+  else { if (color) fwd_dispatch<P, false, true, true>(a, batch, ppt, grid, st); \
+         else if (persistent) GS_F(P, false, true); else GS_F(P, false, false); }
   if (prec == 0) { GS_F2(0) } else if (prec == 1) { GS_F2(1) } else { GS_F2(2) }
 #undef GS_F2
 #undef GS_F
