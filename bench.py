@@ -51,6 +51,9 @@ def parse(argv=None):
     p.add_argument("--densify-every", type=int, default=0,
                    help="densify/prune cycle: clone/prune every K timed steps (grad 2e-4, opacity 0.005)")
     p.add_argument("--deterministic", action="store_true", help="ordered gradient reduction (densify cycle)")
+    p.add_argument("--stored-state", action="store_true",
+                   help="stored-state backward: the forward records per-pixel contributor masks")
+    p.add_argument("--entries-budget", type=float, default=96.0, help="tile-entry capacity per item")
     p.add_argument("--capacity-factor", type=float, default=1.25, help="densify cycle: capacity / initial surfels")
     p.add_argument("--entries-per-item", type=float, default=12.0, help="densify cycle: tile-entry budget per item")
     return p.parse_args(argv)
@@ -212,8 +215,11 @@ def run_ours(args, ws, rank, local):
     wl = workload(args.workload)
     cams = wl.cameras
     n, nv, P = wl.surfels.n, len(cams), wl.pixels
-    max_entries = int(min(4.2e9, 96 * n * nv))
-    rast = Rasterizer(n, 0, 0, max_entries, max_views=nv, max_pixels=P, precision=args.precision, color_only=True)
+    max_entries = int(min(4.2e9, args.entries_budget * n * nv))
+    free0, _ = torch.cuda.mem_get_info()
+    rast = Rasterizer(n, 0, 0, max_entries, max_views=nv, max_pixels=P, precision=args.precision, color_only=True,
+                      stored_state=args.stored_state)
+    free1, _ = torch.cuda.mem_get_info()
     # Target images: the seed-1 scene rendered through the same cameras.
     rast.upload_scene(wl.target_surfels.scene_input())
     rast.forward(cams, n)
@@ -279,6 +285,7 @@ def run_ours(args, ws, rank, local):
     n_tiles = sum(((c.width + 15) // 16) * ((c.height + 15) // 16) for c in cams)
     rast.check(sp)
     result = dict(tuned=tuned, wl=wl, n=n, nv=nv, P=P, E=E, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
+                  handle_bytes=int(free0 - free1),
                   stages=stages, n_tiles=n_tiles, loss=loss_vals, h2d=tgt_host.numel() * 4,
                   d2h=loss_host.numel() * 8)
     rast.close()
@@ -408,6 +415,8 @@ def main():
             "l2": "inputs larger than L2 (params+optimizer state ~1.5 GB, tile entries ~%.1f GB)" % (E * 16 / 1e9),
             "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
             "autotuned": r["tuned"],
+            "backward": "stored-state (forward contributor masks)" if args.stored_state else "recompute",
+            "device_bytes_of_handle": r["handle_bytes"],
         },
         "mpix_per_s": round(steps_s * P / 1e6 * ws, 2),
         "plain": None if r["ms_plain"] is None else {

@@ -52,9 +52,13 @@ enum {
   GS_FLAG_COLOR_ONLY = 1u << 2,    /* backward ignores dl_dcolor.w, dl_dnormal and lambda_dist; the chosen-form
                                       training step's forward writes colour, alpha and final T only (OUT_NORMAL and
                                       the depth in OUT_AUX.y are left as they were) */
-  GS_FLAG_TIGHT_BINNING = 1u << 3  /* bin a surfel only into the tiles its alpha >= 1/255 box overlaps: images and
+  GS_FLAG_TIGHT_BINNING = 1u << 3, /* bin a surfel only into the tiles its alpha >= 1/255 box overlaps: images and
                                       gradients are unchanged; tile lists, ranges and OUT_NCONTRIB then refer to the
                                       shorter lists instead of the reference's conservative rects */
+  GS_FLAG_STORED_STATE = 1u << 4   /* stored-state backward for the chosen-form step (with GS_FLAG_COLOR_ONLY): the
+                                      forward records which tile entries composited into each pixel (one bit per
+                                      pixel and entry, 32 bytes per entry of max_entries held by the handle) and
+                                      the backward evaluates only those; results are identical */
 };
 
 /* Rasterizer::new(ctx, capacity, width, height, max_entries)

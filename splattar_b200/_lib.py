@@ -20,6 +20,7 @@ FLAG_DETERMINISTIC = 1
 FLAG_PERSISTENT = 2
 FLAG_COLOR_ONLY = 4
 FLAG_TIGHT_BINNING = 8
+FLAG_STORED_STATE = 16
 
 BUF = {
     "positions": 0, "scales": 1, "quats": 2, "opacities": 3, "sh": 4, "out_color": 5, "out_aux": 6,

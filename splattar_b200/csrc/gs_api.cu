@@ -95,6 +95,11 @@ struct gs_rasterizer {
   float* partials = nullptr;
   uint2* ranges = nullptr;
   int ent_in1 = 0;
+  // stored-state mode: contributor masks of the last colour-only forward
+  uint32_t* mask = nullptr;
+  uint32_t* mask_off = nullptr;
+  uint32_t* mask_words = nullptr;
+  bool stored_state = false, mask_valid = false;
 
   // device scalars: [0] entry total u64, then u32 words
   unsigned long long* entry_total = nullptr;
@@ -330,11 +335,17 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ra.records = r->records;
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.tile_counter = r->words + 2;
+  r->mask_valid = r->stored_state && color && persistent;
+  if (r->mask_valid) {
+    TRY_LAUNCH(r, launch_mask_offsets(r->ranges, (uint32_t)tiles, r->mask_words, r->mask_off, r->scan_scratch, st));
+    ra.mask = r->mask;
+    ra.mask_off = r->mask_off;
+  }
   const int batch = r->fwd_batch, ppt = r->fwd_ppt;
   int grid = tiles;
   if (persistent) {
     TRY_CUDA(r, cudaMemsetAsync(r->words + 2, 0, sizeof(uint32_t), st));
-    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(prec, batch, ppt, r->det, color));
+    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(prec, batch, ppt, r->det, color, ra.mask != nullptr));
   }
   TRY_LAUNCH(r, launch_raster_fwd(ra, prec, batch, ppt, r->det, persistent, color && persistent, grid, st));
   mark(prof, 5, st);
@@ -360,10 +371,15 @@ gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t n
                               bool aux, bool persistent, cudaStream_t st) {
   if (!r->det) TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)nv * n, st));
   RasterArgs ra = bwd_args(r, vdev, nv, tiles);
+  if (r->mask_valid && !aux) {  // masks of the matching colour-only forward
+    ra.mask = r->mask;
+    ra.mask_off = r->mask_off;
+  }
   int grid = tiles;
   if (persistent) {
     TRY_CUDA(r, cudaMemsetAsync(r->words + 3, 0, sizeof(uint32_t), st));
-    grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(prec, aux, r->bwd_ppt, r->bwd_batch, r->det));
+    grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(prec, aux, r->bwd_ppt, r->bwd_batch, r->det,
+                                                              ra.mask != nullptr));
   }
   TRY_LAUNCH(r, launch_raster_bwd(ra, prec, aux, r->bwd_ppt, r->bwd_batch, r->det, persistent, grid, st));
   return GS_OK;
@@ -596,6 +612,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   r->persistent = (c.flags & GS_FLAG_PERSISTENT) != 0;
   r->color_only = (c.flags & GS_FLAG_COLOR_ONLY) != 0;
   r->tight = (c.flags & GS_FLAG_TIGHT_BINNING) != 0;
+  r->stored_state = (c.flags & GS_FLAG_STORED_STATE) != 0;
   r->fwd_batch = (int)c.batch;
   r->fwd_ppt = (int)c.pixels_per_thread;
   auto bail = [&](cudaError_t e, const char* what) {
@@ -637,6 +654,12 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
     ALLOC(r->entry_offset, I);
   }
   ALLOC(r->ranges, r->max_tiles);
+  if (r->stored_state) {
+    // One bit per (pixel, tile entry): 32 bytes per entry, whole 32-entry words per tile.
+    ALLOC(r->mask, ((size_t)E / 32 + r->max_tiles) * 256);
+    ALLOC(r->mask_off, r->max_tiles);
+    ALLOC(r->mask_words, r->max_tiles);
+  }
   ALLOC(r->entry_total, 1);
   ALLOC(r->words, 8);
   ALLOC(r->out_color, P); ALLOC(r->out_aux, P); ALLOC(r->out_normal, P); ALLOC(r->dl_dcolor, P);
@@ -684,7 +707,8 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->dl_dcolor, r->dl_dnormal, r->target, r->out_nc, r->coef, r->loss_sums, r->grad_geom,
                   r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
                   r->accum_norm, r->dyn_dev, r->dens_flags, r->dens_slots, r->dens_tmp, r->views_dev,
-                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters,
+                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off,
+                  r->mask_words,
                   r->scan_scratch, r->sort_scratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);

@@ -89,10 +89,15 @@ struct RasterArgs {
   float* partials;
   float lambda_dist;
   uint32_t* tile_counter;       // persistent kernels: zeroed before each launch
+  // Stored-state mode: per-pixel contributor bitmasks. Word w of pixel i
+  // (0..255, row-major in the tile) of tile t is mask[(mask_off[t] + w)·256 + i];
+  // bit b of word w is set when list position 32w + b composited into the pixel.
+  uint32_t* mask;               // null: the backward re-evaluates every entry
+  const uint32_t* mask_off;     // per tile, in 256-word groups
 };
 // Blocks per SM the raster kernels sustain (for persistent grids).
-int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color);
-int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det);
+int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color, bool mask);
+int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det, bool mask);
 
 int launch_project(const ProjectArgs& a, int prec, uint32_t n_views, cudaStream_t st);
 int launch_project_bwd(const ProjectBwdArgs& a, int prec, bool aux, cudaStream_t st);
@@ -150,6 +155,9 @@ struct ExpandArgs {
 };
 int launch_expand(const ExpandArgs& a, cudaStream_t st);
 // ranges[t] = [start, end) of tile t in the sorted pairs (ranges zeroed by the callee).
+// mask_off[t] = Σ_{t' < t} ⌈len(t')/32⌉ over the tiles' entry ranges.
+int launch_mask_offsets(const uint2* ranges, uint32_t num_tiles, uint32_t* words, uint32_t* mask_off, void* scratch,
+                        cudaStream_t st);
 int launch_ranges(const uint2* sorted_pairs, const unsigned long long* total, uint64_t capacity, uint2* ranges,
                   uint32_t num_tiles, cudaStream_t st);
 // After the entry scan: on overflow flag the error and zero the entry counts.

@@ -142,8 +142,9 @@ __device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept)
 // COLOR: colour, alpha and final transmittance only (the training step's
 // loss reads nothing else); depth and normal are neither accumulated nor
 // written.
-template <int BATCH, int PREC, bool DET, bool PERSIST, int PPT, bool COLOR = false>
+template <int BATCH, int PREC, bool DET, bool PERSIST, int PPT, bool COLOR = false, bool MASK = false>
 __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
+  static_assert(!MASK || COLOR, "contributor masks belong to the colour-only variant");
   constexpr int NT = 256 / PPT, NW = NT / 32;
   static_assert(BATCH <= NT, "one staging pass per batch");
   __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
@@ -166,12 +167,21 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
     uint32_t nc[PPT];
     bool done[PPT];
     bool tdone = true;
+    // Stored-state contributor masks (colour-only variant): the word being
+    // filled and its index, per pixel.
+    uint32_t mw[PPT];
+    int mi[PPT];
+    constexpr bool masks = MASK;
+    const size_t mbase = masks ? (size_t)__ldg(&a.mask_off[tile]) * 256 : 0;
+    const int mpix = ((tid >> 4) * PPT) * TILE + (tid & 15);  // pixel p is mpix + p·TILE
 #pragma unroll
     for (int p = 0; p < PPT; ++p) {
       T[p] = 1.f; cr[p] = cg[p] = cb[p] = aa[p] = ad[p] = nx[p] = ny[p] = nz[p] = 0.f;
       nc[p] = 0;
       done[p] = !g.inside[p];
       tdone &= done[p];
+      mw[p] = 0u;
+      mi[p] = 0;
     }
     for (uint32_t base = range.x; base < range.y; base += BATCH) {
       if (__syncthreads_count(tdone) == NT) break;
@@ -219,6 +229,18 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
             }
             T[p] = __fmul_rn(T[p], 1.0f - alpha);
             nc[p] = idx1;
+            if (masks) {
+              const uint32_t cidx = idx1 - 1u;
+              const int w = (int)(cidx >> 5);
+              if (w != mi[p]) {  // close the current word, zero the words skipped
+                uint32_t* m = a.mask + mbase + mpix + p * TILE;
+                m[(size_t)mi[p] * 256] = mw[p];
+                for (int z = mi[p] + 1; z < w; ++z) m[(size_t)z * 256] = 0u;
+                mi[p] = w;
+                mw[p] = 0u;
+              }
+              mw[p] |= 1u << (cidx & 31u);
+            }
             if (T[p] < T_TERMINATE) done[p] = true;
           }
           bool all = true;
@@ -233,6 +255,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
       if (!g.inside[p]) continue;
       const long long pix = g.row0 + (long long)p * g.W;
       a.out_color[pix] = make_float4(cr[p], cg[p], cb[p], aa[p]);
+      if (masks && nc[p] > 0) a.mask[mbase + mpix + p * TILE + (size_t)mi[p] * 256] = mw[p];
       if (COLOR) {
         a.out_aux[pix].x = T[p];
       } else {
@@ -246,8 +269,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
   }
 }
 
-template <int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT>
+template <int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT, bool MASK = false>
 __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
+  static_assert(!MASK || !AUX, "contributor masks cover the colour-only backward");
   constexpr int NT = 256 / PPT, NW = NT / 32;
   constexpr int NG = AUX ? 32 : 16;  // reduced components per entry (AUX: 20 used)
   constexpr int NQ = AUX ? 5 : 4;    // float4 groups per entry written out
@@ -314,6 +338,15 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
     if (my_max) atomicMax(&s_maxnc, (int)my_max);
     __syncthreads();
     const uint32_t maxnc = min((uint32_t)s_maxnc, range.y - range.x);
+    // Stored-state mode: contributor masks written by the forward; the word
+    // cached per pixel and its index (list positions are walked downwards).
+    constexpr bool masks = MASK;
+    const size_t mbase = masks ? (size_t)__ldg(&a.mask_off[tile]) * 256 : 0;
+    const int mpix = ((tid >> 4) * PPT) * TILE + (tid & 15);
+    uint32_t cm[PPT];
+    int cw[PPT];
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) { cm[p] = 0u; cw[p] = -1; }
 
     if (DET) {
       // Entries past the tile's last contributor get zero partials.
@@ -364,19 +397,40 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
           if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
           continue;
         }
+        bool bit[PPT];
+        bool anybit = false;
+        if (masks) {
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) {
+            bit[p] = false;
+            if (cidx < nc[p]) {
+              const int w = (int)(cidx >> 5);
+              if (w != cw[p]) {
+                cw[p] = w;
+                cm[p] = __ldg(a.mask + mbase + mpix + p * TILE + (size_t)w * 256);
+              }
+              bit[p] = (cm[p] >> (cidx & 31u)) & 1u;
+              anybit |= bit[p];
+            }
+          }
+          if (!__any_sync(FULL, anybit)) {  // no pixel of this warp composited the entry
+            if (lane < 16) s_part[warp][k][lane] = 0.f;
+            continue;
+          }
+        }
         const float4 bbk = s_bb[k];
         float gg[NG];
 #pragma unroll
         for (int c = 0; c < NG; ++c) gg[c] = 0.f;
         bool contrib = false;
-        if (g.pxc >= bbk.x && g.pxc <= bbk.y) {
+        if (masks ? anybit : (g.pxc >= bbk.x && g.pxc <= bbk.y)) {
           const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
           if (AUX) { r4 = s_r4[k]; depth = r4.w; }
 #pragma unroll
           for (int p = 0; p < PPT; ++p) {
-            if (!(cidx < nc[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
+            if (masks ? !bit[p] : (!(cidx < nc[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w)) continue;
             const Hit h = eval_hit(r0, r1, r2, depth, g.sx, g.sy[p], g.pxc, g.pyc[p]);
             const float raw_alpha = __fmul_rn(r3.w, h.ghat);
             const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
@@ -481,31 +535,31 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
 // Backward: two pixels per thread and 128-entry batches without aux
 // losses; one pixel per thread and 32-entry batches with aux losses (the
 // per-warp partial buffer is NW·BATCH·NG floats of static shared memory).
-template <int PREC, bool DET, bool PERSIST, bool COLOR = false>
+template <int PREC, bool DET, bool PERSIST, bool COLOR = false, bool MASK = false>
 void fwd_dispatch(const RasterArgs& a, int batch, int ppt, int grid, cudaStream_t st) {
   if (ppt == 4) {
-    k_raster_fwd<64, PREC, DET, PERSIST, 4, COLOR><<<grid, 64, 0, st>>>(a);
+    k_raster_fwd<64, PREC, DET, PERSIST, 4, COLOR, MASK><<<grid, 64, 0, st>>>(a);
   } else if (ppt == 2) {
-    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 2, COLOR><<<grid, 128, 0, st>>>(a);
-    else k_raster_fwd<128, PREC, DET, PERSIST, 2, COLOR><<<grid, 128, 0, st>>>(a);
+    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 2, COLOR, MASK><<<grid, 128, 0, st>>>(a);
+    else k_raster_fwd<128, PREC, DET, PERSIST, 2, COLOR, MASK><<<grid, 128, 0, st>>>(a);
   } else {
-    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 1, COLOR><<<grid, 256, 0, st>>>(a);
-    else if (batch == 256) k_raster_fwd<256, PREC, DET, PERSIST, 1, COLOR><<<grid, 256, 0, st>>>(a);
-    else k_raster_fwd<128, PREC, DET, PERSIST, 1, COLOR><<<grid, 256, 0, st>>>(a);
+    if (batch == 64) k_raster_fwd<64, PREC, DET, PERSIST, 1, COLOR, MASK><<<grid, 256, 0, st>>>(a);
+    else if (batch == 256) k_raster_fwd<256, PREC, DET, PERSIST, 1, COLOR, MASK><<<grid, 256, 0, st>>>(a);
+    else k_raster_fwd<128, PREC, DET, PERSIST, 1, COLOR, MASK><<<grid, 256, 0, st>>>(a);
   }
 }
 
 // Backward variants without aux losses: (pixels per thread, batch) ∈
 // {(1, 64), (2, 64), (2, 128)}; with aux losses (1, 32).
-template <int PREC, bool AUX, bool DET, bool PERSIST>
+template <int PREC, bool AUX, bool DET, bool PERSIST, bool MASK = false>
 void bwd_dispatch(const RasterArgs& a, int ppt, int batch, int grid, cudaStream_t st) {
   if constexpr (AUX) {
     k_raster_bwd<32, PREC, true, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
   } else {
-    if (ppt == 4) k_raster_bwd<64, PREC, false, DET, PERSIST, 4><<<grid, 64, 0, st>>>(a);
-    else if (ppt == 1) k_raster_bwd<64, PREC, false, DET, PERSIST, 1><<<grid, 256, 0, st>>>(a);
-    else if (batch == 64) k_raster_bwd<64, PREC, false, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
-    else k_raster_bwd<128, PREC, false, DET, PERSIST, 2><<<grid, 128, 0, st>>>(a);
+    if (ppt == 4) k_raster_bwd<64, PREC, false, DET, PERSIST, 4, MASK><<<grid, 64, 0, st>>>(a);
+    else if (ppt == 1) k_raster_bwd<64, PREC, false, DET, PERSIST, 1, MASK><<<grid, 256, 0, st>>>(a);
+    else if (batch == 64) k_raster_bwd<64, PREC, false, DET, PERSIST, 2, MASK><<<grid, 128, 0, st>>>(a);
+    else k_raster_bwd<128, PREC, false, DET, PERSIST, 2, MASK><<<grid, 128, 0, st>>>(a);
   }
 }
 
@@ -518,9 +572,10 @@ int occ(K kernel, int threads) {
 
 }  // namespace
 
-int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color) {
-#define GS_OC(B, P, D, PPT, NT) (color ? occ(k_raster_fwd<B, P, D, true, PPT, true>, NT) \
-                                       : occ(k_raster_fwd<B, P, D, true, PPT, false>, NT))
+int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color, bool mask) {
+#define GS_OC(B, P, D, PPT, NT) (mask ? occ(k_raster_fwd<B, P, D, true, PPT, true, true>, NT)  \
+                                 : color ? occ(k_raster_fwd<B, P, D, true, PPT, true>, NT) \
+                                         : occ(k_raster_fwd<B, P, D, true, PPT, false>, NT))
 #define GS_O1(B, P) (det ? GS_OC(B, P, true, 1, 256) : GS_OC(B, P, false, 1, 256))
 #define GS_O2(B, P) (det ? GS_OC(B, P, true, 2, 128) : GS_OC(B, P, false, 2, 128))
 #define GS_O4(P) (det ? GS_OC(64, P, true, 4, 64) : GS_OC(64, P, false, 4, 64))
@@ -534,30 +589,35 @@ int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color) {
 #undef GS_OC
 }
 
-int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det) {
-#define GS_OV(P, D) (aux ? occ(k_raster_bwd<32, P, true, D, true, 1>, 256)                         \
-                         : (ppt == 4 ? occ(k_raster_bwd<64, P, false, D, true, 4>, 64)                \
-                         : ppt == 1 ? occ(k_raster_bwd<64, P, false, D, true, 1>, 256)               \
-                                     : (batch == 64 ? occ(k_raster_bwd<64, P, false, D, true, 2>, 128) \
-                                                    : occ(k_raster_bwd<128, P, false, D, true, 2>, 128))))
+int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det, bool mask) {
+#define GS_OM(P, D, M) (ppt == 4 ? occ(k_raster_bwd<64, P, false, D, true, 4, M>, 64)                \
+                         : ppt == 1 ? occ(k_raster_bwd<64, P, false, D, true, 1, M>, 256)               \
+                                     : (batch == 64 ? occ(k_raster_bwd<64, P, false, D, true, 2, M>, 128) \
+                                                    : occ(k_raster_bwd<128, P, false, D, true, 2, M>, 128)))
+#define GS_OV(P, D) (aux ? occ(k_raster_bwd<32, P, true, D, true, 1>, 256) \
+                         : (mask ? GS_OM(P, D, true) : GS_OM(P, D, false)))
 #define GS_O2(P) (det ? GS_OV(P, true) : GS_OV(P, false))
   return prec == 0 ? GS_O2(0) : (prec == 1 ? GS_O2(1) : GS_O2(2));
 #undef GS_O2
 #undef GS_OV
+#undef GS_OM
 }
 
 int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, bool color,
                       int grid, cudaStream_t st) {
   if (a.total_tiles == 0) return 0;
   if (color && !persistent) return (int)cudaErrorInvalidValue;  // the colour-only variant is persistent
+  const bool mask = color && a.mask != nullptr;
 #define GS_F(P, D, S) fwd_dispatch<P, D, S>(a, batch, ppt, grid, st)
+#define GS_FC(P, D) \
+  if (mask) fwd_dispatch<P, D, true, true, true>(a, batch, ppt, grid, st); \
+  else fwd_dispatch<P, D, true, true>(a, batch, ppt, grid, st);
 #define GS_F2(P)                                   \
-  if (det) { if (color) fwd_dispatch<P, true, true, true>(a, batch, ppt, grid, st); \
-             else if (persistent) GS_F(P, true, true); else GS_F(P, true, false); } \
-  else { if (color) fwd_dispatch<P, false, true, true>(a, batch, ppt, grid, st); \
-         else if (persistent) GS_F(P, false, true); else GS_F(P, false, false); }
+  if (det) { if (color) { GS_FC(P, true) } else if (persistent) GS_F(P, true, true); else GS_F(P, true, false); } \
+  else { if (color) { GS_FC(P, false) } else if (persistent) GS_F(P, false, true); else GS_F(P, false, false); }
   if (prec == 0) { GS_F2(0) } else if (prec == 1) { GS_F2(1) } else { GS_F2(2) }
 #undef GS_F2
+#undef GS_FC
 #undef GS_F
   return (int)cudaGetLastError();
 }
@@ -565,7 +625,12 @@ int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool de
 int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, int ppt, int batch, bool det, bool persistent, int grid,
                       cudaStream_t st) {
   if (a.total_tiles == 0) return 0;
-#define GS_B(P, X, D, S) bwd_dispatch<P, X, D, S>(a, ppt, batch, grid, st)
+  const bool mask = !aux && a.mask != nullptr;
+#define GS_B(P, X, D, S)                                                                  \
+  do {                                                                                    \
+    if (mask) bwd_dispatch<P, X, D, S, (!X && S)>(a, ppt, batch, grid, st);               \
+    else bwd_dispatch<P, X, D, S>(a, ppt, batch, grid, st);                               \
+  } while (0)
 #define GS_B3(P, X)                                \
   if (det) { if (persistent) GS_B(P, X, true, true); else GS_B(P, X, true, false); } \
   else { if (persistent) GS_B(P, X, false, true); else GS_B(P, X, false, false); }

@@ -463,6 +463,22 @@ int launch_ranges(const uint2* sorted_pairs, const unsigned long long* total, ui
   return (int)cudaGetLastError();
 }
 
+namespace {
+__global__ void __launch_bounds__(256) k_tile_words(const uint2* ranges, uint32_t num_tiles, uint32_t* words) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles; t += gridDim.x * blockDim.x) {
+    const uint2 r = ranges[t];
+    words[t] = r.y > r.x ? (r.y - r.x + 31u) / 32u : 0u;
+  }
+}
+}  // namespace
+
+int launch_mask_offsets(const uint2* ranges, uint32_t num_tiles, uint32_t* words, uint32_t* mask_off, void* scratch,
+                        cudaStream_t st) {
+  if (num_tiles == 0) return 0;
+  k_tile_words<<<grid_for(num_tiles, 256, 148 * 8), 256, 0, st>>>(ranges, num_tiles, words);
+  return launch_scan(words, nullptr, mask_off, num_tiles, nullptr, nullptr, nullptr, scratch, st);
+}
+
 int launch_pair_values(const uint2* src, uint32_t* dst, const unsigned long long* n, uint64_t capacity,
                        cudaStream_t st) {
   k_pair_values<<<148 * 8, 256, 0, st>>>(src, dst, n, capacity);

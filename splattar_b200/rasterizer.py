@@ -17,7 +17,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import (BUF, FLAG_COLOR_ONLY, FLAG_DETERMINISTIC, FLAG_PERSISTENT, FLAG_TIGHT_BINNING, PREC, AdamConfig, Camera,
+from ._lib import (BUF, FLAG_COLOR_ONLY, FLAG_DETERMINISTIC, FLAG_PERSISTENT, FLAG_STORED_STATE, FLAG_TIGHT_BINNING, PREC,
+                   AdamConfig, Camera,
                    DensifyConfig, GsError, McmcConfig, RasterConfig, SceneInputC, StepConfig, check, lib)
 
 SH_FLOATS = 48
@@ -100,10 +101,11 @@ class Rasterizer:
     def __init__(self, capacity: int, width: int, height: int, max_entries: int = 0, *, max_views: int = 1,
                  max_pixels: int = 0, precision: str = "f32", deterministic: bool = False,
                  persistent: bool = False, color_only: bool = False, tight: bool = False, batch: int = 128,
-                 pixels_per_thread: int = 0):
+                 pixels_per_thread: int = 0, stored_state: bool = False):
         self._h = None
         flags = (FLAG_DETERMINISTIC if deterministic else 0) | (FLAG_PERSISTENT if persistent else 0) | (
-            FLAG_COLOR_ONLY if color_only else 0) | (FLAG_TIGHT_BINNING if tight else 0)
+            FLAG_COLOR_ONLY if color_only else 0) | (FLAG_TIGHT_BINNING if tight else 0) | (
+            FLAG_STORED_STATE if stored_state else 0)
         cfg = RasterConfig(capacity, width, height, max_views, max_pixels, max_entries, 16, batch, PREC[precision],
                            flags, pixels_per_thread)
         h = C.c_void_p()

@@ -51,10 +51,10 @@ def test_batched_forward_equals_per_view_forward():
         assert np.array_equal(rs.read("out_ncontrib", Pv), allnc[off:off + Pv])
 
 
-def _trainer(scene, cams, precision="f32", deterministic=False):
+def _trainer(scene, cams, precision="f32", deterministic=False, stored_state=False):
     P = sum(c.width * c.height for c in cams)
     r = Rasterizer(scene.n, 0, 0, 0, max_views=len(cams), max_pixels=P, precision=precision,
-                   deterministic=deterministic, color_only=True)
+                   deterministic=deterministic, color_only=True, stored_state=stored_state)
     r.upload_scene(scene_input(scene))
     tgt = np.random.default_rng(1).uniform(0, 1, (P, 4)).astype(np.float32)
     r.write("target", tgt.ravel())
@@ -224,3 +224,24 @@ def test_autotune_keeps_results():
     assert (shapes["bwd_batch"], shapes["bwd_pixels_per_thread"]) in ((64, 1), (64, 2), (128, 2), (64, 4))
     r.forward(rc, scene.n)
     assert np.array_equal(r.read("out_color", 4 * P), before)
+
+
+@pytest.mark.parametrize("deterministic", [True, False])
+def test_stored_state_backward_matches_recompute(deterministic):
+    """Contributor masks from the forward select exactly the entries the
+    recomputing backward would keep: identical parameters after three chosen
+    steps (bitwise in deterministic mode)."""
+    scene, cams = multi_view_setup(23, 500)
+    rc = [raster_camera(c, 3) for c in cams]
+    outs = []
+    for stored in (False, True):
+        r = _trainer(scene, cams, precision="f16", deterministic=deterministic, stored_state=stored)
+        for _ in range(3):
+            r.train_step(rc, scene.n, StepSettings(0.8, 0.2, AdamSettings(eps=1e-15), "chosen"))
+        r.check()
+        outs.append(_params(r, scene.n))
+    for k in outs[0]:
+        if deterministic:
+            assert np.array_equal(outs[0][k], outs[1][k]), k
+        else:
+            assert np.allclose(outs[0][k], outs[1][k], rtol=1e-5, atol=1e-6), k
