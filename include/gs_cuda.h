@@ -152,7 +152,8 @@ typedef enum {
   GS_BUF_V_SCALES = 37,
   GS_BUF_V_QUAT = 38,
   GS_BUF_V_OPACITY = 39,
-  GS_BUF_V_SH = 40
+  GS_BUF_V_SH = 40,
+  GS_BUF_NORMAL_LOSS = 41 /* double per view: sum over pixels of alpha (1 - n.N_d) of the last gs_loss_normal */
 } gs_buffer_id;
 
 typedef struct gs_rasterizer gs_rasterizer;
@@ -199,6 +200,30 @@ gs_status gs_last_error(gs_rasterizer* r, char* msg, size_t cap);
  * reference's own form (1-lambda)*L1 + lambda*(1-SSIM)/2 is w_l1 = 1-lambda,
  * w_ssim = lambda/2. */
 gs_status gs_loss_l1_ssim(gs_rasterizer* r, float w_l1, float w_ssim, void* stream);
+
+/* NormalLoss (first_attempt/crates/gs-train/src/normal_loss.rs,
+ * shaders/normal_loss.wgsl:52-145), for every view of the last forward (which
+ * must have written depth and normals, i.e. not the colour-only training
+ * step): with mean depth tbar = depth_acc/alpha (pixels with alpha below
+ * alpha_min are skipped; 0.2 in the reference), P = tbar * ray and
+ * N_d = normalize(dP/dx x dP/dy) facing the camera,
+ * L = lambda/(W*H) * sum_q alpha_q (1 - n_q . N_d), alpha and the orientation
+ * detached (the W*H division is NormalLoss::set_lambda's). Writes
+ * DL_DNORMAL and the depth-gradient channel DL_DCOLOR.w (rgb untouched; run
+ * after gs_loss_l1_ssim) and the per-view sums into GS_BUF_NORMAL_LOSS. */
+gs_status gs_loss_normal(gs_rasterizer* r, float lambda, float alpha_min, void* stream);
+
+/* Camera pose refinement (crates/gs-track/src/lib.rs:289-337), host-only:
+ * gs_camera_step_grad = camera_step_grad (the antisymmetric part of
+ * R^T dL/dR as a rotation gradient, then dL/dC; GS_ERR_NONFINITE for a
+ * non-finite input); gs_camera_adam6 = adam6 (betas 0.9/0.999, eps 1e-10,
+ * separate rotation and centre rates; t is the 1-based step);
+ * gs_camera_apply_step = apply_camera_step (q <- normalize(q * exp(-step[0..3])),
+ * C <- C - step[3..6]). */
+gs_status gs_camera_step_grad(const float grad_cam[16], const float quat[4], float out6[6]);
+gs_status gs_camera_adam6(float m[6], float v[6], uint32_t t, const float grad[6], float lr_rot, float lr_center,
+                          float step[6]);
+gs_status gs_camera_apply_step(gs_camera* cam, const float step[6]);
 
 /* Optimizer (first_attempt/crates/gs-train/src/optim.rs:50-242) over the five
  * classes the trainer registers (trainer.rs:757-761): pos (identity, 4 per

@@ -434,3 +434,56 @@ def mcmc_apply(raw: dict, opacity_act, pairs):
                 out[k][d] = 0
                 out[k][a] = 0
     return out
+
+
+def normal_loss(alpha, depth_acc, normal, W: int, H: int, focal: float, lam: float, alpha_min: float = 0.2):
+    """Restatement in float64 of the normal-consistency loss (first_attempt/
+    crates/gs-train/src/shaders/normal_loss.wgsl:52-145) for one view:
+    L = lam/(W·H) Σ_q α_q (1 − n̂_q·N_d(q)), α and the orientation sign
+    detached. Inputs per pixel (row-major): alpha (P,), depth_acc (P,),
+    normal (P,3). Returns (Σ α(1 − n̂·N_d), dL/dnormal (P,3), dL/ddepth_acc (P,))."""
+    a = np.asarray(alpha, np.float64).reshape(H, W)
+    d = np.asarray(depth_acc, np.float64).reshape(H, W)
+    nv = np.asarray(normal, np.float64).reshape(H, W, 3)
+    ys, xs = np.mgrid[0:H, 0:W]
+    ray = np.stack([(xs + 0.5 - W / 2) / focal, -(ys + 0.5 - H / 2) / focal, -np.ones_like(xs, np.float64)], -1)
+    tbar = np.where(a >= alpha_min, d / np.where(a > 0, a, 1), 0.0)
+    P = tbar[..., None] * ray
+    lam_px = lam / (W * H)
+    dl_dn = np.zeros((H, W, 3))
+    cpx = np.zeros((H, W, 3))
+    cpy = np.zeros((H, W, 3))
+    total = 0.0
+    for y in range(H - 1):
+        for x in range(W - 1):
+            if a[y, x] < alpha_min or a[y, x + 1] < alpha_min or a[y + 1, x] < alpha_min:
+                continue
+            p = P[y, x]
+            dpx, dpy = P[y, x + 1] - p, P[y + 1, x] - p
+            m = np.cross(dpx, dpy)
+            l2 = m @ m
+            if l2 < 1e-18:
+                continue
+            ln = np.sqrt(l2)
+            mh = m / ln
+            sign = -1.0 if mh @ p > 0 else 1.0
+            nd = sign * mh
+            av = nv[y, x]
+            la2 = av @ av
+            if la2 < 1e-18:
+                continue
+            la = np.sqrt(la2)
+            nh = av / la
+            aq = a[y, x]
+            total += (1 - nh @ nd) * aq
+            dl_dnd = -lam_px * aq * nh
+            dl_dnh = -lam_px * aq * nd
+            dl_dn[y, x] = (dl_dnh - nh * (nh @ dl_dnh)) / la
+            dl_dm = sign * (dl_dnd - mh * (mh @ dl_dnd)) / ln
+            cpx[y, x] = np.cross(dpy, dl_dm)
+            cpy[y, x] = np.cross(dl_dm, dpx)
+    acc = -cpx - cpy
+    acc[:, 1:] += cpx[:, :-1]
+    acc[1:, :] += cpy[:-1, :]
+    dd = np.where(a >= alpha_min, (ray * acc).sum(-1) / np.where(a > 0, a, 1), 0.0)
+    return total, dl_dn.reshape(-1, 3), dd.reshape(-1)

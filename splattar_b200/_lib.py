@@ -29,7 +29,7 @@ BUF = {
     "sorted_items": 19, "entry_count": 20, "loss": 21, "raw_pos": 22, "raw_scales": 23, "raw_quat": 24,
     "raw_opacity": 25, "raw_sh": 26, "rects": 27, "depth_keys": 28, "depth_order": 29,
     "grad_norm_sum": 30, "m_pos": 31, "m_scales": 32, "m_quat": 33, "m_opacity": 34, "m_sh": 35, "v_pos": 36,
-    "v_scales": 37, "v_quat": 38, "v_opacity": 39, "v_sh": 40,
+    "v_scales": 37, "v_quat": 38, "v_opacity": 39, "v_sh": 40, "normal_loss": 41,
 }
 
 
@@ -117,6 +117,10 @@ def lib():
         "gs_radix_sort_pairs_noalloc": [vp, vp, u64, u32, vp],
         "gs_exclusive_scan_u32": [vp, vp, u64, vp, vp],
         "gs_camera_rotation": [C.POINTER(Camera), C.POINTER(C.c_float)],
+        "gs_loss_normal": [vp, f32, f32, vp],
+        "gs_camera_step_grad": [C.POINTER(f32), C.POINTER(f32), C.POINTER(f32)],
+        "gs_camera_adam6": [C.POINTER(f32), C.POINTER(f32), u32, C.POINTER(f32), f32, f32, C.POINTER(f32)],
+        "gs_camera_apply_step": [C.POINTER(Camera), C.POINTER(f32)],
         "gs_mcmc_seed": [vp, u64, vp],
         "gs_mcmc_relocate": [vp, C.POINTER(McmcConfig), u32, vp],
         "gs_mcmc_stats": [vp, C.POINTER(u32), C.POINTER(u64), vp],
@@ -160,6 +164,7 @@ def exported_symbols() -> list[str]:
         "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_set_launch_shapes", "gs_binner_create",
         "gs_binner_destroy", "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_radix_sort_pairs_noalloc",
         "gs_exclusive_scan_u32",
-        "gs_camera_rotation", "gs_shutdown", "gs_mcmc_seed", "gs_mcmc_relocate", "gs_mcmc_stats", "gs_mcmc_noise",
+        "gs_camera_rotation", "gs_shutdown", "gs_loss_normal", "gs_camera_step_grad", "gs_camera_adam6",
+        "gs_camera_apply_step", "gs_mcmc_seed", "gs_mcmc_relocate", "gs_mcmc_stats", "gs_mcmc_noise",
         "gs_ply_write", "gs_ply_info", "gs_ply_read", "gs_rasterizer_save_ply",
         "gs_rasterizer_load_ply"]

@@ -95,6 +95,7 @@ struct gs_rasterizer {
   float* partials = nullptr;
   uint2* ranges = nullptr;
   int ent_in1 = 0;
+  double* normal_loss_sums = nullptr;  // per view: Σ α (1 − n̂·N_d) of the last gs_loss_normal
   // stored-state mode: contributor masks of the last colour-only forward
   uint32_t* mask = nullptr;
   uint32_t* mask_off = nullptr;
@@ -666,6 +667,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   ALLOC(r->dl_dnormal, P); ALLOC(r->target, P); ALLOC(r->out_nc, P);
   ALLOC(r->coef, P * 9);
   ALLOC(r->loss_sums, 2 * (size_t)c.max_views);
+  ALLOC(r->normal_loss_sums, (size_t)c.max_views);
   ALLOC(r->grad_geom, I * GG_STRIDE);
   ALLOC(r->grad_pos, N); ALLOC(r->grad_scales, N); ALLOC(r->grad_quat, N); ALLOC(r->grad_opacity, N);
   ALLOC(r->grad_sh, N * SH_FLOATS);
@@ -708,6 +710,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
                   r->accum_norm, r->dyn_dev, r->dens_flags, r->dens_slots, r->dens_tmp, r->views_dev,
                   r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off,
+                  r->normal_loss_sums,
                   r->mask_words,
                   r->scan_scratch, r->sort_scratch};
   for (void* p : ptrs)
@@ -815,6 +818,7 @@ static gs_status buffer_info(gs_rasterizer* r, gs_buffer_id id, void** p, size_t
     case GS_BUF_DEPTH_KEYS: *p = r->item_keys[0]; *bytes = 4 * I; break;
     case GS_BUF_DEPTH_ORDER: *p = r->item_vals[0]; *bytes = 4 * I; break;
     case GS_BUF_GRAD_NORM_SUM: *p = r->accum_norm; *bytes = 4 * N; break;
+    case GS_BUF_NORMAL_LOSS: *p = r->normal_loss_sums; *bytes = 8 * (size_t)r->max_views; break;
     case GS_BUF_M_POS: case GS_BUF_M_SCALES: case GS_BUF_M_QUAT: case GS_BUF_M_OPACITY: case GS_BUF_M_SH: {
       const int k = (int)id - (int)GS_BUF_M_POS;
       *p = r->mom1[k]; *bytes = 4 * N * WIDTH[k];
@@ -913,6 +917,84 @@ gs_status gs_loss_l1_ssim(gs_rasterizer* r, float w_l1, float w_ssim, void* stre
   cudaStream_t st = S(stream);
   TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * r->last_nv, st));
   return run_loss(r, r->last_views_dev, r->last_views_host, r->last_nv, w_l1, w_ssim, r->loss_sums, st);
+}
+
+gs_status gs_loss_normal(gs_rasterizer* r, float lambda, float alpha_min, void* stream) {
+  if (!r) return GS_ERR_INVALID_ARG;
+  if (!r->have_forward) return fail(r, GS_ERR_STATE, "normal loss needs a forward");
+  cudaStream_t st = S(stream);
+  uint64_t px = 0;
+  for (uint32_t v = 0; v < r->last_nv; ++v) px += (uint64_t)r->last_views_host[v].width * r->last_views_host[v].height;
+  TRY_CUDA(r, cudaMemsetAsync(r->normal_loss_sums, 0, sizeof(double) * r->last_nv, st));
+  NormalArgs a{};
+  a.views = r->last_views_dev; a.n_views = (int)r->last_nv; a.total_px = px;
+  a.color = r->out_color; a.aux = r->out_aux; a.normal = r->out_normal;
+  a.cp = r->coef; a.stride = r->max_pixels;  // the SSIM coefficient planes are free after the colour loss
+  a.dl_dnormal = r->dl_dnormal; a.dl_dcolor = r->dl_dcolor; a.loss = r->normal_loss_sums;
+  a.lambda = lambda; a.alpha_min = alpha_min;
+  TRY_LAUNCH(r, launch_normal_loss(a, st));
+  return GS_OK;
+}
+
+// ------------------------------------------------------ camera pose step
+// crates/gs-track/src/lib.rs:289-337: the Riemannian rotation gradient, one
+// Adam step over (rotation, centre) and the right-perturbation update.
+gs_status gs_camera_step_grad(const float grad_cam[16], const float quat[4], float out6[6]) {
+  if (!grad_cam || !quat || !out6) return GS_ERR_INVALID_ARG;
+  for (int k = 0; k < 12; ++k)
+    if (!std::isfinite(grad_cam[k])) return fail(nullptr, GS_ERR_NONFINITE, "non-finite camera gradient");
+  float R[9];
+  rotation_of(quat, R);  // column-major
+  // B = Rᵀ·A with A = dL/dR (column-major): B[c][r] = Σ_k R[r][k]·A[c][k] ... as columns
+  float B[9];
+  for (int c = 0; c < 3; ++c)
+    for (int rr = 0; rr < 3; ++rr) {
+      float acc = 0.f;
+      for (int k = 0; k < 3; ++k) acc += R[3 * rr + k] * grad_cam[3 * c + k];  // (Rᵀ)[rr][k] = R[k][rr] = col rr, row k
+      B[3 * c + rr] = acc;
+    }
+  out6[0] = B[3 * 1 + 2] - B[3 * 2 + 1];
+  out6[1] = B[3 * 2 + 0] - B[3 * 0 + 2];
+  out6[2] = B[3 * 0 + 1] - B[3 * 1 + 0];
+  out6[3] = grad_cam[9]; out6[4] = grad_cam[10]; out6[5] = grad_cam[11];
+  return GS_OK;
+}
+
+gs_status gs_camera_adam6(float m[6], float v[6], uint32_t t, const float grad[6], float lr_rot, float lr_center,
+                          float step[6]) {
+  if (!m || !v || !grad || !step || t == 0) return GS_ERR_INVALID_ARG;
+  float p1 = 1.f, p2 = 1.f;
+  for (uint32_t k = 0; k < t; ++k) { p1 *= 0.9f; p2 *= 0.999f; }
+  const float bc1 = 1.0f - p1, bc2 = 1.0f - p2;
+  for (int k = 0; k < 6; ++k) {
+    m[k] = 0.9f * m[k] + 0.1f * grad[k];
+    v[k] = 0.999f * v[k] + 0.001f * grad[k] * grad[k];
+    const float lr = k < 3 ? lr_rot : lr_center;
+    step[k] = lr * (m[k] / bc1) / (std::sqrt(v[k] / bc2) + 1e-10f);
+  }
+  return GS_OK;
+}
+
+gs_status gs_camera_apply_step(gs_camera* cam, const float step[6]) {
+  if (!cam || !step) return GS_ERR_INVALID_ARG;
+  // R' = R·exp([δ]×) with δ = −step[0..3]: q' = normalize(q · from_scaled_axis(δ)).
+  const float dx = -step[0], dy = -step[1], dz = -step[2];
+  const float ang = std::sqrt(dx * dx + dy * dy + dz * dz);
+  float e[4] = {0.f, 0.f, 0.f, 1.f};
+  if (ang != 0.f) {
+    const float s = std::sin(0.5f * ang) / ang;
+    e[0] = dx * s; e[1] = dy * s; e[2] = dz * s; e[3] = std::cos(0.5f * ang);
+  }
+  const float* q = cam->quat;
+  float o[4];
+  o[0] = q[3] * e[0] + q[0] * e[3] + q[1] * e[2] - q[2] * e[1];
+  o[1] = q[3] * e[1] - q[0] * e[2] + q[1] * e[3] + q[2] * e[0];
+  o[2] = q[3] * e[2] + q[0] * e[1] - q[1] * e[0] + q[2] * e[3];
+  o[3] = q[3] * e[3] - q[0] * e[0] - q[1] * e[1] - q[2] * e[2];
+  const float n = std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
+  for (int k = 0; k < 4; ++k) cam->quat[k] = o[k] / n;
+  cam->center[0] -= step[3]; cam->center[1] -= step[4]; cam->center[2] -= step[5];
+  return GS_OK;
 }
 
 gs_status gs_optimizer_init(gs_rasterizer* r, uint32_t n, void* stream) {

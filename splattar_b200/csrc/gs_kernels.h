@@ -185,6 +185,22 @@ struct SsimArgs {
 };
 int launch_ssim(const SsimArgs& a, cudaStream_t st);
 
+struct NormalArgs {
+  const ViewInfo* views;
+  int n_views;
+  uint64_t total_px;
+  const float4* color;     // alpha in .w
+  const float4* aux;       // depth_acc in .y
+  const float4* normal;
+  float* cp;               // 6 planes of `stride` floats (stencil coefficients)
+  uint64_t stride;
+  float4* dl_dnormal;
+  float4* dl_dcolor;       // .w written
+  double* loss;            // per view: Σ α (1 − n̂·N_d)
+  float lambda, alpha_min;
+};
+int launch_normal_loss(const NormalArgs& a, cudaStream_t st);
+
 int launch_adam_grad(const AdamClass& c, const float* grad, uint64_t n, int activation, float beta1, float beta2,
                      float eps, float bc1_inv, float bc2_inv, cudaStream_t st);
 int launch_accum_norm(const float4* grad_pos, float* accum, uint32_t n, cudaStream_t st);

@@ -14,6 +14,8 @@
 //     (the zero-padded symmetric window is self-adjoint) and combine with the
 //     L1 term into dL/dx (ssim.wgsl:130-143).
 // L = w_l1·mean|x−y| + w_ssim·mean(1−S) over pixels × rgb of each view.
+#include <algorithm>
+
 #include "gs_common.cuh"
 #include "gs_kernels.h"
 
@@ -235,7 +237,113 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
   a.dl_dcolor[pix] = make_float4(out[0], out[1], out[2], 0.f);
 }
 
+// ---- normal-consistency loss (first_attempt/crates/gs-train/src/shaders/normal_loss.wgsl) ----
+// Per pixel q with mean depth t̄ = depth_acc/α (0 below alpha_min): P(q) = t̄·ray(q),
+// N_d = ±normalize((P(q+x) − P(q)) × (P(q+y) − P(q))) facing the camera,
+// L = λ/(W·H) Σ α_q (1 − n̂_q·N_d) with α and the orientation sign detached.
+// pass 1 writes dL/dnormal and the stencil coefficients dL/d(dPx), dL/d(dPy);
+// pass 2 gathers the forward-difference adjoint into dL/d(depth_acc) = dl_dcolor.w.
+__device__ __forceinline__ int view_of(const NormalArgs& a, uint64_t i) {
+  int v = 0;
+  while (v + 1 < a.n_views && (long long)i >= __ldg(&a.views[v + 1].pix_base)) ++v;
+  return v;
+}
+__device__ __forceinline__ float3 ray_at(const ViewInfo* V, int x, int y) {
+  const float cx = (float)__ldg(&V->width) * 0.5f, cy = (float)__ldg(&V->height) * 0.5f, f = __ldg(&V->focal);
+  return make_float3(((float)x + 0.5f - cx) / f, -((float)y + 0.5f - cy) / f, -1.0f);
+}
+__device__ __forceinline__ float3 f3s(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 f3sub(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float f3dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 f3cross(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+__global__ void __launch_bounds__(256) k_normal_pass1(NormalArgs a) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.total_px;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    float* cp = a.cp;
+    for (int k = 0; k < 6; ++k) cp[(size_t)k * a.stride + i] = 0.f;
+    a.dl_dnormal[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (a.lambda == 0.f) continue;
+    const int v = view_of(a, i);
+    const ViewInfo* V = a.views + v;
+    const int W = __ldg(&V->width), H = __ldg(&V->height);
+    const uint64_t li = i - (uint64_t)__ldg(&V->pix_base);
+    const int x = (int)(li % (uint64_t)W), y = (int)(li / (uint64_t)W);
+    if (x + 1 >= W || y + 1 >= H) continue;
+    const uint64_t ix = i + 1, iy = i + (uint64_t)W;
+    const float aq = a.color[i].w, ax = a.color[ix].w, ay = a.color[iy].w;
+    if (aq < a.alpha_min || ax < a.alpha_min || ay < a.alpha_min) continue;
+    const float3 p = f3s(ray_at(V, x, y), a.aux[i].y / aq);
+    const float3 dpx = f3sub(f3s(ray_at(V, x + 1, y), a.aux[ix].y / ax), p);
+    const float3 dpy = f3sub(f3s(ray_at(V, x, y + 1), a.aux[iy].y / ay), p);
+    const float3 m = f3cross(dpx, dpy);
+    const float len2 = f3dot(m, m);
+    if (len2 < 1e-18f) continue;
+    const float len = sqrtf(len2);
+    const float3 mhat = f3s(m, 1.0f / len);
+    const float sign = f3dot(mhat, p) > 0.0f ? -1.0f : 1.0f;
+    const float3 nd = f3s(mhat, sign);
+    const float4 nv = a.normal[i];
+    const float3 av = make_float3(nv.x, nv.y, nv.z);
+    const float la2 = f3dot(av, av);
+    if (la2 < 1e-18f) continue;
+    const float la = sqrtf(la2);
+    const float3 nhat = f3s(av, 1.0f / la);
+    const float lam = a.lambda / ((float)W * (float)H);
+    atomicAdd(a.loss + v, (double)((1.0f - f3dot(nhat, nd)) * aq));
+    const float3 dl_dnd = f3s(nhat, -lam * aq);
+    const float3 dl_dnhat = f3s(nd, -lam * aq);
+    const float3 dl_da = f3s(f3sub(dl_dnhat, f3s(nhat, f3dot(nhat, dl_dnhat))), 1.0f / la);
+    a.dl_dnormal[i] = make_float4(dl_da.x, dl_da.y, dl_da.z, 0.f);
+    const float3 dl_dm = f3s(f3sub(dl_dnd, f3s(mhat, f3dot(mhat, dl_dnd))), sign / len);
+    const float3 cx3 = f3cross(dpy, dl_dm), cy3 = f3cross(dl_dm, dpx);
+    cp[0 * a.stride + i] = cx3.x; cp[1 * a.stride + i] = cx3.y; cp[2 * a.stride + i] = cx3.z;
+    cp[3 * a.stride + i] = cy3.x; cp[4 * a.stride + i] = cy3.y; cp[5 * a.stride + i] = cy3.z;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_normal_pass2(NormalArgs a) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.total_px;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    float4 c = a.dl_dcolor[i];
+    c.w = 0.f;
+    if (a.lambda != 0.f) {
+      const int v = view_of(a, i);
+      const ViewInfo* V = a.views + v;
+      const int W = __ldg(&V->width);
+      const uint64_t li = i - (uint64_t)__ldg(&V->pix_base);
+      const int x = (int)(li % (uint64_t)W), y = (int)(li / (uint64_t)W);
+      const float* cp = a.cp;
+      // Adjoint of the forward differences: the centre gives −cpx −cpy, the
+      // left neighbour's cpx and the upper neighbour's cpy give +.
+      float3 acc = make_float3(-cp[0 * a.stride + i] - cp[3 * a.stride + i],
+                               -cp[1 * a.stride + i] - cp[4 * a.stride + i],
+                               -cp[2 * a.stride + i] - cp[5 * a.stride + i]);
+      if (x > 0) {
+        acc.x += cp[0 * a.stride + i - 1]; acc.y += cp[1 * a.stride + i - 1]; acc.z += cp[2 * a.stride + i - 1];
+      }
+      if (y > 0) {
+        const uint64_t u = i - (uint64_t)W;
+        acc.x += cp[3 * a.stride + u]; acc.y += cp[4 * a.stride + u]; acc.z += cp[5 * a.stride + u];
+      }
+      const float aq = a.color[i].w;
+      if (aq >= a.alpha_min) c.w = f3dot(ray_at(V, x, y), acc) / aq;  // dL/d(depth_acc), α detached
+    }
+    a.dl_dcolor[i] = c;
+  }
+}
+
 }  // namespace
+
+int launch_normal_loss(const NormalArgs& a, cudaStream_t st) {
+  if (a.total_px == 0) return 0;
+  const int grid = (int)std::min<uint64_t>((a.total_px + 255) / 256, 148 * 16);
+  k_normal_pass1<<<grid, 256, 0, st>>>(a);
+  k_normal_pass2<<<grid, 256, 0, st>>>(a);
+  return (int)cudaGetLastError();
+}
 
 int launch_ssim(const SsimArgs& a_in, cudaStream_t st) {
   if (a_in.total_tiles16 == 0) return 0;

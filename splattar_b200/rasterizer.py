@@ -91,6 +91,7 @@ class SceneInput:
 _DTYPES = {
     "out_ncontrib": np.uint32, "ranges": np.uint32, "sorted_items": np.uint32, "entry_count": np.uint64,
     "loss": np.float64, "rects": np.uint32, "depth_keys": np.uint32, "depth_order": np.uint32,
+    "normal_loss": np.float64,
 }
 
 
@@ -234,6 +235,10 @@ class Rasterizer:
         arr = (C.c_uint32 * 4)(fwd_batch, fwd_pixels_per_thread, bwd_batch, bwd_pixels_per_thread)
         self._chk(lib().gs_set_launch_shapes(self._h, arr))
 
+    def loss_normal(self, lam: float, alpha_min: float = 0.2, stream: int = 0):
+        """NormalLoss::encode for every view of the last forward (writes dl_dnormal and dl_dcolor.w)."""
+        self._chk(lib().gs_loss_normal(self._h, lam, alpha_min, stream))
+
     def mcmc_seed(self, xorshift_state: int, stream: int = 0):
         self._chk(lib().gs_mcmc_seed(self._h, xorshift_state, stream))
 
@@ -335,6 +340,34 @@ class TileBinner:
         p, n = C.c_void_p(), C.c_size_t()
         check(lib().gs_binner_buffer(self._h, idx, C.byref(p), C.byref(n)))
         return p.value, n.value
+
+
+def camera_step_grad(grad_cam16, quat4) -> np.ndarray:
+    """camera_step_grad (crates/gs-track/src/lib.rs:289-307)."""
+    g = np.ascontiguousarray(grad_cam16, np.float32)
+    q = np.ascontiguousarray(quat4, np.float32)
+    out = np.zeros(6, np.float32)
+    f = C.POINTER(C.c_float)
+    check(lib().gs_camera_step_grad(g.ctypes.data_as(f), q.ctypes.data_as(f), out.ctypes.data_as(f)))
+    return out
+
+
+def camera_adam6(m, v, t: int, grad6, lr_rot: float, lr_center: float) -> np.ndarray:
+    """adam6 (lib.rs:310-328); m and v (float32 arrays of 6) are updated in place."""
+    g = np.ascontiguousarray(grad6, np.float32)
+    step = np.zeros(6, np.float32)
+    f = C.POINTER(C.c_float)
+    check(lib().gs_camera_adam6(m.ctypes.data_as(f), v.ctypes.data_as(f), t, g.ctypes.data_as(f), lr_rot, lr_center,
+                                step.ctypes.data_as(f)))
+    return step
+
+
+def camera_apply_step(cam: "RasterCamera", step6) -> "RasterCamera":
+    """apply_camera_step (lib.rs:330-337) on a copy of the camera."""
+    c = cam.c()
+    s = np.ascontiguousarray(step6, np.float32)
+    check(lib().gs_camera_apply_step(C.byref(c), s.ctypes.data_as(C.POINTER(C.c_float))))
+    return RasterCamera(tuple(c.center[:]), tuple(c.quat[:]), c.focal, cam.sh_degree, cam.width, cam.height)
 
 
 def write_ply(path: str, positions4, scales2, quats4, opacities, sh48):
