@@ -34,7 +34,7 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 
 struct Hit {
-  float ghat, u, v, t, inv_det;
+  float ghat, u, v, t, inv_det, q2, dy;
   bool ray;
 };
 
@@ -46,22 +46,41 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
+// The part of the hit test that depends on the pixel column only: a thread's
+// pixels share sx, so det, u·det and v·det are one FMA per pixel from these
+// partial sums, and the screen-space distance needs dy alone.
+struct ColPart {
+  float det0, un0, vn0, dx, dx2;
+};
+__device__ __forceinline__ ColPart col_part(const float4& r0, const float4& r1, const float4& r2, float sx,
+                                            float pxc) {
+  ColPart c;
+  c.det0 = fmaf(r0.x, sx, r0.z);
+  c.un0 = fmaf(r1.x, sx, r1.z);
+  c.vn0 = fmaf(r2.x, sx, r2.z);
+  c.dx = __fsub_rn(pxc, r1.w);
+  c.dx2 = __fmul_rn(c.dx, c.dx);
+  return c;
+}
+
 // raster_common.wgsl:69-95 on the record parameterisation, branch-free.
 // Written with explicit rounding intrinsics so the forward and backward
 // kernels compute bit-identical alphas. When the ray branch is unavailable
 // (|det| ≤ 1e-12 or t ≤ near) q_ray is +inf and u, v, t are unused.
-__device__ __forceinline__ Hit eval_hit(const float4& r0, const float4& r1, const float4& r2, float depth, float sx,
-                                        float sy, float pxc, float pyc) {
+// q2 = u² + v² (= 2·q_ray) is kept for the backward.
+__device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
+                                        float depth, float sy, float pyc) {
   Hit h;
-  const float det = fmaf(r0.x, sx, fmaf(r0.y, sy, r0.z));
+  const float det = fmaf(r0.y, sy, c.det0);
   const float inv = rcp_approx(det);
-  const float u = __fmul_rn(fmaf(r1.x, sx, fmaf(r1.y, sy, r1.z)), inv);
-  const float v = __fmul_rn(fmaf(r2.x, sx, fmaf(r2.y, sy, r2.z)), inv);
+  const float u = __fmul_rn(fmaf(r1.y, sy, c.un0), inv);
+  const float v = __fmul_rn(fmaf(r2.y, sy, c.vn0), inv);
   const float t = __fmul_rn(r0.w, inv);
   const bool ray_ok = fabsf(det) > 1e-12f && t > NEAR_DEPTH;
-  const float qr = ray_ok ? __fmul_rn(0.5f, fmaf(u, u, __fmul_rn(v, v))) : __int_as_float(0x7f800000);
-  const float dx = pxc - r1.w, dy = pyc - r2.w;
-  const float qs = fmaf(dx, dx, __fmul_rn(dy, dy));  // (dx²+dy²)/(2σ²) with σ² = 0.5
+  h.q2 = fmaf(u, u, __fmul_rn(v, v));
+  const float qr = ray_ok ? __fmul_rn(0.5f, h.q2) : __int_as_float(0x7f800000);
+  h.dy = __fsub_rn(pyc, r2.w);
+  const float qs = fmaf(h.dy, h.dy, c.dx2);  // (dx²+dy²)/(2σ²) with σ² = 0.5
   h.ray = qr <= qs;
   const float q = h.ray ? qr : qs;
   h.u = u; h.v = v; h.inv_det = inv;
@@ -214,10 +233,11 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(RasterArgs a) {
           const float4 r3 = s_r3[k];
           const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
           const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
+          const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
 #pragma unroll
           for (int p = 0; p < PPT; ++p) {
             if (done[p] || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
-            const Hit h = eval_hit(r0, r1, r2, r4.w, g.sx, g.sy[p], g.pxc, g.pyc[p]);
+            const Hit h = eval_hit(cp, r0, r1, r2, r4.w, g.sy[p], g.pyc[p]);
             const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
             if (alpha < ALPHA_SKIP) continue;
             const float w = T[p] * alpha;
@@ -300,13 +320,18 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
       continue;
     }
     const TileGeo<PPT> g = tile_geo<PPT>(a, tile);
-    float3 dlc[PPT], dln[PPT], suf_c[PPT], suf_n[PPT];
+    // Suffix sums of what lies behind the current entry: colour and normal
+    // enter only through their dot products with dL/dcolour and dL/dnormal,
+    // so those scalars are carried instead of the vectors.
+    float3 dlc[PPT], dln[PPT];
+    float suf_c[PPT], suf_n[PPT];
     float dld[PPT], wtot[PPT], wttot[PPT], T[PPT], suf_d[PPT], suf_w[PPT], suf_cw[PPT];
     uint32_t nc[PPT];
     uint32_t my_max = 0;
 #pragma unroll
     for (int p = 0; p < PPT; ++p) {
-      dlc[p] = dln[p] = suf_c[p] = suf_n[p] = make_float3(0.f, 0.f, 0.f);
+      dlc[p] = dln[p] = make_float3(0.f, 0.f, 0.f);
+      suf_c[p] = suf_n[p] = 0.f;
       dld[p] = wtot[p] = wttot[p] = suf_d[p] = suf_w[p] = suf_cw[p] = 0.f;
       T[p] = 1.f;
       nc[p] = 0;
@@ -428,10 +453,11 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
           if (AUX) { r4 = s_r4[k]; depth = r4.w; }
+          const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
 #pragma unroll
           for (int p = 0; p < PPT; ++p) {
             if (masks ? !bit[p] : (!(cidx < nc[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w)) continue;
-            const Hit h = eval_hit(r0, r1, r2, depth, g.sx, g.sy[p], g.pxc, g.pyc[p]);
+            const Hit h = eval_hit(cp, r0, r1, r2, depth, g.sy[p], g.pyc[p]);
             const float raw_alpha = __fmul_rn(r3.w, h.ghat);
             const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
             if (alpha < ALPHA_SKIP) continue;
@@ -439,8 +465,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
             const float inv_oma = rcp_approx(1.0f - alpha);
             const float t_before = T[p] * inv_oma;
             const float w = t_before * alpha;
-            float dl_dalpha = (dlc[p].x * r3.x + dlc[p].y * r3.y + dlc[p].z * r3.z) * t_before -
-                              (dlc[p].x * suf_c[p].x + dlc[p].y * suf_c[p].y + dlc[p].z * suf_c[p].z) * inv_oma;
+            const float dc = dlc[p].x * r3.x + dlc[p].y * r3.y + dlc[p].z * r3.z;
+            float dl_dalpha = dc * t_before - suf_c[p] * inv_oma;
             float dl_dt = 0.f;
             if (AUX) {
               const float t_hit = h.t;
@@ -452,39 +478,45 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(RasterArgs a) {
                 coef = a.lambda_dist * (2.0f * (t_hit * a_pre - b_pre) + 2.0f * (suf_d[p] - t_hit * suf_w[p]));
               }
               dl_dt = dld[p] * w + dt_dist;
-              dl_dalpha += dld[p] * (t_hit * t_before - suf_d[p] * inv_oma) +
-                           (dln[p].x * r4.x + dln[p].y * r4.y + dln[p].z * r4.z) * t_before -
-                           (dln[p].x * suf_n[p].x + dln[p].y * suf_n[p].y + dln[p].z * suf_n[p].z) * inv_oma +
-                           coef * t_before - suf_cw[p] * inv_oma;
+              const float dn = dln[p].x * r4.x + dln[p].y * r4.y + dln[p].z * r4.z;
+              dl_dalpha += dld[p] * (t_hit * t_before - suf_d[p] * inv_oma) + dn * t_before -
+                           suf_n[p] * inv_oma + coef * t_before - suf_cw[p] * inv_oma;
               suf_d[p] += t_hit * w;
-              suf_n[p].x += r4.x * w; suf_n[p].y += r4.y * w; suf_n[p].z += r4.z * w;
+              suf_n[p] += dn * w;
               suf_w[p] += w;
               suf_cw[p] += coef * w;
               gg[17] += dln[p].x * w; gg[18] += dln[p].y * w; gg[19] += dln[p].z * w;
             }
-            suf_c[p].x += r3.x * w; suf_c[p].y += r3.y * w; suf_c[p].z += r3.z * w;
+            suf_c[p] += dc * w;
             T[p] = t_before;
             gg[11] += dlc[p].x * w; gg[12] += dlc[p].y * w; gg[13] += dlc[p].z * w;
             if (raw_alpha <= ALPHA_CLAMP) {
-              gg[14] += dl_dalpha * h.ghat;
-              const float dl_dghat = dl_dalpha * r3.w;
+              // dL/dĝ·ĝ = dL/dα·o·ĝ; ray branch: ĝ = exp(−(u²+v²)/2) with
+              // u = (s·Bu)/det, v = (s·Bv)/det, det = s·M, so dL/d(s·Bu) = −u·K/det,
+              // dL/d(s·Bv) = −v·K/det and dL/ddet = (u²+v²)·K/det (− t·dL/dt/det
+              // through t = tn/det).
+              const float dg = dl_dalpha * h.ghat;
+              gg[14] += dg;
+              const float K = dg * r3.w;
               if (h.ray) {
-                const float gu = -h.u * h.ghat * dl_dghat;
-                const float gv = -h.v * h.ghat * dl_dghat;
-                const float gun = gu * h.inv_det, gvn = gv * h.inv_det;
-                const float gdet = -(h.u * gu + h.v * gv + (AUX ? h.t * dl_dt : 0.f)) * h.inv_det;
-                gg[0] += gdet * g.sx; gg[1] += gdet * g.sy[p]; gg[2] += gdet;
-                gg[3] += gun * g.sx; gg[4] += gun * g.sy[p]; gg[5] += gun;
-                gg[6] += gvn * g.sx; gg[7] += gvn * g.sy[p]; gg[8] += gvn;
+                const float Ki = K * h.inv_det;
+                const float gun = -h.u * Ki, gvn = -h.v * Ki;
+                float gdet = h.q2 * Ki;
+                if (AUX) gdet -= h.t * dl_dt * h.inv_det;
+                gg[1] += gdet * g.sy[p]; gg[2] += gdet;
+                gg[4] += gun * g.sy[p]; gg[5] += gun;
+                gg[7] += gvn * g.sy[p]; gg[8] += gvn;
                 if (AUX) gg[15] += dl_dt * h.inv_det;
               } else {
-                const float kk = h.ghat * dl_dghat / LOWPASS_SIGMA2;
-                gg[9] += (g.pxc - r1.w) * kk;
-                gg[10] += (g.pyc[p] - r2.w) * kk;
+                const float kk = K * (1.0f / LOWPASS_SIGMA2);
+                gg[9] += cp.dx * kk;
+                gg[10] += h.dy * kk;
                 if (AUX) gg[16] += dl_dt;
               }
             }
           }
+          // A thread's pixels share sx: the sx moments are sx times the plain sums.
+          gg[0] = gg[2] * g.sx; gg[3] = gg[5] * g.sx; gg[6] = gg[8] * g.sx;
         }
         if (__any_sync(FULL, contrib)) {
           float lo16[16];
