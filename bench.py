@@ -54,6 +54,8 @@ def parse(argv=None):
     p.add_argument("--stored-state", action="store_true",
                    help="stored-state backward: the forward records per-pixel contributor masks")
     p.add_argument("--entries-budget", type=float, default=96.0, help="tile-entry capacity per item")
+    p.add_argument("--tile", default="auto", choices=["auto", "8", "16", "32"],
+                   help="tile edge of the chosen form: autotuned over 8/16/32, or fixed (the plain form uses 16)")
     p.add_argument("--capacity-factor", type=float, default=1.25, help="densify cycle: capacity / initial surfels")
     p.add_argument("--entries-per-item", type=float, default=12.0, help="densify cycle: tile-entry budget per item")
     return p.parse_args(argv)
@@ -228,7 +230,12 @@ def run_ours(args, ws, rank, local):
     rast.write("target", target)
     rast.upload_scene(wl.surfels.scene_input())
     rast.optimizer_init(n)
-    tuned = rast.autotune(cams, n)
+    if args.tile == "auto":
+        tuned = rast.autotune_tiles(cams, n)
+    else:
+        rast.tile = int(args.tile)
+        tuned = dict(tile=int(args.tile), **rast.autotune(cams, n))
+    tile = rast.tile
     adam = AdamSettings(eps=1e-15)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
@@ -256,7 +263,14 @@ def run_ours(args, ws, rank, local):
     ms_chosen = timed(chosen, args.steps, args.warmup)
     clk = clocks.stop()
     E = rast.entry_count()
-    ms_plain = None if args.no_plain else timed(plain, max(2, args.steps // 2), args.warmup)
+    ms_plain = None
+    if not args.no_plain:  # the plain form at the reference's 16-pixel tiles
+        rast.tile = 16
+        ms_plain = timed(plain, max(2, args.steps // 2), args.warmup)
+        rast.tile = tile
+        if tile != 16:
+            rast.set_launch_shapes(tuned["fwd_batch"], tuned["fwd_pixels_per_thread"], tuned["bwd_batch"],
+                                   tuned["bwd_pixels_per_thread"])
 
     # End to end through the public API: pinned host targets in, loss out.
     tgt_host = torch.from_numpy(target.view(np.float32)).pin_memory()
@@ -282,7 +296,7 @@ def run_ours(args, ws, rank, local):
     # Stage timing (CUDA events between stages on the launch stream).
     prof = [rast.train_step_profiled(cams, n, chosen, sp) for _ in range(3)]
     stages = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
-    n_tiles = sum(((c.width + 15) // 16) * ((c.height + 15) // 16) for c in cams)
+    n_tiles = sum(((c.width + tile - 1) // tile) * ((c.height + tile - 1) // tile) for c in cams)
     rast.check(sp)
     result = dict(tuned=tuned, wl=wl, n=n, nv=nv, P=P, E=E, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
                   handle_bytes=int(free0 - free1),
@@ -409,7 +423,8 @@ def main():
             "pixels_per_step": P,
             "tile_entries_per_step": E,
             "form": "chosen: views batched per pass, persistent raster kernels, projection backward fused with Adam, "
-                    f"{args.precision} storage of SH and projected colour/normal, CUDA-graph replay",
+                    f"{args.precision} storage of SH and projected colour/normal, CUDA-graph replay, "
+                    f"{r['tuned']['tile']}-pixel tiles",
             "loss": "0.8*L1 + 0.2*(1-SSIM), 11x11 Gaussian sigma 1.5",
             "adam": "lr pos 1.6e-4 scales 5e-3 quat 1e-3 opacity 5e-2 sh 2.5e-3, betas 0.9/0.999, eps 1e-15",
             "l2": "inputs larger than L2 (params+optimizer state ~1.5 GB, tile entries ~%.1f GB)" % (E * 16 / 1e9),
@@ -421,7 +436,8 @@ def main():
         "mpix_per_s": round(steps_s * P / 1e6 * ws, 2),
         "plain": None if r["ms_plain"] is None else {
             "steps_per_s": round(aggregate_steps_per_s(r["ms_plain"], ws), 4), "ms_per_step": round(r["ms_plain"], 4),
-            "form": "views one at a time, FP32 records and SH, separate projection backward and Adam kernels"},
+            "form": "views one at a time, FP32 records and SH, separate projection backward and Adam kernels, "
+                    "16-pixel tiles"},
         "chosen_over_plain": None if r["ms_plain"] is None else round(r["ms_plain"] / r["ms_chosen"], 3),
         "e2e": {"value": round(aggregate_steps_per_s(r["ms_e2e"], ws), 4), "unit": "steps/s", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "ms_per_step": round(r["ms_e2e"], 4),

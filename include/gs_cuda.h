@@ -74,12 +74,13 @@ typedef struct {
   uint32_t max_views;
   uint64_t max_pixels;
   uint64_t max_entries;
-  uint32_t tile;        /* 16 only in this build */
-  uint32_t batch;       /* shared-memory staging depth of the raster kernels: 64, 128 or 256 (0 = 128) */
+  uint32_t tile;        /* tile edge in pixels: 8, 16 or 32 (0 = 16, the reference's); see gs_set_tile_size */
+  uint32_t batch;       /* shared-memory staging depth of the forward raster: 64, 128 or 256 (0 = 128) */
   uint32_t precision;   /* gs_precision */
   uint32_t flags;       /* GS_FLAG_* */
-  uint32_t pixels_per_thread; /* forward raster: vertically adjacent pixels per thread, 1 (any batch), 2 (batch
-                                 64/128) or 4 (batch 64); 0 = 1 */
+  uint32_t pixels_per_thread; /* forward raster: vertically adjacent pixels per thread; (batch, pixels_per_thread)
+                                 must be a forward shape built for the tile (table at gs_autotune); 0 = 1 (4 for
+                                 tile 32) */
 } gs_raster_config;
 
 /* RasterCamera (crates/gs-kernels/src/rasterizer.rs:34-41) plus the image
@@ -276,18 +277,48 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t n_view
 gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
                                  const gs_step_config* cfg, void* stream, float stage_ms[9], uint32_t* n_stages);
 
-/* Autotuner: times the forward raster over (batch, pixels per thread)
- * {(64,1),(128,1),(256,1),(64,2),(128,2),(64,4)} and the backward raster over
- * {(64,1),(64,2),(128,2),(64,4)} on these cameras (the batched form, tight
- * binning, the config's precision) and keeps the fastest for this handle.
- * out = {fwd batch, fwd pixels/thread, bwd batch, bwd pixels/thread}. Tile
- * size is fixed at 16 in this build. Blocking. */
+/* Raster launch shapes (staging batch, pixels per thread) built per tile size:
+ *   forward   tile 8:  ppt 1 or 2 with batch 64/128/256
+ *             tile 16: (64,1) (128,1) (256,1) (64,2) (128,2) (64,4)
+ *             tile 32: ppt 2 or 4 with batch 64/128/256
+ *   backward  tile 8:  (64,1) (64,2) (128,2)
+ *             tile 16: (64,1) (64,2) (128,2) (64,4)
+ *             tile 32: (64,4)
+ * (the backward with aux losses uses its own fixed shape).
+ *
+ * Autotuner (config-2 sweep of the batched form): at the handle's current
+ * tile size, times the forward (projection + binning + raster) over every
+ * forward shape and the colour-only backward raster over every backward
+ * shape on these cameras (tight binning, the config's precision) and keeps
+ * the fastest. out = {fwd batch, fwd pixels/thread, bwd batch, bwd
+ * pixels/thread}. Blocking. GS_ERR_CAPACITY if the tile entries exceed
+ * max_entries. */
 gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels, void* stream,
                       uint32_t out[4]);
+/* The same sweep over tile sizes 8, 16 and 32 (the reference fixes 16,
+ * crates/gs-kernels/src/rasterizer.rs:13): each tile size's shapes are timed
+ * as above, tile sizes whose entries exceed max_entries (or whose tile count
+ * exceeds the handle's tile budget) are skipped, and the fastest forward +
+ * backward total is kept. out = {tile, fwd batch, fwd pixels/thread, bwd
+ * batch, bwd pixels/thread}; times_ms (optional, 6 floats) = {fwd, bwd} ms
+ * per launch of the winning shapes for tiles 8, 16, 32 (-1 where skipped).
+ * The stored-state handle stays at tile 16. Blocking. */
+gs_status gs_autotune_tiles(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
+                            void* stream, uint32_t out[5], float times_ms[6]);
 /* Applies launch shapes (the layout of gs_autotune's out, e.g. a stored
- * result) without timing. Each pair must be one of the shapes gs_autotune
- * tries, else GS_ERR_INVALID_ARG and nothing changes. Host-only. */
+ * result) without timing. Each pair must be built for the handle's tile
+ * size (table above), else GS_ERR_INVALID_ARG and nothing changes. Host-only. */
 gs_status gs_set_launch_shapes(gs_rasterizer* r, const uint32_t shapes[4]);
+/* Changes the tile edge (8, 16 or 32 pixels) of later forwards. Launch
+ * shapes not built for the new size fall back to its first forward shape and
+ * its default backward shape ((128,2) where built, else (64,4)). Tile rects,
+ * entry lists, ranges and contributor indices of later forwards refer to the
+ * new tiling (the oracle's rect arithmetic takes the tile size as a
+ * parameter). GS_ERR_INVALID_ARG for other sizes, or for a tile other than
+ * 16 on a stored-state handle. Host-only. */
+gs_status gs_set_tile_size(gs_rasterizer* r, uint32_t tile);
+/* The handle's current tile edge in pixels (0 for a null handle). */
+uint32_t gs_tile_size(const gs_rasterizer* r);
 
 /* Densify/prune compaction (no reference counterpart; the reference only
  * relocates at fixed budget, trainer.rs:1558-1689): surfels whose mean

@@ -109,6 +109,9 @@ def lib():
         "gs_densify_prune": [vp, C.POINTER(DensifyConfig), u32, C.POINTER(u32), vp],
         "gs_autotune": [vp, C.POINTER(Camera), u32, u32, vp, C.POINTER(u32)],
         "gs_set_launch_shapes": [vp, C.POINTER(u32)],
+        "gs_autotune_tiles": [vp, C.POINTER(Camera), u32, u32, vp, C.POINTER(u32), C.POINTER(f32)],
+        "gs_set_tile_size": [vp, u32],
+        "gs_tile_size": [vp],
         "gs_binner_create": [u32, u64, u32, C.POINTER(vp)],
         "gs_binner_destroy": [vp],
         "gs_binner_encode": [vp, vp, vp, u32, u32, vp],
@@ -161,7 +164,7 @@ def exported_symbols() -> list[str]:
         "gs_rasterizer_forward", "gs_rasterizer_backward", "gs_rasterizer_buffer", "gs_rasterizer_view_offset",
         "gs_rasterizer_read", "gs_rasterizer_write", "gs_rasterizer_read_async", "gs_rasterizer_write_async",
         "gs_rasterizer_check", "gs_last_error", "gs_loss_l1_ssim", "gs_optimizer_init", "gs_optimizer_step",
-        "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_set_launch_shapes", "gs_binner_create",
+        "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_autotune_tiles", "gs_set_tile_size", "gs_tile_size", "gs_set_launch_shapes", "gs_binner_create",
         "gs_binner_destroy", "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_radix_sort_pairs_noalloc",
         "gs_exclusive_scan_u32",
         "gs_camera_rotation", "gs_shutdown", "gs_loss_normal", "gs_camera_step_grad", "gs_camera_adam6",

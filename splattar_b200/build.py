@@ -24,6 +24,8 @@ UNITS = {
     "gs_project.cu": ["--fmad=false"],
     "gs_project_bwd.cu": [],
     "gs_raster.cu": [],
+    "gs_raster_t8.cu": [],
+    "gs_raster_t32.cu": [],
     "gs_sort.cu": [],
     "gs_loss.cu": [],
     "gs_optim.cu": [],
@@ -31,7 +33,7 @@ UNITS = {
     "gs_mcmc.cu": [],
     "gs_ply.cpp": [],
 }
-HEADERS = ["gs_common.cuh", "gs_kernels.h", "gs_geom.cuh"]
+HEADERS = ["gs_common.cuh", "gs_kernels.h", "gs_geom.cuh", "gs_raster.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "-I", INCLUDE]
 

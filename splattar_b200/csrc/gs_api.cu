@@ -69,6 +69,7 @@ struct gs_rasterizer {
   bool det = false, persistent = false, color_only = false, tight = false;
   // Raster launch shapes (autotuned): staging batch and pixels per thread.
   int fwd_batch = 128, fwd_ppt = 1, bwd_batch = 128, bwd_ppt = 2;
+  int tile = 16;  // tile edge in pixels: 8, 16 (the reference's) or 32
   std::string err;
 
   // activated parameters (fp32) and the 16-bit SH copy
@@ -235,7 +236,7 @@ void rotation_of(const float q_in[4], float rot[9]) {
   rot[6] = xz + wy; rot[7] = yz - wx; rot[8] = 1.0f - (xx + yy);
 }
 
-ViewInfo make_view(const gs_camera& c) {
+ViewInfo make_view(const gs_camera& c, int tile) {
   ViewInfo v{};
   rotation_of(c.quat, v.rot);
   for (int k = 0; k < 3; ++k) v.center[k] = c.center[k];
@@ -244,8 +245,9 @@ ViewInfo make_view(const gs_camera& c) {
   v.height = (int)c.height;
   v.cx = (float)c.width * 0.5f;
   v.cy = (float)c.height * 0.5f;
-  v.tiles_x = (int)((c.width + TILE - 1) / TILE);
-  v.tiles_y = (int)((c.height + TILE - 1) / TILE);
+  v.tile = tile;
+  v.tiles_x = (int)((c.width + tile - 1) / tile);
+  v.tiles_y = (int)((c.height + tile - 1) / tile);
   v.sh_degree = (int)c.sh_degree;
   return v;
 }
@@ -264,7 +266,7 @@ gs_status set_views(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32
     const gs_camera& c = cams[v];
     if (c.width == 0 || c.height == 0 || !(c.focal > 0.f) || c.sh_degree > 3)
       return fail(r, GS_ERR_INVALID_ARG, "bad camera (size, focal or sh_degree)");
-    ViewInfo vi = make_view(c);
+    ViewInfo vi = make_view(c, r->tile);
     vi.pix_base = pix;
     vi.tile_base = tiles;
     r->views_batched[v] = vi;
@@ -284,6 +286,25 @@ gs_status upload_views(gs_rasterizer* r, cudaStream_t st) {
   TRY_CUDA(r, cudaMemcpyAsync(r->views_dev + r->max_views, r->views_single.data(), sizeof(ViewInfo) * nv,
                               cudaMemcpyHostToDevice, st));
   return GS_OK;
+}
+
+// Whether (batch, pixels per thread) is a raster shape built for `tile`.
+bool shape_listed(bool fwd, int tile, uint32_t batch, uint32_t ppt) {
+  const RasterShape* tab = nullptr;
+  const int n = fwd ? raster_fwd_shapes(tile, &tab) : raster_bwd_shapes(tile, &tab);
+  for (int k = 0; k < n; ++k)
+    if ((uint32_t)tab[k].batch == batch && (uint32_t)tab[k].ppt == ppt) return true;
+  return false;
+}
+
+// Backward shape for the handle's tile size: (128, 2) where it is built,
+// else the first shape built.
+void default_bwd_shape(gs_rasterizer* r) {
+  if (shape_listed(false, r->tile, 128, 2)) { r->bwd_batch = 128; r->bwd_ppt = 2; return; }
+  const RasterShape* tab = nullptr;
+  raster_bwd_shapes(r->tile, &tab);
+  r->bwd_batch = tab[0].batch;
+  r->bwd_ppt = tab[0].ppt;
 }
 
 const void* sh_for(gs_rasterizer* r, int prec) { return prec == 0 ? (const void*)r->sh : r->sh_half; }
@@ -336,7 +357,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ra.records = r->records;
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.tile_counter = r->words + 2;
-  r->mask_valid = r->stored_state && color && persistent;
+  r->mask_valid = r->stored_state && color && persistent && r->tile == 16;
   if (r->mask_valid) {
     TRY_LAUNCH(r, launch_mask_offsets(r->ranges, (uint32_t)tiles, r->mask_words, r->mask_off, r->scan_scratch, st));
     ra.mask = r->mask;
@@ -346,9 +367,10 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   int grid = tiles;
   if (persistent) {
     TRY_CUDA(r, cudaMemsetAsync(r->words + 2, 0, sizeof(uint32_t), st));
-    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(prec, batch, ppt, r->det, color, ra.mask != nullptr));
+    grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(r->tile, prec, batch, ppt, r->det, color,
+                                                              ra.mask != nullptr));
   }
-  TRY_LAUNCH(r, launch_raster_fwd(ra, prec, batch, ppt, r->det, persistent, color && persistent, grid, st));
+  TRY_LAUNCH(r, launch_raster_fwd(ra, r->tile, prec, batch, ppt, r->det, persistent, color && persistent, grid, st));
   mark(prof, 5, st);
   r->last_nv = nv; r->last_n = n; r->last_tiles = tiles; r->last_views_dev = vdev; r->last_views_host = vhost;
   r->have_forward = true;
@@ -379,10 +401,10 @@ gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t n
   int grid = tiles;
   if (persistent) {
     TRY_CUDA(r, cudaMemsetAsync(r->words + 3, 0, sizeof(uint32_t), st));
-    grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(prec, aux, r->bwd_ppt, r->bwd_batch, r->det,
+    grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(r->tile, prec, aux, r->bwd_ppt, r->bwd_batch, r->det,
                                                               ra.mask != nullptr));
   }
-  TRY_LAUNCH(r, launch_raster_bwd(ra, prec, aux, r->bwd_ppt, r->bwd_batch, r->det, persistent, grid, st));
+  TRY_LAUNCH(r, launch_raster_bwd(ra, r->tile, prec, aux, r->bwd_ppt, r->bwd_batch, r->det, persistent, grid, st));
   return GS_OK;
 }
 
@@ -581,15 +603,18 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   gs_raster_config c = *cfg_in;
   if (c.capacity == 0) return fail(nullptr, GS_ERR_INVALID_ARG, "capacity must be > 0");
   if (c.tile == 0) c.tile = 16;
-  if (c.tile != 16) return fail(nullptr, GS_ERR_INVALID_ARG, "only 16-pixel tiles are built");
+  if (c.tile != 8 && c.tile != 16 && c.tile != 32) return fail(nullptr, GS_ERR_INVALID_ARG, "tile must be 8, 16 or 32");
+  if (c.tile != 16 && (c.flags & GS_FLAG_STORED_STATE))
+    return fail(nullptr, GS_ERR_INVALID_ARG, "the stored-state backward is built for 16-pixel tiles");
   if (c.max_views == 0) c.max_views = 1;
   if (c.max_views > MAX_VIEWS_HARD) return fail(nullptr, GS_ERR_INVALID_ARG, "max_views > 64");
   if (c.batch == 0) c.batch = 128;
   if (c.batch != 64 && c.batch != 128 && c.batch != 256) return fail(nullptr, GS_ERR_INVALID_ARG, "batch must be 64/128/256");
-  if (c.pixels_per_thread == 0) c.pixels_per_thread = 1;
-  if (c.pixels_per_thread == 3 || c.pixels_per_thread > 4 || (c.pixels_per_thread == 2 && c.batch == 256) ||
-      (c.pixels_per_thread == 4 && c.batch != 64))
-    return fail(nullptr, GS_ERR_INVALID_ARG, "pixels_per_thread must be 1, 2 with batch <= 128, or 4 with batch 64");
+  if (c.pixels_per_thread == 0) c.pixels_per_thread = c.tile == 32 ? 4 : 1;
+  if (!shape_listed(true, (int)c.tile, c.batch, c.pixels_per_thread))
+    return fail(nullptr, GS_ERR_INVALID_ARG,
+                "(batch, pixels_per_thread) not built for this tile: tile 8 -> ppt 1/2 with batch 64/128/256; tile 16 -> "
+                "ppt 1 with batch 64/128/256, 2 with 64/128, 4 with 64; tile 32 -> ppt 2/4 with batch 64/128/256");
   if (c.precision > 2) return fail(nullptr, GS_ERR_INVALID_ARG, "bad precision");
   if (c.max_pixels == 0) c.max_pixels = (uint64_t)c.width * c.height * c.max_views;
   if (c.max_pixels == 0) return fail(nullptr, GS_ERR_INVALID_ARG, "width/height or max_pixels required");
@@ -616,6 +641,8 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   r->stored_state = (c.flags & GS_FLAG_STORED_STATE) != 0;
   r->fwd_batch = (int)c.batch;
   r->fwd_ppt = (int)c.pixels_per_thread;
+  r->tile = (int)c.tile;
+  default_bwd_shape(r);
   auto bail = [&](cudaError_t e, const char* what) {
     std::string m = std::string("allocation of ") + what + " failed: " + cudaGetErrorString(e);
     gs_rasterizer_destroy(r);
@@ -1115,21 +1142,12 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
   return GS_OK;
 }
 
-// Launch shapes (batch, pixels per thread) the raster dispatchers instantiate.
-static const int FWD_SHAPES[6][2] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}, {64, 4}};
-static const int BWD_SHAPES[4][2] = {{64, 1}, {64, 2}, {128, 2}, {64, 4}};
-
 gs_status gs_set_launch_shapes(gs_rasterizer* r, const uint32_t shapes[4]) {
   if (!r || !shapes) return GS_ERR_INVALID_ARG;
-  auto listed = [](const auto& tab, uint32_t b, uint32_t p) {
-    for (const auto& s : tab)
-      if ((uint32_t)s[0] == b && (uint32_t)s[1] == p) return true;
-    return false;
-  };
-  if (!listed(FWD_SHAPES, shapes[0], shapes[1]))
-    return fail(r, GS_ERR_INVALID_ARG, "gs_set_launch_shapes: unsupported forward (batch, pixels per thread)");
-  if (!listed(BWD_SHAPES, shapes[2], shapes[3]))
-    return fail(r, GS_ERR_INVALID_ARG, "gs_set_launch_shapes: unsupported backward (batch, pixels per thread)");
+  if (!shape_listed(true, r->tile, shapes[0], shapes[1]))
+    return fail(r, GS_ERR_INVALID_ARG, "gs_set_launch_shapes: forward (batch, pixels per thread) not built for this tile");
+  if (!shape_listed(false, r->tile, shapes[2], shapes[3]))
+    return fail(r, GS_ERR_INVALID_ARG, "gs_set_launch_shapes: backward (batch, pixels per thread) not built for this tile");
   r->fwd_batch = (int)shapes[0];
   r->fwd_ppt = (int)shapes[1];
   r->bwd_batch = (int)shapes[2];
@@ -1138,16 +1156,61 @@ gs_status gs_set_launch_shapes(gs_rasterizer* r, const uint32_t shapes[4]) {
   return GS_OK;
 }
 
-gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32_t n, void* stream, uint32_t out[4]) {
-  if (!r || !out) return GS_ERR_INVALID_ARG;
-  gs_status s = set_views(r, cams, nv, n);
-  if (s) return s;
-  cudaStream_t st = S(stream);
-  s = upload_views(r, st);
+gs_status gs_set_tile_size(gs_rasterizer* r, uint32_t tile) {
+  if (!r) return GS_ERR_INVALID_ARG;
+  if (tile != 8 && tile != 16 && tile != 32) return fail(r, GS_ERR_INVALID_ARG, "tile must be 8, 16 or 32");
+  if (tile != 16 && r->stored_state)
+    return fail(r, GS_ERR_INVALID_ARG, "the stored-state backward is built for 16-pixel tiles");
+  if ((int)tile == r->tile) return GS_OK;
+  r->tile = (int)tile;
+  if (!shape_listed(true, r->tile, r->fwd_batch, r->fwd_ppt)) {
+    const RasterShape* tab = nullptr;
+    raster_fwd_shapes(r->tile, &tab);
+    r->fwd_batch = tab[0].batch;
+    r->fwd_ppt = tab[0].ppt;
+  }
+  if (!shape_listed(false, r->tile, r->bwd_batch, r->bwd_ppt)) default_bwd_shape(r);
+  r->have_forward = false;  // tile lists of the last forward belong to the old tiling
+  r->mask_valid = false;
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
+  return GS_OK;
+}
+
+uint32_t gs_tile_size(const gs_rasterizer* r) { return r ? (uint32_t)r->tile : 0u; }
+
+namespace {
+
+// Times every forward and backward raster shape built for the handle's
+// current tile size on these views (forward = projection + binning + raster,
+// as the step runs it; backward = the colour-only backward raster) and
+// keeps the fastest of each. *fwd_ms / *bwd_ms receive the winners' times
+// (three launches each after one warm-up). *overflow is set, and nothing
+// timed, when the tile entries exceed max_entries at this tile size.
+gs_status tune_current_tile(gs_rasterizer* r, uint32_t nv, uint32_t n, cudaStream_t st, float* fwd_ms, float* bwd_ms,
+                            bool* overflow) {
+  *overflow = false;
+  gs_status s = upload_views(r, st);
   if (s) return s;
   int tiles = 0;
   for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
   const int prec = (int)r->cfg.precision;
+  // Entry budget check at this tile size (the entry guard's sticky bit is
+  // restored afterwards: an overflow here only rules the tile size out).
+  uint32_t err_before = 0;
+  TRY_CUDA(r, cudaMemcpyAsync(&err_before, r->words + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  s = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, nullptr,
+                  r->color_only);
+  if (s) return s;
+  unsigned long long total = 0;
+  TRY_CUDA(r, cudaMemcpyAsync(&total, r->entry_total, sizeof(total), cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaStreamSynchronize(st));
+  if (total > r->max_entries) {
+    TRY_CUDA(r, cudaMemcpyAsync(r->words + 1, &err_before, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    TRY_CUDA(r, cudaStreamSynchronize(st));
+    r->have_forward = false;
+    *overflow = true;
+    return GS_OK;
+  }
   cudaEvent_t e0, e1;
   TRY_CUDA(r, cudaEventCreate(&e0));
   TRY_CUDA(r, cudaEventCreate(&e1));
@@ -1159,48 +1222,104 @@ gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    return ms;
+    return ms / 3.f;
   };
-  // Forward: every (batch, pixels per thread) shape.
-  const auto& fshape = FWD_SHAPES;
+  const RasterShape* fshape = nullptr;
+  const int nf = raster_fwd_shapes(r->tile, &fshape);
   float best = 1e30f;
-  int bf = 1;
-  for (int k = 0; k < 6; ++k) {
-    r->fwd_batch = fshape[k][0];
-    r->fwd_ppt = fshape[k][1];
+  int bf = 0;
+  for (int k = 0; k < nf; ++k) {
+    r->fwd_batch = fshape[k].batch;
+    r->fwd_ppt = fshape[k].ppt;
     gs_status fs = GS_OK;
     const float ms = time_it([&] { fs = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true,
                                                     true, st, nullptr, r->color_only); });
     if (fs) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fs; }
     if (ms < best) { best = ms; bf = k; }
   }
-  r->fwd_batch = fshape[bf][0];
-  r->fwd_ppt = fshape[bf][1];
+  *fwd_ms = best;
+  r->fwd_batch = fshape[bf].batch;
+  r->fwd_ppt = fshape[bf].ppt;
   s = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true, true, st);
   if (!s) {
     TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
     s = run_loss(r, r->views_dev, r->views_batched.data(), nv, 0.8f, 0.2f, r->loss_sums, st);
   }
   if (s) { cudaEventDestroy(e0); cudaEventDestroy(e1); return s; }
-  // Backward (colour-only, as in the training step): every shape.
-  const auto& bshape = BWD_SHAPES;
+  const RasterShape* bshape = nullptr;
+  const int nb = raster_bwd_shapes(r->tile, &bshape);
   best = 1e30f;
-  int bb = 2;
-  for (int k = 0; k < 4; ++k) {
-    r->bwd_batch = bshape[k][0];
-    r->bwd_ppt = bshape[k][1];
+  int bb = 0;
+  for (int k = 0; k < nb; ++k) {
+    r->bwd_batch = bshape[k].batch;
+    r->bwd_ppt = bshape[k].ppt;
     gs_status bs = GS_OK;
     const float ms = time_it([&] { bs = run_backward_raster(r, r->views_dev, nv, tiles, n, prec, false, true, st); });
     if (bs) { cudaEventDestroy(e0); cudaEventDestroy(e1); return bs; }
     if (ms < best) { best = ms; bb = k; }
   }
-  r->bwd_batch = bshape[bb][0];
-  r->bwd_ppt = bshape[bb][1];
+  *bwd_ms = best;
+  r->bwd_batch = bshape[bb].batch;
+  r->bwd_ppt = bshape[bb].ppt;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return GS_OK;
+}
+
+}  // namespace
+
+gs_status gs_autotune(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32_t n, void* stream, uint32_t out[4]) {
+  if (!r || !out) return GS_ERR_INVALID_ARG;
+  gs_status s = set_views(r, cams, nv, n);
+  if (s) return s;
+  float fms = 0.f, bms = 0.f;
+  bool overflow = false;
+  s = tune_current_tile(r, nv, n, S(stream), &fms, &bms, &overflow);
+  if (s) return s;
+  if (overflow) return fail(r, GS_ERR_CAPACITY, "gs_autotune: tile entries exceed max_entries");
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
   out[0] = (uint32_t)r->fwd_batch; out[1] = (uint32_t)r->fwd_ppt;
   out[2] = (uint32_t)r->bwd_batch; out[3] = (uint32_t)r->bwd_ppt;
+  return GS_OK;
+}
+
+gs_status gs_autotune_tiles(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32_t n, void* stream,
+                            uint32_t out[5], float times_ms[6]) {
+  if (!r || !out) return GS_ERR_INVALID_ARG;
+  cudaStream_t st = S(stream);
+  const int tiles[3] = {8, 16, 32};
+  float best = 1e30f;
+  uint32_t best_cfg[5] = {0, 0, 0, 0, 0};
+  for (int i = 0; i < 3; ++i) {
+    if (times_ms) { times_ms[2 * i] = -1.f; times_ms[2 * i + 1] = -1.f; }
+    if (tiles[i] != 16 && r->stored_state) continue;
+    gs_status s = gs_set_tile_size(r, (uint32_t)tiles[i]);
+    if (s) return s;
+    s = set_views(r, cams, nv, n);
+    if (s == GS_ERR_CAPACITY) continue;  // the tile budget of the handle is too small for this tiling
+    if (s) return s;
+    float fms = 0.f, bms = 0.f;
+    bool overflow = false;
+    s = tune_current_tile(r, nv, n, st, &fms, &bms, &overflow);
+    if (s) return s;
+    if (overflow) continue;
+    if (times_ms) { times_ms[2 * i] = fms; times_ms[2 * i + 1] = bms; }
+    if (fms + bms < best) {
+      best = fms + bms;
+      best_cfg[0] = (uint32_t)tiles[i];
+      best_cfg[1] = (uint32_t)r->fwd_batch; best_cfg[2] = (uint32_t)r->fwd_ppt;
+      best_cfg[3] = (uint32_t)r->bwd_batch; best_cfg[4] = (uint32_t)r->bwd_ppt;
+    }
+  }
+  if (best_cfg[0] == 0) return fail(r, GS_ERR_CAPACITY, "gs_autotune_tiles: no tile size fits max_entries");
+  gs_status s = gs_set_tile_size(r, best_cfg[0]);
+  if (s) return s;
+  s = gs_set_launch_shapes(r, best_cfg + 1);
+  if (s) return s;
+  s = set_views(r, cams, nv, n);
+  if (s) return s;
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
+  for (int k = 0; k < 5; ++k) out[k] = best_cfg[k];
   return GS_OK;
 }
 

@@ -20,7 +20,7 @@ constexpr float ALPHA_SKIP = 0.0039215686f;  // 1/255
 constexpr float ALPHA_CLAMP = 0.995f;
 constexpr float T_TERMINATE = 1e-4f;
 constexpr float NEAR_DEPTH = 0.05f;
-constexpr int TILE = 16;
+constexpr int TILE = 16;  // the reference tile size (rasterizer.rs:13); 8 and 32 are also built
 constexpr int SH_FLOATS = 48;
 
 // Sticky device error word bits.
@@ -35,6 +35,7 @@ struct ViewInfo {
   float cx, cy;       // width/2, height/2
   int width, height;
   int tiles_x, tiles_y;
+  int tile;           // tile edge in pixels: 8, 16 or 32
   int tile_base;      // first global tile id of this view
   int sh_degree;
   long long pix_base; // first pixel of this view in per-pixel buffers

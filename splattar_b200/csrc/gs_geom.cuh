@@ -30,7 +30,7 @@ struct Cam {
   float3 r0, r1, r2;  // columns of R
   float3 C;
   float f, cx, cy;
-  int W, H, tiles_x, tiles_y, deg;
+  int W, H, tiles_x, tiles_y, tile, deg;
 };
 
 __device__ __forceinline__ Cam load_cam(const ViewInfo* views, int v) {
@@ -47,6 +47,7 @@ __device__ __forceinline__ Cam load_cam(const ViewInfo* views, int v) {
   c.H = __ldg(&V->height);
   c.tiles_x = __ldg(&V->tiles_x);
   c.tiles_y = __ldg(&V->tiles_y);
+  c.tile = __ldg(&V->tile);
   c.deg = __ldg(&V->sh_degree);
   return c;
 }

@@ -89,24 +89,36 @@ struct RasterArgs {
   float* partials;
   float lambda_dist;
   uint32_t* tile_counter;       // persistent kernels: zeroed before each launch
-  // Stored-state mode: per-pixel contributor bitmasks. Word w of pixel i
-  // (0..255, row-major in the tile) of tile t is mask[(mask_off[t] + w)·256 + i];
+  // Stored-state mode (16-pixel tiles): per-pixel contributor bitmasks. Word w of
+  // pixel i (0..255, row-major in the tile) of tile t is mask[(mask_off[t] + w)·256 + i];
   // bit b of word w is set when list position 32w + b composited into the pixel.
   uint32_t* mask;               // null: the backward re-evaluates every entry
   const uint32_t* mask_off;     // per tile, in 256-word groups
 };
+// Raster launch shapes built for a tile size (8, 16, 32): (staging batch,
+// pixels per thread). Returns the count and points *out at the table.
+struct RasterShape { int batch, ppt; };
+int raster_fwd_shapes(int tile, const RasterShape** out);
+int raster_bwd_shapes(int tile, const RasterShape** out);
 // Blocks per SM the raster kernels sustain (for persistent grids).
-int raster_fwd_occupancy(int prec, int batch, int ppt, bool det, bool color, bool mask);
-int raster_bwd_occupancy(int prec, bool aux, int ppt, int batch, bool det, bool mask);
+int raster_fwd_occupancy(int tile, int prec, int batch, int ppt, bool det, bool color, bool mask);
+int raster_bwd_occupancy(int tile, int prec, bool aux, int ppt, int batch, bool det, bool mask);
+// Per tile size (defined by the unit that instantiates it).
+template <int TS> int raster_fwd_occupancy_t(int prec, int batch, int ppt, bool det, bool color, bool mask);
+template <int TS> int raster_bwd_occupancy_t(int prec, bool aux, int ppt, int batch, bool det, bool mask);
+template <int TS> int launch_raster_fwd_t(const RasterArgs& a, int prec, int batch, int ppt, bool det,
+                                          bool persistent, bool color, int grid, cudaStream_t st);
+template <int TS> int launch_raster_bwd_t(const RasterArgs& a, int prec, bool aux, int ppt, int batch, bool det,
+                                          bool persistent, int grid, cudaStream_t st);
 
 int launch_project(const ProjectArgs& a, int prec, uint32_t n_views, cudaStream_t st);
 int launch_project_bwd(const ProjectBwdArgs& a, int prec, bool aux, cudaStream_t st);
 int prepare_project_kernels();
 int launch_project_bwd_adam(const ProjectBwdArgs& a, const AdamFusedArgs& opt, int prec, bool aux, cudaStream_t st);
-int launch_raster_fwd(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, bool color, int grid,
-                      cudaStream_t st);
-int launch_raster_bwd(const RasterArgs& a, int prec, bool aux, int ppt, int batch, bool det, bool persistent, int grid,
-                      cudaStream_t st);
+int launch_raster_fwd(const RasterArgs& a, int tile, int prec, int batch, int ppt, bool det, bool persistent,
+                      bool color, int grid, cudaStream_t st);
+int launch_raster_bwd(const RasterArgs& a, int tile, int prec, bool aux, int ppt, int batch, bool det,
+                      bool persistent, int grid, cudaStream_t st);
 
 // ---- sort / scan / binning (gs_sort.cu) ----
 // Scratch for the scan and the radix sort; sized by the caller through

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float py = k.cy - k.f * c.y / w;
   const float lu = sqrtf(dot3(tu, tu)), lv = sqrtf(dot3(tv, tv));
   const float r = fminf(3.0f * k.f * (lu + lv) / depth + 3.0f, 64.0f);
-  const float tf = (float)TILE;
+  const float tf = (float)k.tile;
   const float mx = (float)(k.tiles_x - 1), my = (float)(k.tiles_y - 1);
   const uint32_t x0 = (uint32_t)fminf(fmaxf((px - r) / tf, 0.0f), mx);
   const uint32_t y0 = (uint32_t)fminf(fmaxf((py - r) / tf, 0.0f), my);
@@ -137,11 +137,11 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float4 box = count ? alpha_bbox(k, c, tu, tv, px, py, o) : make_float4(1e30f, -1e30f, 1e30f, -1e30f);
   if (a.tight && count) {
     // Tight binning: only the tiles of the reference rect that the α-box
-    // overlaps. Tile t holds pixel centres [16t + 0.5, 16t + 15.5].
-    const float lim = 1e8f;
-    const float fx0 = ceilf((fminf(fmaxf(box.x, -lim), lim) - 15.5f) / tf);
+    // overlaps. Tile t holds pixel centres [T·t + 0.5, T·t + T − 0.5].
+    const float lim = 1e8f, hi = tf - 0.5f;
+    const float fx0 = ceilf((fminf(fmaxf(box.x, -lim), lim) - hi) / tf);
     const float fx1 = floorf((fminf(fmaxf(box.y, -lim), lim) - 0.5f) / tf);
-    const float fy0 = ceilf((fminf(fmaxf(box.z, -lim), lim) - 15.5f) / tf);
+    const float fy0 = ceilf((fminf(fmaxf(box.z, -lim), lim) - hi) / tf);
     const float fy1 = floorf((fminf(fmaxf(box.w, -lim), lim) - 0.5f) / tf);
     const int tx0 = max((int)x0, (int)fmaxf(fx0, -1.f)), tx1 = min((int)x1, (int)fminf(fx1, 1e7f));
     const int ty0 = max((int)y0, (int)fmaxf(fy0, -1.f)), ty1 = min((int)y1, (int)fminf(fy1, 1e7f));

@@ -1,0 +1,764 @@
+// Tile rasterizers: forward front-to-back compositing and its adjoint,
+// templated on the tile edge TS (8, 16 or 32 pixels; the reference uses 16,
+// crates/gs-kernels/src/rasterizer.rs:13). Each tile size is instantiated in
+// its own translation unit (gs_raster.cu, gs_raster_t8.cu, gs_raster_t32.cu).
+//
+// Forward: crates/gs-kernels/src/shaders/rasterize_fwd.wgsl:20-85 with the hit
+// test of raster_common.wgsl:69-95. One CTA per TS×TS tile, PPT pixels per
+// thread; the tile's depth-sorted entries are staged in shared
+// memory in batches and composited front to back in FP32. Beyond the
+// reference:
+//   * the whole CTA stops as soon as every pixel has terminated
+//     (__syncthreads_count);
+//   * while a batch is staged, entries whose α-box (the projection's
+//     conservative pixel box of α ≥ 1/255) misses the tile are dropped and
+//     the rest compacted, each keeping its original list position, and a
+//     pixel outside an entry's box skips it — exact, because such entries
+//     cannot reach the 1/255 threshold there;
+//   * the ray–splat intersection is evaluated from the precomputed record
+//     (three 3-term dot products, one reciprocal, one exp):
+//     ĝ = max(G_ray, G_screen) = exp(−min(q_ray, q_screen)).
+//
+// Backward: rasterize_bwd.wgsl:113-312. Each pixel walks its contributors in
+// reverse from the stored final transmittance and last-contributor index,
+// recovering T_before = T/(1−α), with suffix sums for colour (and depth,
+// normal and depth distortion when aux losses are on). Per-entry gradients
+// are taken with respect to the record fields (M, Bu, Bv, tn, px, py, colour,
+// opacity, …) and reduced across the warp by a 16-lane transpose reduction,
+// then across the CTA's 8 warps in a fixed order, then either added to the
+// per-surfel accumulator with one vector reduction per 4 components (default)
+// or stored per entry for an ordered reduction (deterministic mode).
+#pragma once
+
+#include <type_traits>
+
+#include "gs_common.cuh"
+#include "gs_kernels.h"
+
+namespace gs {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+struct Hit {
+  float ghat, u, v, t, inv_det, q2, dy;
+  bool ray;
+};
+
+// Approximate reciprocal (MUFU, ≤ 1 ulp): the only reciprocal either kernel
+// uses, so forward and backward stay bit-consistent.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// The part of the hit test that depends on the pixel column only: a thread's
+// pixels share sx, so det, u·det and v·det are one FMA per pixel from these
+// partial sums, and the screen-space distance needs dy alone.
+struct ColPart {
+  float det0, un0, vn0, dx, dx2;
+};
+__device__ __forceinline__ ColPart col_part(const float4& r0, const float4& r1, const float4& r2, float sx,
+                                            float pxc) {
+  ColPart c;
+  c.det0 = fmaf(r0.x, sx, r0.z);
+  c.un0 = fmaf(r1.x, sx, r1.z);
+  c.vn0 = fmaf(r2.x, sx, r2.z);
+  c.dx = __fsub_rn(pxc, r1.w);
+  c.dx2 = __fmul_rn(c.dx, c.dx);
+  return c;
+}
+
+// raster_common.wgsl:69-95 on the record parameterisation, branch-free.
+// Written with explicit rounding intrinsics so the forward and backward
+// kernels compute bit-identical alphas. When the ray branch is unavailable
+// (|det| ≤ 1e-12 or t ≤ near) q_ray is +inf and u, v, t are unused.
+// q2 = u² + v² (= 2·q_ray) is kept for the backward.
+__device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
+                                        float depth, float sy, float pyc) {
+  Hit h;
+  const float det = fmaf(r0.y, sy, c.det0);
+  const float inv = rcp_approx(det);
+  const float u = __fmul_rn(fmaf(r1.y, sy, c.un0), inv);
+  const float v = __fmul_rn(fmaf(r2.y, sy, c.vn0), inv);
+  const float t = __fmul_rn(r0.w, inv);
+  const bool ray_ok = fabsf(det) > 1e-12f && t > NEAR_DEPTH;
+  h.q2 = fmaf(u, u, __fmul_rn(v, v));
+  const float qr = ray_ok ? __fmul_rn(0.5f, h.q2) : __int_as_float(0x7f800000);
+  h.dy = __fsub_rn(pyc, r2.w);
+  const float qs = fmaf(h.dy, h.dy, c.dx2);  // (dx²+dy²)/(2σ²) with σ² = 0.5
+  h.ray = qr <= qs;
+  const float q = h.ray ? qr : qs;
+  h.u = u; h.v = v; h.inv_det = inv;
+  h.t = h.ray ? t : depth;
+  h.ghat = __expf(-q);
+  return h;
+}
+
+// Thread → pixel layout of a TS×TS tile with PPT vertically adjacent pixels
+// per thread: each warp owns a compact block of WC columns × WR·PPT rows
+// (16 × 2·PPT for tiles of 16 and 32, 8 × 4·PPT for tiles of 8), blocks laid
+// row-major over the tile.
+template <int TS, int PPT>
+struct Layout {
+  static constexpr int NT = TS * TS / PPT;       // threads per CTA
+  static constexpr int WC = TS < 16 ? TS : 16;   // pixel columns of a warp's block
+  static constexpr int WR = 32 / WC;             // thread rows of a warp's block
+  static constexpr int BPR = TS / WC;            // warp blocks across the tile
+  static_assert(NT % 32 == 0 && NT <= 1024, "whole warps, at most 1024 threads");
+  static __device__ __forceinline__ int col(int tid) { return ((tid >> 5) % BPR) * WC + (tid & 31) % WC; }
+  static __device__ __forceinline__ int row(int tid) { return (((tid >> 5) / BPR) * WR + (tid & 31) / WC) * PPT; }
+};
+
+template <int PPT>
+struct TileGeo {
+  int W, H;
+  long long row0;               // pix_base + y(p=0)·W + x
+  float pxc, sx;
+  float pyc[PPT], sy[PPT];
+  bool inside[PPT];
+  float bx0, bx1, by0, by1;     // pixel-centre extent of the tile's in-image pixels
+};
+
+template <int TS, int PPT>
+__device__ __forceinline__ TileGeo<PPT> tile_geo(const RasterArgs& a, int tile) {
+  TileGeo<PPT> g;
+  int v = 0;
+  while (v + 1 < a.n_views && tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
+  const ViewInfo* V = a.views + v;
+  const int tiles_x = __ldg(&V->tiles_x);
+  g.W = __ldg(&V->width);
+  g.H = __ldg(&V->height);
+  const int lt = tile - __ldg(&V->tile_base);
+  const int x0 = (lt % tiles_x) * TS, y0 = (lt / tiles_x) * TS;
+  const int x = x0 + Layout<TS, PPT>::col(threadIdx.x), yb = y0 + Layout<TS, PPT>::row(threadIdx.x);
+  const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
+  g.pxc = (float)x + 0.5f;
+  g.sx = -((g.pxc - cx) / f);  // s = −d
+#pragma unroll
+  for (int p = 0; p < PPT; ++p) {
+    g.pyc[p] = (float)(yb + p) + 0.5f;
+    g.sy[p] = (g.pyc[p] - cy) / f;
+    g.inside[p] = x < g.W && yb + p < g.H;
+  }
+  g.row0 = __ldg(&V->pix_base) + (long long)yb * g.W + x;
+  g.bx0 = (float)x0 + 0.5f;
+  g.bx1 = (float)(min(x0 + TS, g.W) - 1) + 0.5f;
+  g.by0 = (float)y0 + 0.5f;
+  g.by1 = (float)(min(y0 + TS, g.H) - 1) + 0.5f;
+  return g;
+}
+
+template <int PPT>
+__device__ __forceinline__ bool box_hits_tile(const float4& b, const TileGeo<PPT>& g) {
+  return b.x <= g.bx1 && b.y >= g.bx0 && b.z <= g.by1 && b.w >= g.by0;
+}
+
+// Compaction of one staging round: returns this thread's slot among the kept
+// entries of the round (valid when keep) and the number kept. Order is
+// preserved. Rounds alternate between two s_wcount rows, so the next round's
+// writes never meet a slower warp still reading this one.
+template <int NW>
+__device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(FULL, keep);
+  if (lane == 0) s_wcount[warp] = __popc(bal);
+  __syncthreads();
+  int off = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    const int c = s_wcount[w];
+    if (w < warp) off += c;
+    tot += c;
+  }
+  kept = tot;
+  return off + __popc(bal & lanemask_lt());
+}
+
+// COLOR: colour, alpha and final transmittance only (the training step's
+// loss reads nothing else); depth and normal are neither accumulated nor
+// written.
+template <int TS, int BATCH, int PREC, bool DET, bool PERSIST, int PPT, bool COLOR = false, bool MASK = false>
+__global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
+  static_assert(!MASK || COLOR, "contributor masks belong to the colour-only variant");
+  using L = Layout<TS, PPT>;
+  constexpr int NT = L::NT, NW = NT / 32, TP = TS * TS;
+  constexpr int ROUNDS = (BATCH + NT - 1) / NT;  // staging rounds per batch
+  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
+  __shared__ float4 s_r4[COLOR ? 1 : BATCH];
+  __shared__ int s_j[BATCH];
+  __shared__ int s_wcount[2][NW];
+  __shared__ int s_tile;
+  const int tid = threadIdx.x;
+  int tile = blockIdx.x;
+  for (;;) {
+    if (PERSIST) {
+      if (tid == 0) s_tile = (int)atomicAdd(a.tile_counter, 1u);
+      __syncthreads();
+      tile = s_tile;
+      if (tile >= a.total_tiles) return;
+    }
+    const TileGeo<PPT> g = tile_geo<TS, PPT>(a, tile);
+    const uint2 range = __ldg(&a.ranges[tile]);
+    float T[PPT], cr[PPT], cg[PPT], cb[PPT], aa[PPT], ad[PPT], nx[PPT], ny[PPT], nz[PPT];
+    uint32_t nc[PPT];
+    bool done[PPT];
+    bool tdone = true;
+    // Stored-state contributor masks (colour-only variant): the word being
+    // filled and its index, per pixel.
+    uint32_t mw[PPT];
+    int mi[PPT];
+    constexpr bool masks = MASK;
+    const size_t mbase = masks ? (size_t)__ldg(&a.mask_off[tile]) * TP : 0;
+    const int mpix = L::row(tid) * TS + L::col(tid);  // pixel p is mpix + p·TS
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) {
+      T[p] = 1.f; cr[p] = cg[p] = cb[p] = aa[p] = ad[p] = nx[p] = ny[p] = nz[p] = 0.f;
+      nc[p] = 0;
+      done[p] = !g.inside[p];
+      tdone &= done[p];
+      mw[p] = 0u;
+      mi[p] = 0;
+    }
+    for (uint32_t base = range.x; base < range.y; base += BATCH) {
+      if (__syncthreads_count(tdone) == NT) break;
+      const int count = (int)min((uint32_t)BATCH, range.y - base);
+      int kept = 0;
+#pragma unroll
+      for (int rd = 0; rd < ROUNDS; ++rd) {
+        const int j = rd * NT + tid;
+        bool keep = false;
+        uint32_t item = 0;
+        float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j < count) {
+          item = __ldg(&a.sorted_pairs[base + j].y);
+          if (DET) item = __ldg(&a.exp_item[item]);
+          bb = load_record_box<PREC>(a.records, item);
+          keep = box_hits_tile(bb, g);
+        }
+        int kr;
+        const int slot = kept + compact_slot<NW>(keep, s_wcount[rd & 1], kr);
+        if (keep) {
+          float4 r0, r1, r2, r3, r4;
+          load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
+          s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
+          if (!COLOR) s_r4[slot] = r4;
+          s_bb[slot] = bb;
+          s_j[slot] = j;
+        }
+        kept += kr;
+      }
+      __syncthreads();
+      if (!tdone) {
+        for (int k = 0; k < kept; ++k) {
+          const float4 bbk = s_bb[k];
+          if (g.pxc < bbk.x || g.pxc > bbk.y) continue;
+          const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
+          const float4 r3 = s_r3[k];
+          const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
+          const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
+          const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) {
+            if (done[p] || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
+            const Hit h = eval_hit(cp, r0, r1, r2, r4.w, g.sy[p], g.pyc[p]);
+            const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
+            if (alpha < ALPHA_SKIP) continue;
+            const float w = T[p] * alpha;
+            cr[p] += r3.x * w; cg[p] += r3.y * w; cb[p] += r3.z * w;
+            aa[p] += w;
+            if (!COLOR) {
+              ad[p] += h.t * w;
+              nx[p] += r4.x * w; ny[p] += r4.y * w; nz[p] += r4.z * w;
+            }
+            T[p] = __fmul_rn(T[p], 1.0f - alpha);
+            nc[p] = idx1;
+            if (masks) {
+              const uint32_t cidx = idx1 - 1u;
+              const int w = (int)(cidx >> 5);
+              if (w != mi[p]) {  // close the current word, zero the words skipped
+                uint32_t* m = a.mask + mbase + mpix + p * TS;
+                m[(size_t)mi[p] * TP] = mw[p];
+                for (int z = mi[p] + 1; z < w; ++z) m[(size_t)z * TP] = 0u;
+                mi[p] = w;
+                mw[p] = 0u;
+              }
+              mw[p] |= 1u << (cidx & 31u);
+            }
+            if (T[p] < T_TERMINATE) done[p] = true;
+          }
+          bool all = true;
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) all &= done[p];
+          if (all) { tdone = true; break; }
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) {
+      if (!g.inside[p]) continue;
+      const long long pix = g.row0 + (long long)p * g.W;
+      a.out_color[pix] = make_float4(cr[p], cg[p], cb[p], aa[p]);
+      if (masks && nc[p] > 0) a.mask[mbase + mpix + p * TS + (size_t)mi[p] * TP] = mw[p];
+      if (COLOR) {
+        a.out_aux[pix].x = T[p];
+      } else {
+        a.out_aux[pix] = make_float4(T[p], ad[p], 0.f, 0.f);
+        a.out_normal[pix] = make_float4(nx[p], ny[p], nz[p], 0.f);
+      }
+      a.out_nc[pix] = nc[p];
+    }
+    if (!PERSIST) return;
+    __syncthreads();
+  }
+}
+
+template <int TS, int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT, bool MASK = false>
+__global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
+  static_assert(!MASK || !AUX, "contributor masks cover the colour-only backward");
+  using L = Layout<TS, PPT>;
+  constexpr int NT = L::NT, NW = NT / 32, TP = TS * TS;
+  constexpr int ROUNDS = (BATCH + NT - 1) / NT;  // staging rounds per batch
+  constexpr int NG = AUX ? 32 : 16;  // reduced components per entry (AUX: 20 used)
+  constexpr int NQ = AUX ? 5 : 4;    // float4 groups per entry written out
+  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
+  __shared__ float4 s_r4[AUX ? BATCH : 1];
+  __shared__ uint32_t s_item[BATCH];
+  __shared__ uint32_t s_q[DET ? BATCH : 1];
+  __shared__ int s_j[BATCH];
+  __shared__ float s_part[NW][BATCH][NG];
+  __shared__ int s_wcount[2][NW];
+  __shared__ int s_tile, s_maxnc;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int tile = blockIdx.x;
+  for (;;) {
+    if (PERSIST) {
+      if (tid == 0) s_tile = (int)atomicAdd(a.tile_counter, 1u);
+      __syncthreads();
+      tile = s_tile;
+      if (tile >= a.total_tiles) return;
+    }
+    const uint2 range = __ldg(&a.ranges[tile]);
+    if (range.y <= range.x) {
+      if (!PERSIST) return;
+      __syncthreads();
+      continue;
+    }
+    const TileGeo<PPT> g = tile_geo<TS, PPT>(a, tile);
+    // Suffix sums of what lies behind the current entry: colour and normal
+    // enter only through their dot products with dL/dcolour and dL/dnormal,
+    // so those scalars are carried instead of the vectors.
+    float3 dlc[PPT], dln[PPT];
+    float suf_c[PPT], suf_n[PPT];
+    float dld[PPT], wtot[PPT], wttot[PPT], T[PPT], suf_d[PPT], suf_w[PPT], suf_cw[PPT];
+    uint32_t nc[PPT];
+    uint32_t my_max = 0;
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) {
+      dlc[p] = dln[p] = make_float3(0.f, 0.f, 0.f);
+      suf_c[p] = suf_n[p] = 0.f;
+      dld[p] = wtot[p] = wttot[p] = suf_d[p] = suf_w[p] = suf_cw[p] = 0.f;
+      T[p] = 1.f;
+      nc[p] = 0;
+      if (g.inside[p]) {
+        const long long pix = g.row0 + (long long)p * g.W;
+        const float4 gc = a.dl_dcolor[pix];
+        dlc[p] = make_float3(gc.x, gc.y, gc.z);
+        const float4 aux = a.out_aux[pix];
+        T[p] = aux.x;
+        nc[p] = a.out_nc[pix];
+        if (AUX) {
+          dld[p] = gc.w;
+          const float4 gn = a.dl_dnormal[pix];
+          dln[p] = make_float3(gn.x, gn.y, gn.z);
+          wtot[p] = a.out_color[pix].w;
+          wttot[p] = aux.y;
+        }
+      }
+      bool has_loss = g.inside[p] && (dlc[p].x != 0.f || dlc[p].y != 0.f || dlc[p].z != 0.f);
+      if (AUX) has_loss = g.inside[p] && (has_loss || dld[p] != 0.f || dln[p].x != 0.f || dln[p].y != 0.f ||
+                                          dln[p].z != 0.f || a.lambda_dist != 0.f);
+      if (!has_loss) nc[p] = 0;  // nc = 0 disables the pixel's walk
+      my_max = max(my_max, nc[p]);
+    }
+    // Entries at or past this warp's last contributor are skipped warp-wide.
+    const uint32_t warp_maxnc = __reduce_max_sync(FULL, my_max);
+    if (tid == 0) s_maxnc = 0;
+    __syncthreads();
+    if (my_max) atomicMax(&s_maxnc, (int)my_max);
+    __syncthreads();
+    const uint32_t maxnc = min((uint32_t)s_maxnc, range.y - range.x);
+    // Stored-state mode: contributor masks written by the forward; the word
+    // cached per pixel and its index (list positions are walked downwards).
+    constexpr bool masks = MASK;
+    const size_t mbase = masks ? (size_t)__ldg(&a.mask_off[tile]) * TP : 0;
+    const int mpix = L::row(tid) * TS + L::col(tid);
+    uint32_t cm[PPT];
+    int cw[PPT];
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) { cm[p] = 0u; cw[p] = -1; }
+
+    if (DET) {
+      // Entries past the tile's last contributor get zero partials.
+      for (uint32_t e = range.x + maxnc + tid; e < range.y; e += NT) {
+        const uint32_t q = __ldg(&a.sorted_pairs[e].y);
+        float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)q * GG_STRIDE);
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+
+    uint32_t hi = range.x + maxnc;
+    while (hi > range.x) {
+      const uint32_t lo = (hi - range.x > (uint32_t)BATCH) ? hi - BATCH : range.x;
+      const int count = (int)(hi - lo);
+      int kept = 0;
+#pragma unroll
+      for (int rd = 0; rd < ROUNDS; ++rd) {
+        const int j = rd * NT + tid;
+        bool keep = false;
+        uint32_t item = 0, q = 0;
+        float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j < count) {
+          item = __ldg(&a.sorted_pairs[lo + j].y);
+          q = item;
+          if (DET) item = __ldg(&a.exp_item[q]);
+          bb = load_record_box<PREC>(a.records, item);
+          keep = box_hits_tile(bb, g);
+          if (DET && !keep) {
+            float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)q * GG_STRIDE);
+#pragma unroll
+            for (int k = 0; k < NQ; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+        int kr;
+        const int slot = kept + compact_slot<NW>(keep, s_wcount[rd & 1], kr);
+        if (keep) {
+          float4 r0, r1, r2, r3, r4;
+          load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
+          s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
+          if (AUX) s_r4[slot] = r4;
+          s_bb[slot] = bb;
+          s_item[slot] = item;
+          if (DET) s_q[slot] = q;
+          s_j[slot] = j;
+        }
+        kept += kr;
+      }
+      __syncthreads();
+      for (int k = kept - 1; k >= 0; --k) {
+        const uint32_t cidx = lo - range.x + (uint32_t)s_j[k];
+        if (cidx >= warp_maxnc) {
+          if (lane < 16) s_part[warp][k][lane] = 0.f;
+          if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
+          continue;
+        }
+        bool bit[PPT];
+        bool anybit = false;
+        if (masks) {
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) {
+            bit[p] = false;
+            if (cidx < nc[p]) {
+              const int w = (int)(cidx >> 5);
+              if (w != cw[p]) {
+                cw[p] = w;
+                cm[p] = __ldg(a.mask + mbase + mpix + p * TS + (size_t)w * TP);
+              }
+              bit[p] = (cm[p] >> (cidx & 31u)) & 1u;
+              anybit |= bit[p];
+            }
+          }
+          if (!__any_sync(FULL, anybit)) {  // no pixel of this warp composited the entry
+            if (lane < 16) s_part[warp][k][lane] = 0.f;
+            continue;
+          }
+        }
+        const float4 bbk = s_bb[k];
+        float gg[NG];
+#pragma unroll
+        for (int c = 0; c < NG; ++c) gg[c] = 0.f;
+        bool contrib = false;
+        if (masks ? anybit : (g.pxc >= bbk.x && g.pxc <= bbk.y)) {
+          const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
+          float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
+          float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
+          if (AUX) { r4 = s_r4[k]; depth = r4.w; }
+          const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
+#pragma unroll
+          for (int p = 0; p < PPT; ++p) {
+            if (masks ? !bit[p] : (!(cidx < nc[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w)) continue;
+            const Hit h = eval_hit(cp, r0, r1, r2, depth, g.sy[p], g.pyc[p]);
+            const float raw_alpha = __fmul_rn(r3.w, h.ghat);
+            const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
+            if (alpha < ALPHA_SKIP) continue;
+            contrib = true;
+            const float inv_oma = rcp_approx(1.0f - alpha);
+            const float t_before = T[p] * inv_oma;
+            const float w = t_before * alpha;
+            const float dc = dlc[p].x * r3.x + dlc[p].y * r3.y + dlc[p].z * r3.z;
+            float dl_dalpha = dc * t_before - suf_c[p] * inv_oma;
+            float dl_dt = 0.f;
+            if (AUX) {
+              const float t_hit = h.t;
+              float dt_dist = 0.f, coef = 0.f;
+              if (a.lambda_dist != 0.f) {
+                const float a_pre = wtot[p] - suf_w[p] - w;
+                const float b_pre = wttot[p] - suf_d[p] - w * t_hit;
+                dt_dist = a.lambda_dist * 2.0f * w * (a_pre - suf_w[p]);
+                coef = a.lambda_dist * (2.0f * (t_hit * a_pre - b_pre) + 2.0f * (suf_d[p] - t_hit * suf_w[p]));
+              }
+              dl_dt = dld[p] * w + dt_dist;
+              const float dn = dln[p].x * r4.x + dln[p].y * r4.y + dln[p].z * r4.z;
+              dl_dalpha += dld[p] * (t_hit * t_before - suf_d[p] * inv_oma) + dn * t_before -
+                           suf_n[p] * inv_oma + coef * t_before - suf_cw[p] * inv_oma;
+              suf_d[p] += t_hit * w;
+              suf_n[p] += dn * w;
+              suf_w[p] += w;
+              suf_cw[p] += coef * w;
+              gg[17] += dln[p].x * w; gg[18] += dln[p].y * w; gg[19] += dln[p].z * w;
+            }
+            suf_c[p] += dc * w;
+            T[p] = t_before;
+            gg[11] += dlc[p].x * w; gg[12] += dlc[p].y * w; gg[13] += dlc[p].z * w;
+            if (raw_alpha <= ALPHA_CLAMP) {
+              // dL/dĝ·ĝ = dL/dα·o·ĝ; ray branch: ĝ = exp(−(u²+v²)/2) with
+              // u = (s·Bu)/det, v = (s·Bv)/det, det = s·M, so dL/d(s·Bu) = −u·K/det,
+              // dL/d(s·Bv) = −v·K/det and dL/ddet = (u²+v²)·K/det (− t·dL/dt/det
+              // through t = tn/det).
+              const float dg = dl_dalpha * h.ghat;
+              gg[14] += dg;
+              const float K = dg * r3.w;
+              if (h.ray) {
+                const float Ki = K * h.inv_det;
+                const float gun = -h.u * Ki, gvn = -h.v * Ki;
+                float gdet = h.q2 * Ki;
+                if (AUX) gdet -= h.t * dl_dt * h.inv_det;
+                gg[1] += gdet * g.sy[p]; gg[2] += gdet;
+                gg[4] += gun * g.sy[p]; gg[5] += gun;
+                gg[7] += gvn * g.sy[p]; gg[8] += gvn;
+                if (AUX) gg[15] += dl_dt * h.inv_det;
+              } else {
+                const float kk = K * (1.0f / LOWPASS_SIGMA2);
+                gg[9] += cp.dx * kk;
+                gg[10] += h.dy * kk;
+                if (AUX) gg[16] += dl_dt;
+              }
+            }
+          }
+          // A thread's pixels share sx: the sx moments are sx times the plain sums.
+          gg[0] = gg[2] * g.sx; gg[3] = gg[5] * g.sx; gg[6] = gg[8] * g.sx;
+        }
+        if (__any_sync(FULL, contrib)) {
+          float lo16[16];
+#pragma unroll
+          for (int c = 0; c < 16; ++c) lo16[c] = gg[c];
+          const float r = warp_reduce16(lo16);
+          if (!(lane & 1)) s_part[warp][k][lane >> 1] = r;
+          if (AUX) {
+            float hi16[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) hi16[c] = gg[16 + c];
+            const float r2 = warp_reduce16(hi16);
+            if (!(lane & 1)) s_part[warp][k][16 + (lane >> 1)] = r2;
+          }
+        } else {
+          if (lane < 16) s_part[warp][k][lane] = 0.f;
+          if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
+        }
+      }
+      __syncthreads();
+      // Cross-warp sum in fixed warp order, then one vector reduction (or
+      // one ordered store) per 4 components.
+      for (int w4 = tid; w4 < kept * NQ; w4 += NT) {
+        const int k = w4 / NQ, q4 = w4 % NQ;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+        for (int ww = 0; ww < NW; ++ww) {
+          s0 += s_part[ww][k][4 * q4]; s1 += s_part[ww][k][4 * q4 + 1];
+          s2 += s_part[ww][k][4 * q4 + 2]; s3 += s_part[ww][k][4 * q4 + 3];
+        }
+        if (DET) {
+          reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[q4] = make_float4(s0, s1, s2, s3);
+        } else if (s0 != 0.f || s1 != 0.f || s2 != 0.f || s3 != 0.f) {
+          red_add_v4(a.grad_geom + (size_t)s_item[k] * GG_STRIDE + 4 * q4, s0, s1, s2, s3);
+        }
+      }
+      __syncthreads();
+      hi = lo;
+    }
+    if (!PERSIST) return;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- dispatch
+// Launch shapes (staging batch, pixels per thread) built per tile size.
+// Forward: TS 8 → ppt 1/2 × batch 64/128/256; TS 16 → (64,1) (128,1) (256,1)
+// (64,2) (128,2) (64,4); TS 32 → ppt 2/4 × batch 64/128/256. Backward
+// without aux losses: TS 8 → (64,1) (64,2) (128,2); TS 16 → (64,1) (64,2)
+// (128,2) (64,4); TS 32 → (64,4). With aux losses: batch 32 at ppt 1 (TS 8,
+// 16) or 4 (TS 32). The backward's per-warp partial buffer NW·BATCH·NG floats
+// is static shared memory, which bounds the backward shapes.
+template <int TS, int PREC, bool DET, bool PERSIST, bool COLOR, bool MASK, typename F>
+bool fwd_shape(int batch, int ppt, F&& f) {
+#define GS_FWD(B, P)                                                                   \
+  if (batch == B && ppt == P) {                                                        \
+    f(k_raster_fwd<TS, B, PREC, DET, PERSIST, P, COLOR, MASK>, TS * TS / P);           \
+    return true;                                                                       \
+  }
+  if constexpr (TS == 8) {
+    GS_FWD(64, 1) GS_FWD(128, 1) GS_FWD(256, 1) GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(256, 2)
+  } else if constexpr (TS == 16) {
+    GS_FWD(64, 1) GS_FWD(128, 1) GS_FWD(256, 1) GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(64, 4)
+  } else {
+    GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(256, 2) GS_FWD(64, 4) GS_FWD(128, 4) GS_FWD(256, 4)
+  }
+#undef GS_FWD
+  return false;
+}
+
+template <int TS, int PREC, bool AUX, bool DET, bool PERSIST, bool MASK, typename F>
+bool bwd_shape(int batch, int ppt, F&& f) {
+#define GS_BWD(B, P)                                                                   \
+  if (batch == B && ppt == P) {                                                        \
+    f(k_raster_bwd<TS, B, PREC, AUX, DET, PERSIST, P, MASK>, TS * TS / P);             \
+    return true;                                                                       \
+  }
+  if constexpr (AUX) {
+    if constexpr (TS == 32) {
+      GS_BWD(32, 4)
+    } else {
+      GS_BWD(32, 1)
+    }
+  } else if constexpr (TS == 8) {
+    GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2)
+  } else if constexpr (TS == 16) {
+    GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2) GS_BWD(64, 4)
+  } else {
+    GS_BWD(64, 4)
+  }
+#undef GS_BWD
+  return false;
+}
+
+template <int V>
+using IC = std::integral_constant<int, V>;
+
+template <typename G>
+bool by_prec(int prec, G&& g) {
+  return prec == 0 ? g(IC<0>{}) : prec == 1 ? g(IC<1>{}) : g(IC<2>{});
+}
+
+// Calls f(kernel, threads) with the forward kernel of these options, or
+// returns false when the combination is not built. Contributor masks exist
+// for TS 16 only; the colour-only variant is persistent.
+template <int TS, typename F>
+bool fwd_kernel(int prec, int batch, int ppt, bool det, bool persistent, bool color, bool mask, F&& f) {
+  return by_prec(prec, [&](auto pc) -> bool {
+    constexpr int P = decltype(pc)::value;
+    if (color) {
+      if (!persistent) return false;
+      if (mask) {
+        if constexpr (TS == 16) {
+          return det ? fwd_shape<TS, P, true, true, true, true>(batch, ppt, f)
+                     : fwd_shape<TS, P, false, true, true, true>(batch, ppt, f);
+        } else {
+          return false;
+        }
+      }
+      return det ? fwd_shape<TS, P, true, true, true, false>(batch, ppt, f)
+                 : fwd_shape<TS, P, false, true, true, false>(batch, ppt, f);
+    }
+    if (det) return persistent ? fwd_shape<TS, P, true, true, false, false>(batch, ppt, f)
+                               : fwd_shape<TS, P, true, false, false, false>(batch, ppt, f);
+    return persistent ? fwd_shape<TS, P, false, true, false, false>(batch, ppt, f)
+                      : fwd_shape<TS, P, false, false, false, false>(batch, ppt, f);
+  });
+}
+
+template <int TS, typename F>
+bool bwd_kernel(int prec, bool aux, int batch, int ppt, bool det, bool persistent, bool mask, F&& f) {
+  if (aux) {  // one shape per tile size with aux losses
+    batch = 32;
+    ppt = TS == 32 ? 4 : 1;
+  }
+  return by_prec(prec, [&](auto pc) -> bool {
+    constexpr int P = decltype(pc)::value;
+    if (aux) {
+      if (mask) return false;
+      if (det) return persistent ? bwd_shape<TS, P, true, true, true, false>(batch, ppt, f)
+                                 : bwd_shape<TS, P, true, true, false, false>(batch, ppt, f);
+      return persistent ? bwd_shape<TS, P, true, false, true, false>(batch, ppt, f)
+                        : bwd_shape<TS, P, true, false, false, false>(batch, ppt, f);
+    }
+    if (mask) {
+      if constexpr (TS == 16) {
+        if (!persistent) return false;
+        return det ? bwd_shape<TS, P, false, true, true, true>(batch, ppt, f)
+                   : bwd_shape<TS, P, false, false, true, true>(batch, ppt, f);
+      } else {
+        return false;
+      }
+    }
+    if (det) return persistent ? bwd_shape<TS, P, false, true, true, false>(batch, ppt, f)
+                               : bwd_shape<TS, P, false, true, false, false>(batch, ppt, f);
+    return persistent ? bwd_shape<TS, P, false, false, true, false>(batch, ppt, f)
+                      : bwd_shape<TS, P, false, false, false, false>(batch, ppt, f);
+  });
+}
+
+template <typename K>
+int occupancy_of(K kernel, int threads) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess) return 1;
+  return n < 1 ? 1 : n;
+}
+
+template <int TS>
+int raster_fwd_occupancy_t(int prec, int batch, int ppt, bool det, bool color, bool mask) {
+  int n = 1;
+  fwd_kernel<TS>(prec, batch, ppt, det, true, color, mask, [&](auto k, int threads) { n = occupancy_of(k, threads); });
+  return n;
+}
+
+template <int TS>
+int raster_bwd_occupancy_t(int prec, bool aux, int ppt, int batch, bool det, bool mask) {
+  int n = 1;
+  bwd_kernel<TS>(prec, aux, batch, ppt, det, true, mask, [&](auto k, int threads) { n = occupancy_of(k, threads); });
+  return n;
+}
+
+template <int TS>
+int launch_raster_fwd_t(const RasterArgs& a, int prec, int batch, int ppt, bool det, bool persistent, bool color,
+                        int grid, cudaStream_t st) {
+  if (a.total_tiles == 0) return 0;
+  const bool mask = color && a.mask != nullptr;
+  const bool ok = fwd_kernel<TS>(prec, batch, ppt, det, persistent, color, mask,
+                                 [&](auto k, int threads) { k<<<grid, threads, 0, st>>>(a); });
+  if (!ok) return (int)cudaErrorInvalidValue;
+  return (int)cudaGetLastError();
+}
+
+template <int TS>
+int launch_raster_bwd_t(const RasterArgs& a, int prec, bool aux, int ppt, int batch, bool det, bool persistent,
+                        int grid, cudaStream_t st) {
+  if (a.total_tiles == 0) return 0;
+  const bool mask = !aux && a.mask != nullptr;
+  const bool ok = bwd_kernel<TS>(prec, aux, batch, ppt, det, persistent, mask,
+                                 [&](auto k, int threads) { k<<<grid, threads, 0, st>>>(a); });
+  if (!ok) return (int)cudaErrorInvalidValue;
+  return (int)cudaGetLastError();
+}
+
+// Explicit instantiation of one tile size's launchers (one translation unit each).
+#define GS_RASTER_INSTANTIATE(TS)                                                                             \
+  template int raster_fwd_occupancy_t<TS>(int, int, int, bool, bool, bool);                                  \
+  template int raster_bwd_occupancy_t<TS>(int, bool, int, int, bool, bool);                                  \
+  template int launch_raster_fwd_t<TS>(const RasterArgs&, int, int, int, bool, bool, bool, int, cudaStream_t); \
+  template int launch_raster_bwd_t<TS>(const RasterArgs&, int, bool, int, int, bool, bool, int, cudaStream_t);
+
+}  // namespace gs

@@ -102,12 +102,12 @@ class Rasterizer:
     def __init__(self, capacity: int, width: int, height: int, max_entries: int = 0, *, max_views: int = 1,
                  max_pixels: int = 0, precision: str = "f32", deterministic: bool = False,
                  persistent: bool = False, color_only: bool = False, tight: bool = False, batch: int = 128,
-                 pixels_per_thread: int = 0, stored_state: bool = False):
+                 pixels_per_thread: int = 0, stored_state: bool = False, tile: int = 16):
         self._h = None
         flags = (FLAG_DETERMINISTIC if deterministic else 0) | (FLAG_PERSISTENT if persistent else 0) | (
             FLAG_COLOR_ONLY if color_only else 0) | (FLAG_TIGHT_BINNING if tight else 0) | (
             FLAG_STORED_STATE if stored_state else 0)
-        cfg = RasterConfig(capacity, width, height, max_views, max_pixels, max_entries, 16, batch, PREC[precision],
+        cfg = RasterConfig(capacity, width, height, max_views, max_pixels, max_entries, tile, batch, PREC[precision],
                            flags, pixels_per_thread)
         h = C.c_void_p()
         check(lib().gs_rasterizer_create(C.byref(cfg), C.byref(h)))
@@ -228,6 +228,25 @@ class Rasterizer:
         self._chk(lib().gs_autotune(self._h, cams, len(cams), num_surfels, stream, out))
         return {"fwd_batch": out[0], "fwd_pixels_per_thread": out[1], "bwd_batch": out[2],
                 "bwd_pixels_per_thread": out[3]}
+
+    def autotune_tiles(self, cameras, num_surfels: int, stream: int = 0) -> dict:
+        """Time every tile size (8, 16, 32) with each of its raster launch shapes and keep the fastest."""
+        cams = camera_array(cameras)
+        out = (C.c_uint32 * 5)()
+        times = (C.c_float * 6)()
+        self._chk(lib().gs_autotune_tiles(self._h, cams, len(cams), num_surfels, stream, out, times))
+        per_tile = {t: (None if times[2 * i] < 0 else {"fwd_ms": float(times[2 * i]), "bwd_ms": float(times[2 * i + 1])})
+                    for i, t in enumerate((8, 16, 32))}
+        return {"tile": out[0], "fwd_batch": out[1], "fwd_pixels_per_thread": out[2], "bwd_batch": out[3],
+                "bwd_pixels_per_thread": out[4], "per_tile": per_tile}
+
+    @property
+    def tile(self) -> int:
+        return int(lib().gs_tile_size(self._h))
+
+    @tile.setter
+    def tile(self, t: int):
+        self._chk(lib().gs_set_tile_size(self._h, t))
 
     def set_launch_shapes(self, fwd_batch: int, fwd_pixels_per_thread: int, bwd_batch: int,
                           bwd_pixels_per_thread: int):

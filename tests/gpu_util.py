@@ -32,7 +32,10 @@ def f32_cam(cam: oracle.Camera) -> oracle.Camera:
 def forward(scene, cam, rast=None, **kw):
     n = scene.n
     if rast is None:
-        rast = Rasterizer(n, cam.width, cam.height, n * 64, **kw)
+        # 64 entries per surfel at 16-pixel tiles (the reference trainer's
+        # budget), scaled by the tile-count ratio for smaller tiles.
+        tile = kw.get("tile", 16)
+        rast = Rasterizer(n, cam.width, cam.height, kw.pop("max_entries", n * 64 * max(1, (16 // tile) ** 2)), **kw)
     rast.upload_scene(scene_input(scene))
     rast.forward(raster_camera(cam, scene.sh_degree), n)
     rast.check()
