@@ -279,11 +279,11 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
 
 /* Raster launch shapes (staging batch, pixels per thread) built per tile size:
  *   forward   tile 8:  ppt 1 or 2 with batch 64/128/256
- *             tile 16: (64,1) (128,1) (256,1) (64,2) (128,2) (64,4)
- *             tile 32: ppt 2 or 4 with batch 64/128/256
+ *             tile 16: (64,1) (128,1) (256,1) (64,2) (128,2) (64,4) (64,8) (128,8)
+ *             tile 32: ppt 2 or 4 with batch 64/128/256, and (128,8)
  *   backward  tile 8:  (64,1) (64,2) (128,2)
- *             tile 16: (64,1) (64,2) (128,2) (64,4)
- *             tile 32: (64,4)
+ *             tile 16: (64,1) (64,2) (128,2) (64,4) (64,8) (128,8)
+ *             tile 32: (64,4) (64,8)
  * (the backward with aux losses uses its own fixed shape).
  *
  * Autotuner (config-2 sweep of the batched form): at the handle's current

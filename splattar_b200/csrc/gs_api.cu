@@ -102,6 +102,10 @@ struct gs_rasterizer {
   uint32_t* mask_off = nullptr;
   uint32_t* mask_words = nullptr;
   bool stored_state = false, mask_valid = false;
+  // colour-only forward on 16-pixel tiles: per tile entry, the 4-row pixel
+  // groups it composited into (read by the matching backward)
+  uint8_t* gmask = nullptr;
+  bool gmask_valid = false;
 
   // device scalars: [0] entry total u64, then u32 words
   unsigned long long* entry_total = nullptr;
@@ -358,6 +362,8 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.tile_counter = r->words + 2;
   r->mask_valid = r->stored_state && color && persistent && r->tile == 16;
+  r->gmask_valid = color && persistent && r->tile == 16 && !r->mask_valid && r->gmask != nullptr;
+  if (r->gmask_valid) ra.gmask = r->gmask;
   if (r->mask_valid) {
     TRY_LAUNCH(r, launch_mask_offsets(r->ranges, (uint32_t)tiles, r->mask_words, r->mask_off, r->scan_scratch, st));
     ra.mask = r->mask;
@@ -394,6 +400,7 @@ gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t n
                               bool aux, bool persistent, cudaStream_t st) {
   if (!r->det) TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)nv * n, st));
   RasterArgs ra = bwd_args(r, vdev, nv, tiles);
+  if (r->gmask_valid && !aux && r->tile == 16) ra.gmask = r->gmask;  // summary of the matching forward
   if (r->mask_valid && !aux) {  // masks of the matching colour-only forward
     ra.mask = r->mask;
     ra.mask_off = r->mask_off;
@@ -688,6 +695,10 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
     ALLOC(r->mask_off, r->max_tiles);
     ALLOC(r->mask_words, r->max_tiles);
   }
+  if (r->color_only && !r->stored_state) {
+    // One byte per tile entry: the 4-row groups of a 16-pixel tile it composited into.
+    ALLOC(r->gmask, E);
+  }
   ALLOC(r->entry_total, 1);
   ALLOC(r->words, 8);
   ALLOC(r->out_color, P); ALLOC(r->out_aux, P); ALLOC(r->out_normal, P); ALLOC(r->dl_dcolor, P);
@@ -736,7 +747,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->dl_dcolor, r->dl_dnormal, r->target, r->out_nc, r->coef, r->loss_sums, r->grad_geom,
                   r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
                   r->accum_norm, r->dyn_dev, r->dens_flags, r->dens_slots, r->dens_tmp, r->views_dev,
-                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off,
+                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask,
                   r->normal_loss_sums,
                   r->mask_words,
                   r->scan_scratch, r->sort_scratch};
@@ -1172,6 +1183,7 @@ gs_status gs_set_tile_size(gs_rasterizer* r, uint32_t tile) {
   if (!shape_listed(false, r->tile, r->bwd_batch, r->bwd_ppt)) default_bwd_shape(r);
   r->have_forward = false;  // tile lists of the last forward belong to the old tiling
   r->mask_valid = false;
+  r->gmask_valid = false;
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
   return GS_OK;
 }

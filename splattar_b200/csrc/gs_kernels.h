@@ -92,6 +92,10 @@ struct RasterArgs {
   // Stored-state mode (16-pixel tiles): per-pixel contributor bitmasks. Word w of
   // pixel i (0..255, row-major in the tile) of tile t is mask[(mask_off[t] + w)·256 + i];
   // bit b of word w is set when list position 32w + b composited into the pixel.
+  // Colour-only forward on 16-pixel tiles: per tile entry (index into
+  // sorted_pairs), bit g set when a pixel of rows 4g..4g+3 composited it.
+  // Written by the forward and read by the backward when non-null.
+  uint8_t* gmask;
   uint32_t* mask;               // null: the backward re-evaluates every entry
   const uint32_t* mask_off;     // per tile, in 256-word groups
 };

@@ -176,6 +176,26 @@ __device__ __forceinline__ int compact_slot(bool keep, int* s_wcount, int& kept)
   return off + __popc(bal & lanemask_lt());
 }
 
+// Row-group word flush of the colour-only forward: ORs a 32-entry word of
+// contributor bits over the lanes that share a row group (the 16 lanes of a
+// thread row, and both thread rows of a warp when a thread covers fewer than
+// 4 rows) and adds it into s_gw[group][word]; clears the lane's words.
+template <int PPT, int GPL, int GW>
+__device__ __forceinline__ void flush_row_groups(uint32_t (&gcur)[GPL], uint32_t (*s_gw)[GW], int g0, int word) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < GPL; ++i) {
+    uint32_t v = gcur[i];
+    v |= __shfl_xor_sync(FULL, v, 1);
+    v |= __shfl_xor_sync(FULL, v, 2);
+    v |= __shfl_xor_sync(FULL, v, 4);
+    v |= __shfl_xor_sync(FULL, v, 8);
+    if (PPT < 4) v |= __shfl_xor_sync(FULL, v, 16);
+    if (v && (lane & (PPT < 4 ? 31 : 15)) == 0) atomicOr(&s_gw[g0 + i][word], v);
+    gcur[i] = 0u;
+  }
+}
+
 // COLOR: colour, alpha and final transmittance only (the training step's
 // loss reads nothing else); depth and normal are neither accumulated nor
 // written.
@@ -185,12 +205,26 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
   using L = Layout<TS, PPT>;
   constexpr int NT = L::NT, NW = NT / 32, TP = TS * TS;
   constexpr int ROUNDS = (BATCH + NT - 1) / NT;  // staging rounds per batch
+  // Row-group contributor summary (colour-only forward, 16-pixel tiles): for
+  // every staged entry, bit g is set when some pixel of rows 4g..4g+3 of the
+  // tile composited it; written to gmask[entry] for the backward. Each lane
+  // collects the entries its pixels composited as bits of a 32-entry word per
+  // row group it covers (GPL = 1, or 2 at 8 pixels per thread); every 32
+  // entries the lanes of a row group OR their words together and one lane
+  // adds the result into s_gw[group][word].
+  constexpr bool GM = COLOR && !MASK && TS == 16;
+  constexpr int GPL = PPT >= 8 ? 2 : 1;              // row groups per lane
+  constexpr int GW = (BATCH + 31) / 32;              // 32-entry words per batch
   __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
   __shared__ float4 s_r4[COLOR ? 1 : BATCH];
   __shared__ int s_j[BATCH];
+  __shared__ uint32_t s_gw[GM ? 4 : 1][GM ? GW : 1];
   __shared__ int s_wcount[2][NW];
   __shared__ int s_tile;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const bool gm_on = GM && a.gmask != nullptr;
+  const int g0 = L::row(tid) >> 2;  // first row group of this lane's pixels
+  uint32_t gcur[GPL];
   int tile = blockIdx.x;
   for (;;) {
     if (PERSIST) {
@@ -249,49 +283,71 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
         }
         kept += kr;
       }
+      if (GM && tid < 4 * GW) (&s_gw[0][0])[tid] = 0u;
+#pragma unroll
+      for (int i = 0; i < GPL; ++i) gcur[i] = 0u;
       __syncthreads();
-      if (!tdone) {
-        for (int k = 0; k < kept; ++k) {
+      // Warp-synchronous walk: every lane runs every iteration (lanes whose
+      // pixels are done idle), so the per-entry warp reduction is legal.
+      if (__any_sync(FULL, !tdone)) {
+        int k = 0;
+        for (; k < kept; ++k) {
+          const uint32_t kbit = 1u << (k & 31);
           const float4 bbk = s_bb[k];
-          if (g.pxc < bbk.x || g.pxc > bbk.y) continue;
-          const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
-          const float4 r3 = s_r3[k];
-          const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
-          const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
-          const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
+          if (!tdone && g.pxc >= bbk.x && g.pxc <= bbk.y) {
+            const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
+            const float4 r3 = s_r3[k];
+            const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
+            const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
+            const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
 #pragma unroll
-          for (int p = 0; p < PPT; ++p) {
-            if (done[p] || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
-            const Hit h = eval_hit(cp, r0, r1, r2, r4.w, g.sy[p], g.pyc[p]);
-            const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
-            if (alpha < ALPHA_SKIP) continue;
-            const float w = T[p] * alpha;
-            cr[p] += r3.x * w; cg[p] += r3.y * w; cb[p] += r3.z * w;
-            aa[p] += w;
-            if (!COLOR) {
-              ad[p] += h.t * w;
-              nx[p] += r4.x * w; ny[p] += r4.y * w; nz[p] += r4.z * w;
-            }
-            T[p] = __fmul_rn(T[p], 1.0f - alpha);
-            nc[p] = idx1;
-            if (masks) {
-              const uint32_t cidx = idx1 - 1u;
-              const int w = (int)(cidx >> 5);
-              if (w != mi[p]) {  // close the current word, zero the words skipped
-                uint32_t* m = a.mask + mbase + mpix + p * TS;
-                m[(size_t)mi[p] * TP] = mw[p];
-                for (int z = mi[p] + 1; z < w; ++z) m[(size_t)z * TP] = 0u;
-                mi[p] = w;
-                mw[p] = 0u;
+            for (int p = 0; p < PPT; ++p) {
+              if (done[p] || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
+              const Hit h = eval_hit(cp, r0, r1, r2, r4.w, g.sy[p], g.pyc[p]);
+              const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
+              if (alpha < ALPHA_SKIP) continue;
+              const float w = T[p] * alpha;
+              cr[p] += r3.x * w; cg[p] += r3.y * w; cb[p] += r3.z * w;
+              aa[p] += w;
+              if (!COLOR) {
+                ad[p] += h.t * w;
+                nx[p] += r4.x * w; ny[p] += r4.y * w; nz[p] += r4.z * w;
               }
-              mw[p] |= 1u << (cidx & 31u);
+              T[p] = __fmul_rn(T[p], 1.0f - alpha);
+              nc[p] = idx1;
+              if (GM) gcur[(((L::row(tid) & 3) + p) >> 2) & (GPL - 1)] |= kbit;
+              if (masks) {
+                const uint32_t cidx = idx1 - 1u;
+                const int w = (int)(cidx >> 5);
+                if (w != mi[p]) {  // close the current word, zero the words skipped
+                  uint32_t* m = a.mask + mbase + mpix + p * TS;
+                  m[(size_t)mi[p] * TP] = mw[p];
+                  for (int z = mi[p] + 1; z < w; ++z) m[(size_t)z * TP] = 0u;
+                  mi[p] = w;
+                  mw[p] = 0u;
+                }
+                mw[p] |= 1u << (cidx & 31u);
+              }
+              if (T[p] < T_TERMINATE) done[p] = true;
             }
-            if (T[p] < T_TERMINATE) done[p] = true;
-          }
-          bool all = true;
+            bool all = true;
 #pragma unroll
-          for (int p = 0; p < PPT; ++p) all &= done[p];
-          if (all) { tdone = true; break; }
+            for (int p = 0; p < PPT; ++p) all &= done[p];
+            if (all) tdone = true;
+          }
+          if (GM && gm_on && (k & 31) == 31) flush_row_groups<PPT, GPL, GM ? GW : 1>(gcur, s_gw, g0, k >> 5);
+          if (__all_sync(FULL, tdone)) break;
+        }
+        const int last = k < kept ? k : kept - 1;  // last entry walked (the walk breaks after it)
+        if (GM && gm_on && last >= 0 && (last & 31) != 31) flush_row_groups<PPT, GPL, GM ? GW : 1>(gcur, s_gw, g0, last >> 5);
+      }
+      if (GM && gm_on) {
+        __syncthreads();
+        for (int k = tid; k < kept; k += NT) {
+          const int w = k >> 5, b = k & 31;
+          const uint32_t m = ((s_gw[0][w] >> b) & 1u) | (((s_gw[1][w] >> b) & 1u) << 1) |
+                             (((s_gw[2][w] >> b) & 1u) << 2) | (((s_gw[3][w] >> b) & 1u) << 3);
+          a.gmask[base + (uint32_t)s_j[k]] = (uint8_t)m;
         }
       }
     }
@@ -322,15 +378,28 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
   constexpr int ROUNDS = (BATCH + NT - 1) / NT;  // staging rounds per batch
   constexpr int NG = AUX ? 32 : 16;  // reduced components per entry (AUX: 20 used)
   constexpr int NQ = AUX ? 5 : 4;    // float4 groups per entry written out
+  // Row-group contributor summary of the matching colour-only forward
+  // (16-pixel tiles): entries no pixel of a group composited are skipped for
+  // that group's pixels without evaluating them.
+  constexpr bool GM = !AUX && !MASK && TS == 16;
   __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
   __shared__ float4 s_r4[AUX ? BATCH : 1];
   __shared__ uint32_t s_item[BATCH];
   __shared__ uint32_t s_q[DET ? BATCH : 1];
   __shared__ int s_j[BATCH];
+  __shared__ uint8_t s_gm[GM ? BATCH : 1];
   __shared__ float s_part[NW][BATCH][NG];
   __shared__ int s_wcount[2][NW];
   __shared__ int s_tile, s_maxnc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool gm_on = GM && a.gmask != nullptr;
+  uint32_t pbit[PPT], thread_gbits = 0u;
+#pragma unroll
+  for (int p = 0; p < PPT; ++p) {
+    pbit[p] = 1u << ((L::row(tid) + p) >> 2);
+    thread_gbits |= pbit[p];
+  }
+  const uint32_t warp_gbits = __reduce_or_sync(FULL, thread_gbits);
   int tile = blockIdx.x;
   for (;;) {
     if (PERSIST) {
@@ -443,6 +512,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
           s_item[slot] = item;
           if (DET) s_q[slot] = q;
           s_j[slot] = j;
+          if (GM) s_gm[slot] = gm_on ? __ldg(a.gmask + lo + j) : (uint8_t)0xffu;
         }
         kept += kr;
       }
@@ -475,12 +545,20 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             continue;
           }
         }
+        uint32_t gm = 0xffu;
+        if (GM) {
+          gm = s_gm[k];
+          if (!(gm & warp_gbits)) {  // no pixel of this warp's row groups composited the entry
+            if (lane < 16) s_part[warp][k][lane] = 0.f;
+            continue;
+          }
+        }
         const float4 bbk = s_bb[k];
         float gg[NG];
 #pragma unroll
         for (int c = 0; c < NG; ++c) gg[c] = 0.f;
         bool contrib = false;
-        if (masks ? anybit : (g.pxc >= bbk.x && g.pxc <= bbk.y)) {
+        if (masks ? anybit : ((gm & thread_gbits) && g.pxc >= bbk.x && g.pxc <= bbk.y)) {
           const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
@@ -488,7 +566,8 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
           const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
 #pragma unroll
           for (int p = 0; p < PPT; ++p) {
-            if (masks ? !bit[p] : (!(cidx < nc[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w)) continue;
+            if (masks ? !bit[p] : (!(cidx < nc[p]) || !(gm & pbit[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w))
+              continue;
             const Hit h = eval_hit(cp, r0, r1, r2, depth, g.sy[p], g.pyc[p]);
             const float raw_alpha = __fmul_rn(r3.w, h.ghat);
             const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
@@ -598,9 +677,9 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
 // ------------------------------------------------------------- dispatch
 // Launch shapes (staging batch, pixels per thread) built per tile size.
 // Forward: TS 8 → ppt 1/2 × batch 64/128/256; TS 16 → (64,1) (128,1) (256,1)
-// (64,2) (128,2) (64,4); TS 32 → ppt 2/4 × batch 64/128/256. Backward
-// without aux losses: TS 8 → (64,1) (64,2) (128,2); TS 16 → (64,1) (64,2)
-// (128,2) (64,4); TS 32 → (64,4). With aux losses: batch 32 at ppt 1 (TS 8,
+// (64,2) (128,2) (64,4) (64,8) (128,8); TS 32 → ppt 2/4 × batch 64/128/256
+// and (128,8). Backward without aux losses: TS 8 → (64,1) (64,2) (128,2);
+// TS 16 → (64,1) (64,2) (128,2) (64,4) (64,8) (128,8); TS 32 → (64,4) (64,8). With aux losses: batch 32 at ppt 1 (TS 8,
 // 16) or 4 (TS 32). The backward's per-warp partial buffer NW·BATCH·NG floats
 // is static shared memory, which bounds the backward shapes.
 template <int TS, int PREC, bool DET, bool PERSIST, bool COLOR, bool MASK, typename F>
@@ -613,9 +692,10 @@ bool fwd_shape(int batch, int ppt, F&& f) {
   if constexpr (TS == 8) {
     GS_FWD(64, 1) GS_FWD(128, 1) GS_FWD(256, 1) GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(256, 2)
   } else if constexpr (TS == 16) {
-    GS_FWD(64, 1) GS_FWD(128, 1) GS_FWD(256, 1) GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(64, 4)
+    GS_FWD(64, 1) GS_FWD(128, 1) GS_FWD(256, 1) GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(64, 4) GS_FWD(64, 8)
+    GS_FWD(128, 8)
   } else {
-    GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(256, 2) GS_FWD(64, 4) GS_FWD(128, 4) GS_FWD(256, 4)
+    GS_FWD(64, 2) GS_FWD(128, 2) GS_FWD(256, 2) GS_FWD(64, 4) GS_FWD(128, 4) GS_FWD(256, 4) GS_FWD(128, 8)
   }
 #undef GS_FWD
   return false;
@@ -637,9 +717,9 @@ bool bwd_shape(int batch, int ppt, F&& f) {
   } else if constexpr (TS == 8) {
     GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2)
   } else if constexpr (TS == 16) {
-    GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2) GS_BWD(64, 4)
+    GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2) GS_BWD(64, 4) GS_BWD(64, 8) GS_BWD(128, 8)
   } else {
-    GS_BWD(64, 4)
+    GS_BWD(64, 4) GS_BWD(64, 8)
   }
 #undef GS_BWD
   return false;

@@ -21,8 +21,10 @@ from test_gpu_project_binning import gpu_rects_keys
 pytestmark = pytest.mark.gpu
 
 FWD_SHAPES = {8: [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2), (256, 2)],
-              32: [(64, 2), (128, 2), (256, 2), (64, 4), (128, 4), (256, 4)]}
-BWD_SHAPES = {8: [(64, 1), (64, 2), (128, 2)], 32: [(64, 4)]}
+              16: [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2), (64, 4), (64, 8), (128, 8)],
+              32: [(64, 2), (128, 2), (256, 2), (64, 4), (128, 4), (256, 4), (128, 8)]}
+BWD_SHAPES = {8: [(64, 1), (64, 2), (128, 2)], 16: [(64, 1), (64, 2), (128, 2), (64, 4), (64, 8), (128, 8)],
+              32: [(64, 4), (64, 8)]}
 
 
 def check_rects_keys(s: SceneInput, deg, cam, tile):
@@ -66,7 +68,7 @@ def test_forward_matches_cpu_oracle(tile, seed, n, deg, size):
     assert not mism.any(), f"n_contrib differs on {int(mism.sum())} non-marginal pixels"
 
 
-@pytest.mark.parametrize("tile", [8, 32])
+@pytest.mark.parametrize("tile", [8, 16, 32])
 @pytest.mark.parametrize("persistent", [False, True])
 def test_forward_launch_shapes_agree(tile, persistent):
     """Every built (batch, pixels per thread) of a tile size, including the
@@ -113,7 +115,7 @@ def grad_parity(tile, seed, n, deg, size, aux=False, rel=2e-3, cam_rel=2e-3, bwd
     return g
 
 
-@pytest.mark.parametrize("tile", [8, 32])
+@pytest.mark.parametrize("tile", [8, 16, 32])
 @pytest.mark.parametrize("seed,n,deg,size", [(111, 15, 0, 48), (333, 10, 3, 40)])
 def test_backward_matches_cpu_oracle(tile, seed, n, deg, size):
     for shape in BWD_SHAPES[tile]:
@@ -176,7 +178,7 @@ def test_autotune_tiles_picks_a_built_configuration():
     res = r.autotune_tiles(rc, scene.n)
     assert res["tile"] in (8, 16, 32) and r.tile == res["tile"]
     assert all(v is not None and v["fwd_ms"] > 0 and v["bwd_ms"] > 0 for v in res["per_tile"].values())
-    shapes = FWD_SHAPES.get(res["tile"], [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2), (64, 4)])
+    shapes = FWD_SHAPES[res["tile"]]
     assert (res["fwd_batch"], res["fwd_pixels_per_thread"]) in shapes
     # the training step runs at the chosen tiling
     r.train_step(rc, scene.n, StepSettings(form="chosen"))

@@ -220,8 +220,9 @@ def test_autotune_keeps_results():
     before = r.read("out_color", 4 * P)
     r.write("target", before)
     shapes = r.autotune(rc, scene.n)
-    assert shapes["fwd_batch"] in (64, 128, 256) and shapes["fwd_pixels_per_thread"] in (1, 2, 4)
-    assert (shapes["bwd_batch"], shapes["bwd_pixels_per_thread"]) in ((64, 1), (64, 2), (128, 2), (64, 4))
+    assert shapes["fwd_batch"] in (64, 128, 256) and shapes["fwd_pixels_per_thread"] in (1, 2, 4, 8)
+    assert (shapes["bwd_batch"], shapes["bwd_pixels_per_thread"]) in ((64, 1), (64, 2), (128, 2), (64, 4), (64, 8),
+                                                                      (128, 8))
     r.forward(rc, scene.n)
     assert np.array_equal(r.read("out_color", 4 * P), before)
 
