@@ -34,6 +34,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd+Adam steps/s, 1M surfels 1080p: chosen vs plain form; HBM roofline frac"
+# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel,
+# from one ncu capture of the same workload and launch shapes
+# (profile_step --workload ring8_1m --shapes 64,4,64,8).
+TRAFFIC = {("ring8_1m", "raster_bwd"): 849_430_272}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -444,7 +448,8 @@ def main():
                 "path": "Rasterizer.write_async(target, pinned) + gs_train_step + read_async(loss, pinned)"},
         "gpu_launches": launches_per_step(r["n_tiles"], nv, "chosen") * args.steps,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "frac": round(achieved / peak, 4), "traffic": TRAFFIC.get((args.workload, dom)),
+                     "traffic_unit": "DRAM bytes read + written per launch (ncu, profiles/raster_traffic_ring8_1m.md)",
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
                      else "fallback 6.65 TB/s",
                      "algorithmic_bytes": alg, "kernel_ms": round(stages[dom], 4)},
