@@ -285,8 +285,9 @@ __device__ __forceinline__ void adam1_fast(float& raw, float& m, float& v, float
 //     gradient, summed over the block's surfels and added with one vector
 //     reduction per group of lanes.
 //   Phase 2: after a bounded wait on the copies, each thread updates floats
-//     of the block's parameter rows: gradient = sum over views in view order,
-//     then Adam and the activation, stored coalesced.
+//     of the block's parameter rows: gradient = sum over views (in view order
+//     in deterministic mode, else accumulated by shared-memory atomics in
+//     phase 1), then Adam and the activation, stored coalesced.
 // Parameter gradients never reach global memory. The optimizer arrays are
 // allocated in whole multiples of 64 surfels so the last block's copies stay
 // inside them.
@@ -304,9 +305,11 @@ __host__ __device__ constexpr int pba_surfels(int views) {
   return s;
 }
 __host__ __device__ constexpr int pba_threads(int views) { return (views * pba_surfels(views) + 31) / 32 * 32; }
-__host__ __device__ constexpr size_t pba_smem(int views) {
+// Gradient slots: per (view, surfel) thread (ordered: summed over views in
+// view order in phase 2) or per surfel (atomic: views add into one slot).
+__host__ __device__ constexpr size_t pba_smem(int views, bool ordered) {
   return sizeof(float) * ((size_t)PBA_PARAMS * 3 * pba_surfels(views) + (size_t)SH_FLOATS * pba_surfels(views) +
-                          (size_t)PBA_SLOTS * (pba_threads(views) + 1));
+                          (size_t)PBA_SLOTS * (ordered ? pba_threads(views) + 1 : pba_surfels(views)));
 }
 
 struct GeoGrads {
@@ -373,12 +376,17 @@ __device__ __forceinline__ void flush_cam_group(float* grad_cam_view, const floa
   }
 }
 
-template <int PREC, bool AUX>
-__global__ void __launch_bounds__(PBA_MAX_THREADS, 2) k_project_bwd_adam(ProjectBwdArgs a, AdamFusedArgs opt) {
+// ORD (deterministic mode): every (view, surfel) thread keeps its own
+// gradient slots and phase 2 sums them in view order (88 KB of shared memory
+// at 8 views, 2 blocks per SM). Otherwise the views of a surfel add into one
+// slot with shared-memory atomics (36 KB, 3 blocks per SM at ≤ 80 registers).
+template <int PREC, bool AUX, bool ORD>
+__global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_adam(ProjectBwdArgs a, AdamFusedArgs opt) {
   extern __shared__ __align__(16) float s_dyn[];
   __shared__ uint64_t s_bar;
   const int tid = threadIdx.x;
-  const int V = a.n_views, S = pba_surfels(V), NT = blockDim.x, PITCH = NT + 1;
+  const int V = a.n_views, S = pba_surfels(V), NT = blockDim.x;
+  const int PITCH = ORD ? NT + 1 : S;                  // slot stride
   float* s_stage = s_dyn;                              // [class][raw|m|v][S*W]
   float* s_sh = s_stage + PBA_PARAMS * 3 * S;          // [SH_FLOATS][S]: the block's activated SH, transposed
   float* s_g = s_sh + SH_FLOATS * S;                   // [PBA_SLOTS][PITCH]
@@ -423,13 +431,20 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, 2) k_project_bwd_adam(Project
       }
     }
   }
+  if (!ORD)
+    for (int k = tid; k < PBA_SLOTS * S; k += NT) s_g[k] = 0.0f;
   __syncthreads();
   // ---- phase 1
   {
     const int v = tid / S, sl = tid % S;
     const uint32_t i = i0 + (uint32_t)sl;
     const bool active = v < V && i < a.n;
-    float* col = s_g + tid;
+    // ORD: this thread's column; atomic: the surfel's column, shared by its views.
+    float* col = s_g + (ORD ? tid : sl);
+    auto put = [&](int slot, float g) {
+      if (ORD) col[slot * PITCH] = g;
+      else if (g != 0.0f) atomicAdd(col + slot * PITCH, g);
+    };
     GeoGrads o;
     o.pos = f3(0, 0, 0); o.scales = make_float2(0, 0); o.quat = make_float4(0, 0, 0, 0); o.opacity = 0;
 #pragma unroll
@@ -444,28 +459,29 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, 2) k_project_bwd_adam(Project
         chain_core<PREC, AUX>(k, __ldg(a.pos + i), __ldg(a.scales + i), __ldg(a.quats + i),
                               [&](int kk) { return f3(shc[(3 * kk) * S], shc[(3 * kk + 1) * S], shc[(3 * kk + 2) * S]); },
                               G, o, [&](int kk, float3 g) {
-                                col[(10 + 3 * kk) * PITCH] = g.x;
-                                col[(11 + 3 * kk) * PITCH] = g.y;
-                                col[(12 + 3 * kk) * PITCH] = g.z;
+                                put(10 + 3 * kk, g.x);
+                                put(11 + 3 * kk, g.y);
+                                put(12 + 3 * kk, g.z);
                                 written |= 1u << kk;
                               });
         any = true;
+        if (ORD) {
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-          if (!(written >> kk & 1u)) {
-            col[(10 + 3 * kk) * PITCH] = 0.0f;
-            col[(11 + 3 * kk) * PITCH] = 0.0f;
-            col[(12 + 3 * kk) * PITCH] = 0.0f;
+          for (int kk = 0; kk < 16; ++kk) {
+            if (!(written >> kk & 1u)) {
+              col[(10 + 3 * kk) * PITCH] = 0.0f;
+              col[(11 + 3 * kk) * PITCH] = 0.0f;
+              col[(12 + 3 * kk) * PITCH] = 0.0f;
+            }
           }
         }
-        col[0] = o.pos.x; col[PITCH] = o.pos.y; col[2 * PITCH] = o.pos.z;
-        col[3 * PITCH] = o.scales.x; col[4 * PITCH] = o.scales.y;
-        col[5 * PITCH] = o.quat.x; col[6 * PITCH] = o.quat.y;
-        col[7 * PITCH] = o.quat.z; col[8 * PITCH] = o.quat.w;
-        col[9 * PITCH] = o.opacity;
+        put(0, o.pos.x); put(1, o.pos.y); put(2, o.pos.z);
+        put(3, o.scales.x); put(4, o.scales.y);
+        put(5, o.quat.x); put(6, o.quat.y); put(7, o.quat.z); put(8, o.quat.w);
+        put(9, o.opacity);
       }
     }
-    if (!any) {
+    if (ORD && !any) {
 #pragma unroll 2
       for (int j = 0; j < PBA_SLOTS; ++j) col[j * PITCH] = 0.0f;
     }
@@ -495,8 +511,9 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, 2) k_project_bwd_adam(Project
   }
   const uint32_t ns = min((uint32_t)S, a.n - i0);
   auto grad_sum = [&](int slot, int sl) {
-    float g = 0.0f;
     const float* p = s_g + slot * PITCH + sl;
+    if (!ORD) return *p;
+    float g = 0.0f;
 #pragma unroll 8
     for (int v = 0; v < V; ++v) g += p[v * S];
     return g;
@@ -542,11 +559,15 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, 2) k_project_bwd_adam(Project
 // the current device. Called when a handle is created (outside any capture).
 int prepare_project_kernels() {
   size_t big = 0;
-  for (int v = 1; v <= 64; ++v) big = pba_smem(v) > big ? pba_smem(v) : big;
+  for (int v = 1; v <= 64; ++v) big = pba_smem(v, true) > big ? pba_smem(v, true) : big;
   const int smem = (int)big;
-  const void* fns[6] = {(const void*)k_project_bwd_adam<0, false>, (const void*)k_project_bwd_adam<0, true>,
-                        (const void*)k_project_bwd_adam<1, false>, (const void*)k_project_bwd_adam<1, true>,
-                        (const void*)k_project_bwd_adam<2, false>, (const void*)k_project_bwd_adam<2, true>};
+  const void* fns[12] = {
+      (const void*)k_project_bwd_adam<0, false, true>, (const void*)k_project_bwd_adam<0, true, true>,
+      (const void*)k_project_bwd_adam<1, false, true>, (const void*)k_project_bwd_adam<1, true, true>,
+      (const void*)k_project_bwd_adam<2, false, true>, (const void*)k_project_bwd_adam<2, true, true>,
+      (const void*)k_project_bwd_adam<0, false, false>, (const void*)k_project_bwd_adam<0, true, false>,
+      (const void*)k_project_bwd_adam<1, false, false>, (const void*)k_project_bwd_adam<1, true, false>,
+      (const void*)k_project_bwd_adam<2, false, false>, (const void*)k_project_bwd_adam<2, true, false>};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return (int)e;
@@ -570,8 +591,14 @@ int launch_project_bwd_adam(const ProjectBwdArgs& a, const AdamFusedArgs& opt, i
   if (a.n_views < 1 || a.n_views > PBA_MAX_THREADS) return (int)cudaErrorInvalidValue;
   const int S = pba_surfels(a.n_views);
   dim3 grid((a.n + S - 1) / S);
-  const size_t smem = pba_smem(a.n_views);
-#define GS_PBA(P, X) k_project_bwd_adam<P, X><<<grid, pba_threads(a.n_views), smem, st>>>(a, opt)
+  // Deterministic mode (per-entry partials) keeps the view-ordered sum.
+  const bool ord = a.partials != nullptr;
+  const size_t smem = pba_smem(a.n_views, ord);
+#define GS_PBA(P, X)                                                                              \
+  do {                                                                                            \
+    if (ord) k_project_bwd_adam<P, X, true><<<grid, pba_threads(a.n_views), smem, st>>>(a, opt);  \
+    else k_project_bwd_adam<P, X, false><<<grid, pba_threads(a.n_views), smem, st>>>(a, opt);     \
+  } while (0)
   if (prec == 0) { if (aux) GS_PBA(0, true); else GS_PBA(0, false); }
   else if (prec == 1) { if (aux) GS_PBA(1, true); else GS_PBA(1, false); }
   else { if (aux) GS_PBA(2, true); else GS_PBA(2, false); }
