@@ -96,6 +96,36 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
   return h;
 }
 
+// eval_hit for two pixels of one column (rows with sy.x, sy.y) with the
+// packed two-wide FP32 instructions of sm_100 (FFMA2/FMUL2/FADD2): every
+// product and sum of the hit test takes one instruction for both pixels.
+// Each component rounds exactly as the scalar operation of eval_hit, so
+// either form gives bit-identical results for a pixel.
+__device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
+                                          float depth, float2 sy, float2 pyc, Hit& ha, Hit& hb) {
+  const float2 det = __ffma2_rn(make_float2(r0.y, r0.y), sy, make_float2(c.det0, c.det0));
+  const float2 inv = make_float2(rcp_approx(det.x), rcp_approx(det.y));
+  const float2 un = __ffma2_rn(make_float2(r1.y, r1.y), sy, make_float2(c.un0, c.un0));
+  const float2 vn = __ffma2_rn(make_float2(r2.y, r2.y), sy, make_float2(c.vn0, c.vn0));
+  const float2 u = __fmul2_rn(un, inv), v = __fmul2_rn(vn, inv);
+  const float2 t = __fmul2_rn(make_float2(r0.w, r0.w), inv);
+  const float2 q2 = __ffma2_rn(u, u, __fmul2_rn(v, v));
+  const float2 qr0 = __fmul2_rn(make_float2(0.5f, 0.5f), q2);
+  const float2 dy = __fadd2_rn(pyc, make_float2(-r2.w, -r2.w));  // pyc − r2.w, exactly
+  const float2 qs = __ffma2_rn(dy, dy, make_float2(c.dx2, c.dx2));
+  const float inf = __int_as_float(0x7f800000);
+  const float qra = fabsf(det.x) > 1e-12f && t.x > NEAR_DEPTH ? qr0.x : inf;
+  const float qrb = fabsf(det.y) > 1e-12f && t.y > NEAR_DEPTH ? qr0.y : inf;
+  ha.ray = qra <= qs.x;
+  hb.ray = qrb <= qs.y;
+  ha.u = u.x; ha.v = v.x; ha.inv_det = inv.x; ha.q2 = q2.x; ha.dy = dy.x;
+  hb.u = u.y; hb.v = v.y; hb.inv_det = inv.y; hb.q2 = q2.y; hb.dy = dy.y;
+  ha.t = ha.ray ? t.x : depth;
+  hb.t = hb.ray ? t.y : depth;
+  ha.ghat = __expf(-(ha.ray ? qra : qs.x));
+  hb.ghat = __expf(-(hb.ray ? qrb : qs.y));
+}
+
 // Thread → pixel layout of a TS×TS tile with PPT vertically adjacent pixels
 // per thread: each warp owns a compact block of WC columns × WR·PPT rows
 // (16 × 2·PPT for tiles of 16 and 32, 8 × 4·PPT for tiles of 8), blocks laid
@@ -300,10 +330,27 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
             const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
             const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
             const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
+            constexpr int PS = PPT >= 2 ? 2 : 1;  // pixels per hit evaluation
 #pragma unroll
-            for (int p = 0; p < PPT; ++p) {
-              if (done[p] || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w) continue;
-              const Hit h = eval_hit(cp, r0, r1, r2, r4.w, g.sy[p], g.pyc[p]);
+            for (int pp = 0; pp < PPT; pp += PS) {
+            bool need[PS];
+            Hit hh[PS];
+#pragma unroll
+            for (int q = 0; q < PS; ++q)
+              need[q] = !(done[pp + q] || g.pyc[pp + q] < bbk.z || g.pyc[pp + q] > bbk.w);
+            if constexpr (PS == 2) {
+              if (!need[0] && !need[1]) continue;
+              eval_hit2(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
+                        make_float2(g.pyc[pp], g.pyc[pp + 1]), hh[0], hh[PS - 1]);
+            } else {
+              if (!need[0]) continue;
+              hh[0] = eval_hit(cp, r0, r1, r2, r4.w, g.sy[pp], g.pyc[pp]);
+            }
+#pragma unroll
+            for (int q = 0; q < PS; ++q) {
+              const int p = pp + q;
+              if (!need[q]) continue;
+              const Hit& h = hh[q];
               const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
               if (alpha < ALPHA_SKIP) continue;
               const float w = T[p] * alpha;
@@ -329,6 +376,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
                 mw[p] |= 1u << (cidx & 31u);
               }
               if (T[p] < T_TERMINATE) done[p] = true;
+            }
             }
             bool all = true;
 #pragma unroll
@@ -564,11 +612,32 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
           if (AUX) { r4 = s_r4[k]; depth = r4.w; }
           const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
+          // One pixel per hit evaluation: evaluating pairs (eval_hit2) keeps two
+          // hits live through the gradient code and costs more registers than
+          // it saves instructions here.
+          constexpr int PS = 1;
 #pragma unroll
-          for (int p = 0; p < PPT; ++p) {
-            if (masks ? !bit[p] : (!(cidx < nc[p]) || !(gm & pbit[p]) || g.pyc[p] < bbk.z || g.pyc[p] > bbk.w))
-              continue;
-            const Hit h = eval_hit(cp, r0, r1, r2, depth, g.sy[p], g.pyc[p]);
+          for (int pp = 0; pp < PPT; pp += PS) {
+          bool need[PS];
+          Hit hh[PS];
+#pragma unroll
+          for (int q = 0; q < PS; ++q) {
+            const int p = pp + q;
+            need[q] = masks ? bit[p] : (cidx < nc[p] && (gm & pbit[p]) && g.pyc[p] >= bbk.z && g.pyc[p] <= bbk.w);
+          }
+          if constexpr (PS == 2) {
+            if (!need[0] && !need[1]) continue;
+            eval_hit2(cp, r0, r1, r2, depth, make_float2(g.sy[pp], g.sy[pp + 1]),
+                      make_float2(g.pyc[pp], g.pyc[pp + 1]), hh[0], hh[PS - 1]);
+          } else {
+            if (!need[0]) continue;
+            hh[0] = eval_hit(cp, r0, r1, r2, depth, g.sy[pp], g.pyc[pp]);
+          }
+#pragma unroll
+          for (int q = 0; q < PS; ++q) {
+            const int p = pp + q;
+            if (!need[q]) continue;
+            const Hit& h = hh[q];
             const float raw_alpha = __fmul_rn(r3.w, h.ghat);
             const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
             if (alpha < ALPHA_SKIP) continue;
@@ -625,6 +694,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
                 if (AUX) gg[16] += dl_dt;
               }
             }
+          }
           }
           // A thread's pixels share sx: the sx moments are sx times the plain sums.
           gg[0] = gg[2] * g.sx; gg[3] = gg[5] * g.sx; gg[6] = gg[8] * g.sx;
