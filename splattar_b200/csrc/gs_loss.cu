@@ -8,8 +8,8 @@
 //   k_ssim_moments: per 16×16 tile, stage x and y with a 5-pixel halo in
 //     shared memory, blur the five moments (μx, μy, x², y², xy) of the three
 //     channels separably, form SSIM and the three coefficient maps Cμ, Cx²,
-//     Cxy per channel (ssim.wgsl:94-126), stored as nine planes, and
-//     accumulate the per-view loss sums.
+//     Cxy per channel (ssim.wgsl:94-126), stored as four float2 planes and
+//     one float plane, and accumulate the per-view loss sums.
 //   k_ssim_grad: stage the nine coefficient planes with a halo, blur them
 //     (the zero-padded symmetric window is self-adjoint) and combine with the
 //     L1 term into dL/dx (ssim.wgsl:130-143).
@@ -24,20 +24,22 @@ namespace {
 
 // Output tiles of 16×16 pixels, inputs staged with a 5-pixel halo (26×26).
 // Separable 11-tap blurs run as sliding windows in registers: a horizontal
-// pass where each thread owns one (row, map) and slides along x, then a
-// vertical pass where each thread owns one (column, map) and slides along y,
-// so every staged value is read from shared memory once per pass.
+// pass where each thread owns one (row, channel or plane) and slides along x,
+// then a vertical pass where each thread owns one (column, channel or plane)
+// and slides along y, so every staged value is read from shared memory once
+// per pass. Pairs of maps blur together in the packed two-wide FP32
+// instructions of sm_100 (FFMA2/FADD2/FMUL2): (μx, μy) and (E[x²], E[y²]) per
+// channel in the moments kernel, two coefficient planes at a time in the
+// gradient kernel; each component rounds as the scalar operation would.
 constexpr int T16 = 16, HALO = 5, EXT = T16 + 2 * HALO;  // 26
 constexpr int TAPS = 2 * HALO + 1;                       // 11
-// Shared-memory strides chosen against bank conflicts: staged planes use an
-// odd row pitch (rows are read by consecutive lanes); horizontal results use
-// an odd row pitch (written by lanes holding consecutive rows) and a plane
-// stride ≡ 16 (mod 32) words (read by two half-warps of different planes);
-// vertical results use a plane stride ≡ 16 (mod 32) for the same reason.
+// Staged rows use an odd pitch (read by lanes holding consecutive rows; for
+// 8-byte elements the two 16-lane phases then hit distinct banks), horizontal
+// results an odd row pitch, vertical results dense 16×16 planes.
 constexpr int IN_PITCH = EXT + 1;                        // 27
 constexpr int H_ROW = T16 + 1;                           // 17
-constexpr int H_PLANE = 464;                             // ≥ EXT·H_ROW = 442, ≡ 16 mod 32
-constexpr int V_PLANE = T16 * T16 + 16;                  // 272
+constexpr int H_PLANE = EXT * H_ROW;                     // 442
+constexpr int V_PLANE = T16 * T16;                       // 256
 
 struct TileLoc {
   int v, x0, y0, W, H;
@@ -63,8 +65,10 @@ __device__ __forceinline__ TileLoc locate(const SsimArgs& a, int t) {
   }
 }
 
-// Slides an 11-tap window along `n_out` outputs: out[o] = Σ_d w[|d−5|]·in(o+d).
-// `in(i)` produces input i (0 ≤ i < n_out + 10), `out(o, value)` consumes.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// Slides an 11-tap window along `N_OUT` outputs: out[o] = Σ_d w[|d−5|]·in(o+d)
+// (w[k] is the weight at offset ±k), for a scalar map.
 template <int N_OUT, class In, class Out>
 __device__ __forceinline__ void slide11(const float (&w)[6], In in, Out out) {
   float win[TAPS];
@@ -73,7 +77,7 @@ __device__ __forceinline__ void slide11(const float (&w)[6], In in, Out out) {
 #pragma unroll
   for (int o = 0; o < N_OUT; ++o) {
     win[TAPS - 1] = in(o + TAPS - 1);
-    float acc = w[0] * win[HALO];  // w[k] is the weight at offset ±k
+    float acc = w[0] * win[HALO];
 #pragma unroll
     for (int d = 0; d < HALO; ++d) acc += w[HALO - d] * (win[d] + win[TAPS - 1 - d]);
     out(o, acc);
@@ -82,14 +86,38 @@ __device__ __forceinline__ void slide11(const float (&w)[6], In in, Out out) {
   }
 }
 
+// The same for two maps at once (float2 windows, packed instructions).
+template <int N_OUT, class In, class Out>
+__device__ __forceinline__ void slide11x2(const float (&w)[6], In in, Out out) {
+  float2 win[TAPS];
+#pragma unroll
+  for (int i = 0; i < TAPS - 1; ++i) win[i] = in(i);
+#pragma unroll
+  for (int o = 0; o < N_OUT; ++o) {
+    win[TAPS - 1] = in(o + TAPS - 1);
+    float2 acc = __fmul2_rn(f2(w[0]), win[HALO]);
+#pragma unroll
+    for (int d = 0; d < HALO; ++d) acc = __ffma2_rn(f2(w[HALO - d]), __fadd2_rn(win[d], win[TAPS - 1 - d]), acc);
+    out(o, acc);
+#pragma unroll
+    for (int i = 0; i < TAPS - 1; ++i) win[i] = win[i + 1];
+  }
+}
+
 // Moments → SSIM, its coefficient maps and the per-view loss sums.
-// Horizontal maps per channel: μx, μy, x², y², xy (15 in all).
+// Per channel: (μx, μy), (E[x²], E[y²]) as packed pairs and E[xy] scalar.
+// Coefficient planes (scratch, coef_stride pixels each): float2 planes
+// (Cμ_r, Cμ_g), (Cx²_r, Cx²_g), (Cxy_r, Cxy_g), (Cμ_b, Cx²_b) at
+// coef + 2k·stride, and Cxy_b at coef + 8·stride.
 __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
-  __shared__ float s_in[6][EXT][IN_PITCH];   // x rgb, y rgb with halo
-  __shared__ float s_h[15 * H_PLANE];        // horizontal results [map][row][col]
+  __shared__ float2 s_in[3][EXT][IN_PITCH];     // (x, y) per channel, with halo
+  __shared__ float2 s_h2[3][2][EXT * H_ROW];    // horizontal: [ch][(μx,μy) | (x²,y²)][row][col]
+  __shared__ float s_h1[3][EXT * H_ROW];        // horizontal: [ch] E[xy]
   __shared__ double s_red[2][8];
-  float* s_v = &s_in[0][0][0];  // vertical results [map][row][col], reusing s_in after pass 1
-  static_assert(15 * V_PLANE <= 6 * EXT * IN_PITCH, "s_v fits in s_in");
+  // Vertical results reuse s_in after the horizontal pass.
+  float2* s_v2 = &s_in[0][0][0];                 // [ch][2][16×16]
+  float* s_v1 = reinterpret_cast<float*>(s_v2 + 3 * 2 * V_PLANE);  // [ch][16×16]
+  static_assert(3 * 2 * V_PLANE * 2 + 3 * V_PLANE <= 3 * EXT * IN_PITCH * 2, "vertical results fit in s_in");
   const int tid = threadIdx.x;
   const TileLoc L = locate(a, blockIdx.x);
   for (int k = tid; k < EXT * EXT; k += 256) {
@@ -101,27 +129,28 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
       xv = a.img[p];
       yv = a.target[p];
     }
-    s_in[0][ly][lx] = xv.x; s_in[1][ly][lx] = xv.y; s_in[2][ly][lx] = xv.z;
-    s_in[3][ly][lx] = yv.x; s_in[4][ly][lx] = yv.y; s_in[5][ly][lx] = yv.z;
+    s_in[0][ly][lx] = make_float2(xv.x, yv.x);
+    s_in[1][ly][lx] = make_float2(xv.y, yv.y);
+    s_in[2][ly][lx] = make_float2(xv.z, yv.z);
   }
   float w[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) w[k] = a.w[k];
   __syncthreads();
-  // Horizontal: item = (map mc, row r); map mc = 5·channel + moment.
-  for (int it = tid; it < 15 * EXT; it += 256) {
-    const int mc = it / EXT, r = it - mc * EXT;
-    const int ch = mc / 5, m = mc - ch * 5;
-    const float* X = &s_in[ch][r][0];
-    const float* Y = &s_in[3 + ch][r][0];
-    float* O = s_h + mc * H_PLANE + r * H_ROW;
-    auto put = [&](int o, float v) { O[o] = v; };
-    switch (m) {
-      case 0: slide11<T16>(w, [&](int i) { return X[i]; }, put); break;
-      case 1: slide11<T16>(w, [&](int i) { return Y[i]; }, put); break;
-      case 2: slide11<T16>(w, [&](int i) { const float x = X[i]; return x * x; }, put); break;
-      case 3: slide11<T16>(w, [&](int i) { const float y = Y[i]; return y * y; }, put); break;
-      default: slide11<T16>(w, [&](int i) { return X[i] * Y[i]; }, put); break;
+  // Horizontal: item = (channel, map kind, row): kind 0 (μx, μy) and kind 1
+  // (E[x²], E[y²]) packed, kind 2 E[xy] scalar.
+  for (int it = tid; it < 9 * EXT; it += 256) {
+    const int km = it / EXT, r = it - km * EXT, ch = km / 3, kind = km - ch * 3;
+    const float2* XY = &s_in[ch][r][0];
+    if (kind == 0) {
+      float2* O = &s_h2[ch][0][r * H_ROW];
+      slide11x2<T16>(w, [&](int i) { return XY[i]; }, [&](int o, float2 v) { O[o] = v; });
+    } else if (kind == 1) {
+      float2* O = &s_h2[ch][1][r * H_ROW];
+      slide11x2<T16>(w, [&](int i) { const float2 v = XY[i]; return __fmul2_rn(v, v); }, [&](int o, float2 v) { O[o] = v; });
+    } else {
+      float* O = &s_h1[ch][r * H_ROW];
+      slide11<T16>(w, [&](int i) { const float2 v = XY[i]; return v.x * v.y; }, [&](int o, float v) { O[o] = v; });
     }
   }
   // L1 of this thread's pixel, read before s_in is reused.
@@ -129,20 +158,24 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
   const int gx = L.x0 + ox, gy = L.y0 + oy;
   const bool inside = gx < L.W && gy < L.H;
   float l1 = 0.f;
-  float xs[3], ys[3];
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) {
-    xs[ch] = s_in[ch][oy + HALO][ox + HALO];
-    ys[ch] = s_in[3 + ch][oy + HALO][ox + HALO];
-    if (inside) l1 += fabsf(xs[ch] - ys[ch]);
+    const float2 v = s_in[ch][oy + HALO][ox + HALO];
+    if (inside) l1 += fabsf(v.x - v.y);
   }
   __syncthreads();
-  // Vertical: item = (map mc, column c).
-  if (tid < 15 * T16) {
-    const int mc = tid / T16, c = tid - mc * T16;
-    const float* I = s_h + mc * H_PLANE + c;
-    float* O = s_v + mc * V_PLANE + c;
-    slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+  // Vertical: item = (channel, map kind, column): kinds 0, 1 packed, 2 scalar.
+  if (tid < 3 * 3 * T16) {
+    const int c = tid % T16, km = tid / T16, ch = km / 3, kind = km % 3;
+    if (kind < 2) {
+      const float2* I = &s_h2[ch][kind][c];
+      float2* O = s_v2 + (ch * 2 + kind) * V_PLANE + c;
+      slide11x2<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float2 v) { O[o * T16] = v; });
+    } else {
+      const float* I = &s_h1[ch][c];
+      float* O = s_v1 + ch * V_PLANE + c;
+      slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+    }
   }
   __syncthreads();
   float ss = 0.f;
@@ -151,25 +184,30 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
     const float inv_n3 = 1.0f / (3.0f * (float)L.W * (float)L.H);
     const float C1 = 1e-4f, C2 = 9e-4f;
     const float dw = -a.w_ssim * inv_n3;
+    float cm[3], cx2[3], cxy[3];
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
-      const float* V = s_v + oy * T16 + ox;
-      const float mu_x = V[(5 * ch) * V_PLANE], mu_y = V[(5 * ch + 1) * V_PLANE];
-      const float bx2 = V[(5 * ch + 2) * V_PLANE], by2 = V[(5 * ch + 3) * V_PLANE], bxy = V[(5 * ch + 4) * V_PLANE];
-      const float sx2 = bx2 - mu_x * mu_x, sy2 = by2 - mu_y * mu_y, sxy = bxy - mu_x * mu_y;
+      const int q = oy * T16 + ox;
+      const float2 mu = s_v2[(ch * 2) * V_PLANE + q], b2 = s_v2[(ch * 2 + 1) * V_PLANE + q];
+      const float bxy = s_v1[ch * V_PLANE + q];
+      const float mu_x = mu.x, mu_y = mu.y;
+      const float sx2 = b2.x - mu_x * mu_x, sy2 = b2.y - mu_y * mu_y, sxy = bxy - mu_x * mu_y;
       const float p = mu_x * mu_x + mu_y * mu_y + C1;
-      const float q = sx2 + sy2 + C2;
+      const float qd = sx2 + sy2 + C2;
       const float l = (2.0f * mu_x * mu_y + C1) / p;
-      const float cs = (2.0f * sxy + C2) / q;
-      const float S = l * cs;
-      const float ds_dmux = cs * (2.0f * mu_y - 2.0f * mu_x * l) / p + l * (-2.0f * mu_y + 2.0f * mu_x * cs) / q;
-      const float ds_dbx2 = -l * cs / q;
-      const float ds_dbxy = 2.0f * l / q;
-      a.coef[(size_t)(3 * ch) * a.coef_stride + pix] = ds_dmux * dw;
-      a.coef[(size_t)(3 * ch + 1) * a.coef_stride + pix] = ds_dbx2 * dw;
-      a.coef[(size_t)(3 * ch + 2) * a.coef_stride + pix] = ds_dbxy * dw;
-      ss += S;
+      const float cs = (2.0f * sxy + C2) / qd;
+      ss += l * cs;
+      cm[ch] = (cs * (2.0f * mu_y - 2.0f * mu_x * l) / p + l * (-2.0f * mu_y + 2.0f * mu_x * cs) / qd) * dw;
+      cx2[ch] = (-l * cs / qd) * dw;
+      cxy[ch] = (2.0f * l / qd) * dw;
     }
+    float2* P2 = reinterpret_cast<float2*>(a.coef);
+    const size_t st2 = a.coef_stride;  // float2 plane k starts at float offset 2k·stride
+    P2[0 * st2 + pix] = make_float2(cm[0], cm[1]);
+    P2[1 * st2 + pix] = make_float2(cx2[0], cx2[1]);
+    P2[2 * st2 + pix] = make_float2(cxy[0], cxy[1]);
+    P2[3 * st2 + pix] = make_float2(cm[2], cx2[2]);
+    a.coef[8 * a.coef_stride + pix] = cxy[2];
   }
   // Per-view loss sums: warp, then block, then one double atomic each.
   double dl1 = warp_sum(l1), dss = warp_sum(ss);
@@ -184,38 +222,57 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
 }
 
 // Blur of the nine coefficient maps (the zero-padded symmetric window is
-// self-adjoint) combined with the L1 term into dL/dx.
+// self-adjoint) combined with the L1 term into dL/dx: four float2 planes
+// blurred as packed pairs and one scalar plane.
 __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
-  __shared__ float s_c[9][EXT][IN_PITCH];
-  __shared__ float s_h[9 * H_PLANE];
-  float* s_v = &s_c[0][0][0];  // vertical results [map][row][col], reusing s_c after pass 1
-  static_assert(9 * V_PLANE <= 9 * EXT * IN_PITCH, "s_v fits in s_c");
+  __shared__ float2 s_c2[4][EXT][IN_PITCH];
+  __shared__ float s_c1[EXT][IN_PITCH];
+  __shared__ float2 s_h2[4][EXT * H_ROW];
+  __shared__ float s_h1[EXT * H_ROW];
+  float2* s_v2 = &s_c2[0][0][0];                                    // [4][16×16], reusing s_c2
+  float* s_v1 = reinterpret_cast<float*>(s_v2 + 4 * V_PLANE);        // [16×16]
+  static_assert(4 * V_PLANE * 2 + V_PLANE <= 4 * EXT * IN_PITCH * 2, "vertical results fit in s_c2");
   const int tid = threadIdx.x;
   const TileLoc L = locate(a, blockIdx.x);
+  const float2* P2 = reinterpret_cast<const float2*>(a.coef);
+  const size_t st2 = a.coef_stride;
   for (int k = tid; k < EXT * EXT; k += 256) {
     const int ly = k / EXT, lx = k % EXT;
     const int gx = L.x0 + lx - HALO, gy = L.y0 + ly - HALO;
     const bool in = gx >= 0 && gy >= 0 && gx < L.W && gy < L.H;
     const size_t p = in ? (size_t)(L.pix_base + (long long)gy * L.W + gx) : 0;
 #pragma unroll
-    for (int m = 0; m < 9; ++m) s_c[m][ly][lx] = in ? __ldg(a.coef + (size_t)m * a.coef_stride + p) : 0.f;
+    for (int m = 0; m < 4; ++m) s_c2[m][ly][lx] = in ? __ldg(P2 + m * st2 + p) : make_float2(0.f, 0.f);
+    s_c1[ly][lx] = in ? __ldg(a.coef + 8 * a.coef_stride + p) : 0.f;
   }
   float w[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) w[k] = a.w[k];
   __syncthreads();
-  for (int it = tid; it < 9 * EXT; it += 256) {
+  for (int it = tid; it < 5 * EXT; it += 256) {
     const int m = it / EXT, r = it - m * EXT;
-    const float* X = &s_c[m][r][0];
-    float* O = s_h + m * H_PLANE + r * H_ROW;
-    slide11<T16>(w, [&](int i) { return X[i]; }, [&](int o, float v) { O[o] = v; });
+    if (m < 4) {
+      const float2* X = &s_c2[m][r][0];
+      float2* O = &s_h2[m][r * H_ROW];
+      slide11x2<T16>(w, [&](int i) { return X[i]; }, [&](int o, float2 v) { O[o] = v; });
+    } else {
+      const float* X = &s_c1[r][0];
+      float* O = &s_h1[r * H_ROW];
+      slide11<T16>(w, [&](int i) { return X[i]; }, [&](int o, float v) { O[o] = v; });
+    }
   }
   __syncthreads();
-  if (tid < 9 * T16) {
+  if (tid < 5 * T16) {
     const int m = tid / T16, c = tid - m * T16;
-    const float* I = s_h + m * H_PLANE + c;
-    float* O = s_v + m * V_PLANE + c;
-    slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+    if (m < 4) {
+      const float2* I = &s_h2[m][c];
+      float2* O = s_v2 + m * V_PLANE + c;
+      slide11x2<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float2 v) { O[o * T16] = v; });
+    } else {
+      const float* I = &s_h1[c];
+      float* O = s_v1 + c;
+      slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+    }
   }
   __syncthreads();
   const int ox = tid & 15, oy = tid >> 4;
@@ -224,15 +281,18 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
   const long long pix = L.pix_base + (long long)gy * L.W + gx;
   const float4 x = a.img[pix], y = a.target[pix];
   const float k1 = a.w_l1 / (3.0f * (float)L.W * (float)L.H);
+  const int q = oy * T16 + ox;
+  const float2 vm = s_v2[0 * V_PLANE + q], vx2 = s_v2[1 * V_PLANE + q], vxy = s_v2[2 * V_PLANE + q];
+  const float2 vb = s_v2[3 * V_PLANE + q];
+  const float vxy_b = s_v1[q];
+  const float cmu[3] = {vm.x, vm.y, vb.x}, cx2[3] = {vx2.x, vx2.y, vb.y}, cxy[3] = {vxy.x, vxy.y, vxy_b};
   const float xs[3] = {x.x, x.y, x.z}, ys[3] = {y.x, y.y, y.z};
   float out[3];
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) {
     const float diff = xs[ch] - ys[ch];
     const float sg = diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f);
-    const float* V = s_v + oy * T16 + ox;
-    out[ch] = sg * k1 + V[(3 * ch) * V_PLANE] + 2.0f * xs[ch] * V[(3 * ch + 1) * V_PLANE] +
-              ys[ch] * V[(3 * ch + 2) * V_PLANE];
+    out[ch] = sg * k1 + cmu[ch] + 2.0f * xs[ch] * cx2[ch] + ys[ch] * cxy[ch];
   }
   a.dl_dcolor[pix] = make_float4(out[0], out[1], out[2], 0.f);
 }
