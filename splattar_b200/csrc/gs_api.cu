@@ -1252,7 +1252,10 @@ gs_status tune_current_tile(gs_rasterizer* r, uint32_t nv, uint32_t n, cudaStrea
   *fwd_ms = best;
   r->fwd_batch = fshape[bf].batch;
   r->fwd_ppt = fshape[bf].ppt;
-  s = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true, true, st);
+  // The forward the backward shapes are timed after is the step's own (the
+  // colour-only forward also writes the row-group contributor summary).
+  s = run_forward(r, r->views_dev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, nullptr,
+                  r->color_only);
   if (!s) {
     TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
     s = run_loss(r, r->views_dev, r->views_batched.data(), nv, 0.8f, 0.2f, r->loss_sums, st);
