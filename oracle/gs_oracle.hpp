@@ -55,6 +55,17 @@ constexpr double MARGIN_ALPHA = 2e-5;  // absolute, on alpha in [0,1]
 constexpr double MARGIN_T = 1e-3;      // relative, on transmittance vs T_TERMINATE
 constexpr double MARGIN_RECT = 1e-5;   // absolute, in tile units
 constexpr double MARGIN_BRANCH = 1e-6; // absolute, on g_ray - g_scr
+// Conditioning of the float32 evaluation: a float32 rasterizer computes M =
+// τu×τv, Bu = τv×c, Bv = c×τu, tn = −c·M and the dot products with s in
+// single precision, so each carries an absolute error up to about
+// COND_K·ε32 times the product of its factors' magnitudes. Propagated through
+// u = (s·Bu)/det, v = (s·Bv)/det, t = tn/det, that gives a bound δq on the
+// exponent the hit uses. Decisions within δq of a threshold, and hits whose
+// δq exceeds COND_MAX_DQ (near-grazing surfels, where det ≈ 0), make the
+// pixel marginal.
+constexpr double EPS32 = 5.9604644775390625e-8;  // 2^-24
+constexpr double COND_K = 16.0;
+constexpr double COND_MAX_DQ = 1e-2;
 
 struct V3 {
   double x = 0, y = 0, z = 0;
@@ -330,6 +341,7 @@ struct Hit {
   bool ray_branch;
   double u, v, t;
   bool branch_marginal;
+  double q, dq;  // exponent of ghat (ghat = exp(−q)) and its float32 error bound
 };
 
 // forward.rs:136-169
@@ -337,19 +349,34 @@ inline Hit evaluate(const SurfelCam& sc, const V3& d, double pix_x, double pix_y
   V3 s = -d;
   double det = triple(sc.tu, sc.tv, s);
   double g_ray = 0, u = 0, v = 0, t = 0;
+  double q_ray = INFINITY, dq_ray = 0.0;
   bool marg = false;
+  const double e = COND_K * EPS32;
   if (std::fabs(det) > 1e-12) {
     u = triple(-sc.c, sc.tv, s) / det;
     v = triple(sc.tu, -sc.c, s) / det;
     t = triple(sc.tu, sc.tv, -sc.c) / det;
-    if (t > NEAR_DEPTH) g_ray = std::exp(-(u * u + v * v) * 0.5);
-    if (std::fabs(t - NEAR_DEPTH) < 1e-6) marg = true;
+    const double ns = length(s), ntu = length(sc.tu), ntv = length(sc.tv), nc = length(sc.c);
+    const double ddet = e * ns * ntu * ntv, adet = std::fabs(det);
+    const double du = (e * ns * ntv * nc + std::fabs(u) * ddet) / adet;
+    const double dv = (e * ns * nc * ntu + std::fabs(v) * ddet) / adet;
+    const double dt = (e * nc * ntu * ntv + std::fabs(t) * ddet) / adet;
+    if (t > NEAR_DEPTH) {
+      q_ray = (u * u + v * v) * 0.5;
+      dq_ray = std::fabs(u) * du + std::fabs(v) * dv;
+      g_ray = std::exp(-q_ray);
+    }
+    if (std::fabs(t - NEAR_DEPTH) < 1e-6 + dt) marg = true;
   }
   double dx = pix_x - sc.px, dy = pix_y - sc.py;
-  double g_scr = std::exp(-(dx * dx + dy * dy) / (2.0 * LOWPASS_SIGMA2));
+  const double q_scr = (dx * dx + dy * dy) / (2.0 * LOWPASS_SIGMA2);
+  const double dq_scr = (std::fabs(dx) * e * (std::fabs(sc.px) + pix_x) + std::fabs(dy) * e * (std::fabs(sc.py) + pix_y)) /
+                        LOWPASS_SIGMA2;
+  double g_scr = std::exp(-q_scr);
   if (std::fabs(g_ray - g_scr) < MARGIN_BRANCH * std::max(1.0, g_scr) && (g_ray > 0 || g_scr > 0)) marg = true;
-  if (g_ray >= g_scr) return {g_ray, true, u, v, t, marg};
-  return {g_scr, false, u, v, sc.depth, marg};
+  if (std::fabs(q_ray - q_scr) < dq_ray + dq_scr) marg = true;
+  if (g_ray >= g_scr) return {g_ray, true, u, v, t, marg, q_ray, dq_ray};
+  return {g_scr, false, u, v, sc.depth, marg, q_scr, dq_scr};
 }
 
 // Per-tile entry lists in depth order: list[tile] = indices into the sorted
@@ -395,8 +422,13 @@ inline void render_pixel(const std::vector<SurfelCam>& sc, const std::vector<int
     double alpha = std::min(raw, ALPHA_CLAMP);
     if (std::fabs(alpha - ALPHA_SKIP) < MARGIN_ALPHA) marg = true;
     if (std::fabs(raw - ALPHA_CLAMP) < MARGIN_ALPHA) marg = true;
+    if (s.opacity > 0.0) {  // the skip and clamp decisions in exponent space, within the float32 bound
+      if (std::fabs(h.q - std::log(255.0 * s.opacity)) < h.dq) marg = true;
+      if (s.opacity > ALPHA_CLAMP && std::fabs(h.q - std::log(s.opacity / ALPHA_CLAMP)) < h.dq) marg = true;
+    }
     if (alpha < ALPHA_SKIP) continue;
     if (h.branch_marginal) marg = true;
+    if (h.dq > COND_MAX_DQ) marg = true;  // an ill-conditioned contribution
     double w = T * alpha;
     col += s.color * w;
     a += w;

@@ -3,7 +3,11 @@ storage of SH and projected record fields (geometry, compositing and
 accumulation stay FP32), each against the FP64 oracle (tile-binned walk) on
 the same f32-rounded scene: image PSNR and, for the linear loss Σ w·colour,
 the relative L2 error of each parameter class's gradient. Pixels the oracle
-flags as marginal carry no loss weight and are left out of the PSNR.
+flags as marginal carry no loss weight and are left out of the PSNR; besides
+the fixed bands around the α, clamp, transmittance and branch thresholds, the
+oracle flags a pixel where a float32 evaluation of a hit's exponent is
+ill-conditioned (surfels seen nearly edge-on, where the ray–splat solve divides
+by det ≈ 0) or a decision lies within that error bound.
 
 Default size: 200,000 clustered surfels (SH degree 3) and one 1280×720 view.
 With GS_PRECISION_FULL=1: 3,000,000 surfels and four 1920×1080 views."""
@@ -21,7 +25,7 @@ pytestmark = pytest.mark.gpu
 
 CLASSES = (("pos", 4, 3), ("scales", 2, 2), ("quat", 4, 4), ("opacity", 1, 1), ("sh", 48, 48))
 MIN_PSNR = {"f32": 60.0, "f16": 50.0, "bf16": 40.0}
-MAX_GRAD_ERR = {"f32": 5e-3, "f16": 2e-2, "bf16": 8e-2}
+MAX_GRAD_ERR = {"f32": 1e-3, "f16": 2e-3, "bf16": 1e-2}
 
 
 def _setup():
