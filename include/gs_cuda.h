@@ -183,8 +183,11 @@ gs_status gs_rasterizer_read(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_of
                              void* stream);
 gs_status gs_rasterizer_write(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_offset, const void* host, size_t bytes,
                               void* stream);
-/* Asynchronous variants: host memory must be pinned and stay valid until the
- * stream reaches the copy. */
+/* Asynchronous variants: the other side may be pinned host memory or device
+ * memory (the direction follows from the pointer, cudaMemcpyDefault), and
+ * must stay valid until the stream reaches the copy. A device source lets a
+ * caller prefetch the next step's input on another stream and move it into
+ * the handle with a device-to-device copy. */
 gs_status gs_rasterizer_read_async(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_offset, void* host, size_t bytes,
                                    void* stream);
 gs_status gs_rasterizer_write_async(gs_rasterizer* r, gs_buffer_id id, uint64_t byte_offset, const void* host,

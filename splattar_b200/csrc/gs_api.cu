@@ -922,7 +922,7 @@ gs_status gs_rasterizer_read_async(gs_rasterizer* r, gs_buffer_id id, uint64_t o
   void* d = nullptr;
   gs_status s = copy_common(r, id, off, bytes, &d);
   if (s) return s;
-  TRY_CUDA(r, cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, S(stream)));
+  TRY_CUDA(r, cudaMemcpyAsync(host, d, bytes, cudaMemcpyDefault, S(stream)));  // host or device destination
   return GS_OK;
 }
 
@@ -932,7 +932,7 @@ gs_status gs_rasterizer_write_async(gs_rasterizer* r, gs_buffer_id id, uint64_t 
   void* d = nullptr;
   gs_status s = copy_common(r, id, off, bytes, &d);
   if (s) return s;
-  TRY_CUDA(r, cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, S(stream)));
+  TRY_CUDA(r, cudaMemcpyAsync(d, host, bytes, cudaMemcpyDefault, S(stream)));  // host or device source
   return GS_OK;
 }
 

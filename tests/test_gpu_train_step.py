@@ -246,3 +246,22 @@ def test_stored_state_backward_matches_recompute(deterministic):
             assert np.array_equal(outs[0][k], outs[1][k]), k
         else:
             assert np.allclose(outs[0][k], outs[1][k], rtol=1e-5, atol=1e-6), k
+
+
+def test_async_copies_take_device_pointers():
+    """write_async/read_async move data between a handle buffer and either
+    pinned host memory or device memory (a prefetched input on the device)."""
+    import torch
+    r = Rasterizer(100, 64, 32)
+    P = 64 * 32
+    src = torch.arange(4 * P, dtype=torch.float32, device="cuda")
+    r.write_async("target", src.data_ptr(), src.numel() * 4, 0, 0)
+    back = torch.zeros_like(src)
+    r.read_async("target", back.data_ptr(), back.numel() * 4, 0, 0)
+    r.check()
+    assert np.array_equal(r.read("target", 4 * P), src.cpu().numpy())
+    assert torch.equal(back, src)
+    host = torch.full((4 * P,), 7.0).pin_memory()
+    r.write_async("target", host.data_ptr(), host.numel() * 4, 0, 0)
+    r.check()
+    assert np.all(r.read("target", 4 * P) == 7.0)
