@@ -350,10 +350,13 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   TRY_LAUNCH(r, launch_expand(ea, st));
   mark(prof, 2, st);
   const int bits = tile_key_bits((uint32_t)std::max(tiles, 1));
+  // The tile sort's final pass also records each tile's range; the fix-up
+  // turns it into [start, end).
+  TRY_CUDA(r, cudaMemsetAsync(r->ranges, 0, sizeof(uint2) * (size_t)tiles, st));
   TRY_LAUNCH(r, launch_radix_sort_pairs(r->ent_pairs[0], r->ent_pairs[1], r->max_entries, n_entries, bits,
-                                        r->sort_scratch, &r->ent_in1, st));
+                                        r->sort_scratch, &r->ent_in1, st, r->ranges, (uint32_t)tiles));
   mark(prof, 3, st);
-  TRY_LAUNCH(r, launch_ranges(r->ent_pairs[r->ent_in1], r->entry_total, r->max_entries, r->ranges, (uint32_t)tiles, st));
+  TRY_LAUNCH(r, launch_ranges_fix(r->ranges, (uint32_t)tiles, st));
   mark(prof, 4, st);
   RasterArgs ra{};
   ra.views = vdev; ra.n_views = (int)nv; ra.total_tiles = tiles;

@@ -143,7 +143,12 @@ int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, ui
                       int key_bits, void* scratch, int* result_in_1, cudaStream_t st);
 // The same sort on interleaved (key, val) pairs, ping-ponging between p0 and p1.
 int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch,
-                            int* result_in_1, cudaStream_t st);
+                            int* result_in_1, cudaStream_t st, uint2* ranges = nullptr, uint32_t num_ranges = 0);
+// With `ranges` (zero-filled, num_ranges entries) the sort's final pass also
+// records each key's output range; launch_ranges_fix then converts it to
+// [start, end) per key ((0, 0) for absent keys) — the tile ranges without a
+// separate pass over the sorted entries.
+int launch_ranges_fix(uint2* ranges, uint32_t num_tiles, cudaStream_t st);
 // dst[i] = src[i].y for i < min(*n, capacity).
 int launch_pair_values(const uint2* src, uint32_t* dst, const unsigned long long* n, uint64_t capacity,
                        cudaStream_t st);

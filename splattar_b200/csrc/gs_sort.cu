@@ -181,10 +181,18 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(IO io, uint64_t n_hos
   }
 }
 
+// ranges (final pass of a key sort only, else null): every run of one key
+// inside a staged tile is folded into that key's output range, stored as
+// (~first position, one past the last position) with atomicMax on both, so
+// the zero-filled buffer needs no other initialisation (launch_ranges_fix
+// turns it into [start, end) afterwards). Staged tiles are ordered by the
+// full key in the final pass: by this pass's digit, and within a digit by
+// the lower digits the earlier passes sorted.
 template <class IO>
 __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_downsweep(IO io, uint64_t n_host, const uint32_t* n_dev,
                                                                 int shift, int nbits,
-                                                                const uint32_t* __restrict__ hist) {
+                                                                const uint32_t* __restrict__ hist,
+                                                                uint2* ranges, uint32_t num_ranges) {
   __shared__ uint2 s_e[RS_TILE];
   __shared__ uint32_t s_wh[RS_WARPS][RS_BINS];
   __shared__ uint32_t s_start[RS_BINS], s_gofs[RS_BINS], s_run[RS_BINS];
@@ -264,7 +272,12 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_downsweep(IO io, uint64_t 
 #pragma unroll 4
     for (int i = tid; i < tn; i += RS_THREADS) {
       const uint2 v = s_e[i];
-      io.store((size_t)(s_gofs[(v.x >> shift) & mask] + (uint32_t)i), v);
+      const uint32_t pos = s_gofs[(v.x >> shift) & mask] + (uint32_t)i;
+      io.store((size_t)pos, v);
+      if (ranges != nullptr && v.x < num_ranges) {
+        if (i == 0 || s_e[i - 1].x != v.x) atomicMax(&ranges[v.x].x, ~pos);
+        if (i == tn - 1 || s_e[i + 1].x != v.x) atomicMax(&ranges[v.x].y, pos + 1u);
+      }
     }
     __syncthreads();
   }
@@ -415,7 +428,7 @@ int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_
 
 template <class IO, class SWAP>
 int radix_passes(IO io, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch, int* result_in_1,
-                 cudaStream_t st, SWAP swap) {
+                 cudaStream_t st, SWAP swap, uint2* ranges = nullptr, uint32_t num_ranges = 0) {
   auto* hist = reinterpret_cast<uint32_t*>(scratch);
   int in1 = 0;
   for (int shift = 0; shift < key_bits; shift += 8) {
@@ -424,7 +437,9 @@ int radix_passes(IO io, uint64_t n_host, const uint32_t* n_dev, int key_bits, vo
     const int e = launch_scan(hist, nullptr, hist, (uint64_t)RS_BINS * SORT_GRID, nullptr, nullptr, nullptr,
                               hist + RS_BINS * SORT_GRID, st);
     if (e) return e;
-    k_rs_downsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist);
+    const bool last = shift + 8 >= key_bits;
+    k_rs_downsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist,
+                                                         last ? ranges : nullptr, num_ranges);
     swap(io);
     in1 ^= 1;
   }
@@ -442,12 +457,15 @@ int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, ui
 }
 
 int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch,
-                            int* result_in_1, cudaStream_t st) {
+                            int* result_in_1, cudaStream_t st, uint2* ranges, uint32_t num_ranges) {
   PairIO io{p0, p1};
-  return radix_passes(io, n_host, n_dev, key_bits, scratch, result_in_1, st, [](PairIO& x) {
-    PairIO y{x.out, const_cast<uint2*>(x.in)};
-    x = y;
-  });
+  return radix_passes(
+      io, n_host, n_dev, key_bits, scratch, result_in_1, st,
+      [](PairIO& x) {
+        PairIO y{x.out, const_cast<uint2*>(x.in)};
+        x = y;
+      },
+      ranges, num_ranges);
 }
 
 int launch_expand(const ExpandArgs& a, cudaStream_t st) {
@@ -464,6 +482,15 @@ int launch_ranges(const uint2* sorted_pairs, const unsigned long long* total, ui
 }
 
 namespace {
+// (~first, end) from the final sort pass → [first, end); (0, 0) for a key no
+// element carried.
+__global__ void __launch_bounds__(256) k_ranges_fix(uint2* ranges, uint32_t num_tiles) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles; t += gridDim.x * blockDim.x) {
+    const uint2 r = ranges[t];
+    ranges[t] = r.y ? make_uint2(~r.x, r.y) : make_uint2(0u, 0u);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_tile_words(const uint2* ranges, uint32_t num_tiles, uint32_t* words) {
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles; t += gridDim.x * blockDim.x) {
     const uint2 r = ranges[t];
@@ -471,6 +498,12 @@ __global__ void __launch_bounds__(256) k_tile_words(const uint2* ranges, uint32_
   }
 }
 }  // namespace
+
+int launch_ranges_fix(uint2* ranges, uint32_t num_tiles, cudaStream_t st) {
+  if (num_tiles == 0) return 0;
+  k_ranges_fix<<<grid_for(num_tiles, 256, 148 * 8), 256, 0, st>>>(ranges, num_tiles);
+  return (int)cudaGetLastError();
+}
 
 int launch_mask_offsets(const uint2* ranges, uint32_t num_tiles, uint32_t* words, uint32_t* mask_off, void* scratch,
                         cudaStream_t st) {

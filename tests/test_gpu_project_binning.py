@@ -217,3 +217,27 @@ def test_entry_capacity_overflow_is_reported_not_written():
     rast.forward(raster_camera(cam, 1), scene.n)
     with pytest.raises(GsError, match="GS_ERR_CAPACITY"):
         rast.check()
+
+
+@pytest.mark.parametrize("tight,tile", [(False, 16), (True, 16), (True, 8), (False, 32)])
+def test_rasterizer_tile_ranges_match_sorted_entries(tight, tile):
+    """The tile sort's final pass records each tile's [start, end) in the
+    sorted entry list (empty tiles (0, 0)); the result equals the ranges read
+    off the sorted keys on the host."""
+    s = make_surfels(20_000, 5, True, 1, 0.1)
+    cams = ring_cameras([(640, 480), (320, 200)])
+    P = sum(c.width * c.height for c in cams)
+    r = Rasterizer(s.n, 0, 0, 300 * s.n, max_views=2, max_pixels=P, tight=tight, tile=tile)
+    r.upload_scene(s.scene_input())
+    r.forward(cams, s.n)
+    r.check()
+    E = r.entry_count()
+    keys = r.read("sorted_items", 2 * E).reshape(E, 2)[:, 0].astype(np.int64)
+    assert np.all(np.diff(keys) >= 0)
+    tiles = sum(((c.width + tile - 1) // tile) * ((c.height + tile - 1) // tile) for c in cams)
+    want = np.zeros((tiles, 2), np.int64)
+    present = np.unique(keys)
+    want[present, 0] = np.searchsorted(keys, present, side="left")
+    want[present, 1] = np.searchsorted(keys, present, side="right")
+    got = r.read("ranges", 2 * tiles).reshape(tiles, 2).astype(np.int64)
+    assert np.array_equal(got, want)
