@@ -308,8 +308,8 @@ __host__ __device__ constexpr int pba_threads(int views) { return (views * pba_s
 // Gradient slots: per (view, surfel) thread (ordered: summed over views in
 // view order in phase 2) or per surfel (atomic: views add into one slot).
 __host__ __device__ constexpr size_t pba_smem(int views, bool ordered) {
-  return sizeof(float) * ((size_t)PBA_PARAMS * 3 * pba_surfels(views) + (size_t)SH_FLOATS * pba_surfels(views) +
-                          (size_t)PBA_SLOTS * (ordered ? pba_threads(views) + 1 : pba_surfels(views)));
+  return sizeof(float) * ((size_t)PBA_PARAMS * 3 * pba_surfels(views) + (size_t)SH_FLOATS * (pba_surfels(views) + 1) +
+                          (size_t)PBA_SLOTS * (ordered ? pba_threads(views) + 1 : pba_surfels(views) + 1));
 }
 
 struct GeoGrads {
@@ -386,10 +386,14 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
   __shared__ uint64_t s_bar;
   const int tid = threadIdx.x;
   const int V = a.n_views, S = pba_surfels(V), NT = blockDim.x;
-  const int PITCH = ORD ? NT + 1 : S;                  // slot stride
+  // Slot and SH strides are one more than a multiple of 32 floats, so the
+  // threads of a warp that walk consecutive slots (or coefficients) of one
+  // surfel hit distinct banks.
+  const int PITCH = ORD ? NT + 1 : S + 1;              // slot stride
+  const int SHP = S + 1;                               // SH coefficient stride
   float* s_stage = s_dyn;                              // [class][raw|m|v][S*W]
-  float* s_sh = s_stage + PBA_PARAMS * 3 * S;          // [SH_FLOATS][S]: the block's activated SH, transposed
-  float* s_g = s_sh + SH_FLOATS * S;                   // [PBA_SLOTS][PITCH]
+  float* s_sh = s_stage + PBA_PARAMS * 3 * S;          // [SH_FLOATS][SHP]: the block's activated SH, transposed
+  float* s_g = s_sh + SH_FLOATS * SHP;                 // [PBA_SLOTS][PITCH]
   const uint32_t i0 = blockIdx.x * (uint32_t)S;
   if (tid == 0) mbar_init(&s_bar);
   __syncthreads();
@@ -416,7 +420,7 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
       const uint32_t w[4] = {u.x, u.y, u.z, u.w};
       if constexpr (PREC == 0) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) s_sh[(f0 + j) * S + sl] = __uint_as_float(w[j]);
+        for (int j = 0; j < 4; ++j) s_sh[(f0 + j) * SHP + sl] = __uint_as_float(w[j]);
       } else {
         using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
 #pragma unroll
@@ -425,14 +429,14 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
           const unsigned short bl = (unsigned short)(w[j] & 0xffffu), bh = (unsigned short)(w[j] >> 16);
           memcpy(&lo, &bl, 2);
           memcpy(&hi, &bh, 2);
-          s_sh[(f0 + 2 * j) * S + sl] = h2f<H>(lo);
-          s_sh[(f0 + 2 * j + 1) * S + sl] = h2f<H>(hi);
+          s_sh[(f0 + 2 * j) * SHP + sl] = h2f<H>(lo);
+          s_sh[(f0 + 2 * j + 1) * SHP + sl] = h2f<H>(hi);
         }
       }
     }
   }
   if (!ORD)
-    for (int k = tid; k < PBA_SLOTS * S; k += NT) s_g[k] = 0.0f;
+    for (int k = tid; k < PBA_SLOTS * PITCH; k += NT) s_g[k] = 0.0f;
   __syncthreads();
   // ---- phase 1
   {
@@ -457,7 +461,7 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
         const Cam k = load_cam(a.views, v);
         const float* shc = s_sh + sl;
         chain_core<PREC, AUX>(k, __ldg(a.pos + i), __ldg(a.scales + i), __ldg(a.quats + i),
-                              [&](int kk) { return f3(shc[(3 * kk) * S], shc[(3 * kk + 1) * S], shc[(3 * kk + 2) * S]); },
+                              [&](int kk) { return f3(shc[(3 * kk) * SHP], shc[(3 * kk + 1) * SHP], shc[(3 * kk + 2) * SHP]); },
                               G, o, [&](int kk, float3 g) {
                                 put(10 + 3 * kk, g.x);
                                 put(11 + 3 * kk, g.y);
