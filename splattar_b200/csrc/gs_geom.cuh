@@ -132,10 +132,17 @@ __device__ __forceinline__ float3 sh_coeff(const void* sh, size_t i, int k) {
 template <class Coeff>
 __device__ __forceinline__ float3 sh_raw_color_with(Coeff coeff, int deg, float3 dir, float b[16], int& nb) {
   nb = sh_basis(deg, dir, b);
+  // Explicit FMAs: the projection (built without contraction) and its
+  // adjoint (built with it) then round the raw colour identically, so they
+  // agree on its clamp at zero.
   float3 acc = f3(0, 0, 0);
 #pragma unroll
-  for (int k = 0; k < 16; ++k)  // constant indices keep b[] in registers
-    if (k < nb) acc += coeff(k) * b[k];
+  for (int k = 0; k < 16; ++k) {  // constant indices keep b[] in registers
+    if (k < nb) {
+      const float3 c = coeff(k);
+      acc = f3(fmaf(c.x, b[k], acc.x), fmaf(c.y, b[k], acc.y), fmaf(c.z, b[k], acc.z));
+    }
+  }
   return acc + f3(0.5f, 0.5f, 0.5f);
 }
 template <int PREC>
