@@ -14,24 +14,27 @@
 namespace gs {
 namespace {
 
-// Range of f·N(θ)/D(θ) over θ for N = a0 + a1 cosθ + a2 sinθ and
+// Range of N(θ)/D(θ) over θ for N = a0 + a1 cosθ + a2 sinθ and
 // D = b0 + b1 cosθ + b2 sinθ > 0: the extremes solve
-// (a0 b1 − a1 b0) sinθ + (a2 b0 − a0 b2) cosθ + (a2 b1 − a1 b2) = 0.
+// P sinθ + Q cosθ + R = 0 with P = a0 b1 − a1 b0, Q = a2 b0 − a0 b2,
+// R = a2 b1 − a1 b2. On the unit circle (s, c) = (sinθ, cosθ) that line meets
+// it at (s, c) = (−R·(P, Q) ± (Q, −P)·√(h² − R²)) / h², h² = P² + Q². The
+// result only bounds a box that gets a pixel of margin, so divisions are the
+// fast ones.
 __device__ __forceinline__ void ratio_range(float a0, float a1, float a2, float b0, float b1, float b2, float& lo,
                                             float& hi) {
   const float P = a0 * b1 - a1 * b0, Q = a2 * b0 - a0 * b2, R = a2 * b1 - a1 * b2;
-  const float h = sqrtf(P * P + Q * Q);
+  const float h2 = P * P + Q * Q;
   // Interval bound, always valid: |N| ≤ |a0| + |(a1,a2)|, D ≥ b0 − |(b1,b2)|.
-  const float na = sqrtf(a1 * a1 + a2 * a2), dmin = b0 - sqrtf(b1 * b1 + b2 * b2);
-  float blo = (a0 - na) / (a0 - na < 0.f ? dmin : b0 + sqrtf(b1 * b1 + b2 * b2));
-  float bhi = (a0 + na) / (a0 + na > 0.f ? dmin : b0 + sqrtf(b1 * b1 + b2 * b2));
-  if (h > 1e-12f && fabsf(R) <= h) {
-    const float phi = atan2f(P, Q), dth = acosf(fminf(fmaxf(-R / h, -1.f), 1.f));
-    float s0, c0, s1, c1;
-    sincosf(phi + dth, &s0, &c0);
-    sincosf(phi - dth, &s1, &c1);
-    const float v0 = (a0 + a1 * c0 + a2 * s0) / (b0 + b1 * c0 + b2 * s0);
-    const float v1 = (a0 + a1 * c1 + a2 * s1) / (b0 + b1 * c1 + b2 * s1);
+  const float na = sqrtf(a1 * a1 + a2 * a2), nb = sqrtf(b1 * b1 + b2 * b2), dmin = b0 - nb;
+  float blo = __fdividef(a0 - na, a0 - na < 0.f ? dmin : b0 + nb);
+  float bhi = __fdividef(a0 + na, a0 + na > 0.f ? dmin : b0 + nb);
+  if (h2 > 1e-24f && R * R <= h2) {
+    const float w = sqrtf(h2 - R * R), ih2 = __fdividef(1.0f, h2);
+    const float s0 = (-R * P + Q * w) * ih2, c0 = (-R * Q - P * w) * ih2;
+    const float s1 = (-R * P - Q * w) * ih2, c1 = (-R * Q + P * w) * ih2;
+    const float v0 = __fdividef(a0 + a1 * c0 + a2 * s0, b0 + b1 * c0 + b2 * s0);
+    const float v1 = __fdividef(a0 + a1 * c1 + a2 * s1, b0 + b1 * c1 + b2 * s1);
     lo = fmaxf(fminf(v0, v1), blo);
     hi = fminf(fmaxf(v0, v1), bhi);
     if (!(lo <= hi)) { lo = blo; hi = bhi; }
