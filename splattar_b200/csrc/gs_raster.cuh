@@ -430,13 +430,18 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
   // (16-pixel tiles): entries no pixel of a group composited are skipped for
   // that group's pixels without evaluating them.
   constexpr bool GM = !AUX && !MASK && TS == 16;
+  // A single-warp CTA (8 pixels per thread on 16-pixel tiles) has nothing to
+  // sum across warps: the lanes holding each group of four reduced components
+  // gather them by shuffles and emit the vector reduction (or ordered store)
+  // at once, without staging them in shared memory.
+  constexpr bool DIRECT = !AUX && NW == 1;
   __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
   __shared__ float4 s_r4[AUX ? BATCH : 1];
   __shared__ uint32_t s_item[BATCH];
   __shared__ uint32_t s_q[DET ? BATCH : 1];
   __shared__ int s_j[BATCH];
   __shared__ uint8_t s_gm[GM ? BATCH : 1];
-  __shared__ float s_part[NW][BATCH][NG];
+  __shared__ float s_part[DIRECT ? 1 : NW][DIRECT ? 1 : BATCH][NG];
   __shared__ int s_wcount[2][NW];
   __shared__ int s_tile, s_maxnc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -448,6 +453,23 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
     thread_gbits |= pbit[p];
   }
   const uint32_t warp_gbits = __reduce_or_sync(FULL, thread_gbits);
+  // Results of staged entry k: group q4 of four reduced components, or zeros
+  // for an entry this warp's pixels did not composite.
+  auto emit4 = [&](int k, int q4, float s0, float s1, float s2, float s3) {
+    if (DET) {
+      reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[q4] = make_float4(s0, s1, s2, s3);
+    } else if (s0 != 0.f || s1 != 0.f || s2 != 0.f || s3 != 0.f) {
+      red_add_v4(a.grad_geom + (size_t)s_item[k] * GG_STRIDE + 4 * q4, s0, s1, s2, s3);
+    }
+  };
+  auto emit_zero = [&](int k) {
+    if constexpr (DIRECT) {
+      if (DET && lane < NQ) emit4(k, lane, 0.f, 0.f, 0.f, 0.f);
+    } else {
+      if (lane < 16) s_part[warp][k][lane] = 0.f;
+      if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
+    }
+  };
   int tile = blockIdx.x;
   for (;;) {
     if (PERSIST) {
@@ -568,8 +590,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
       for (int k = kept - 1; k >= 0; --k) {
         const uint32_t cidx = lo - range.x + (uint32_t)s_j[k];
         if (cidx >= warp_maxnc) {
-          if (lane < 16) s_part[warp][k][lane] = 0.f;
-          if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
+          emit_zero(k);
           continue;
         }
         bool bit[PPT];
@@ -589,7 +610,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             }
           }
           if (!__any_sync(FULL, anybit)) {  // no pixel of this warp composited the entry
-            if (lane < 16) s_part[warp][k][lane] = 0.f;
+            emit_zero(k);
             continue;
           }
         }
@@ -597,7 +618,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
         if (GM) {
           gm = s_gm[k];
           if (!(gm & warp_gbits)) {  // no pixel of this warp's row groups composited the entry
-            if (lane < 16) s_part[warp][k][lane] = 0.f;
+            emit_zero(k);
             continue;
           }
         }
@@ -704,7 +725,14 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
 #pragma unroll
           for (int c = 0; c < 16; ++c) lo16[c] = gg[c];
           const float r = warp_reduce16(lo16);
-          if (!(lane & 1)) s_part[warp][k][lane >> 1] = r;
+          if constexpr (DIRECT) {
+            // component c sits in lanes 2c and 2c+1: lane 8q gathers 4q..4q+3
+            const float r1 = __shfl_down_sync(FULL, r, 2), r2 = __shfl_down_sync(FULL, r, 4);
+            const float r3 = __shfl_down_sync(FULL, r, 6);
+            if ((lane & 7) == 0) emit4(k, lane >> 3, r, r1, r2, r3);
+          } else {
+            if (!(lane & 1)) s_part[warp][k][lane >> 1] = r;
+          }
           if (AUX) {
             float hi16[16];
 #pragma unroll
@@ -713,14 +741,13 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             if (!(lane & 1)) s_part[warp][k][16 + (lane >> 1)] = r2;
           }
         } else {
-          if (lane < 16) s_part[warp][k][lane] = 0.f;
-          if (AUX && lane >= 16) s_part[warp][k][lane] = 0.f;
+          emit_zero(k);
         }
       }
       __syncthreads();
       // Cross-warp sum in fixed warp order, then one vector reduction (or
       // one ordered store) per 4 components.
-      for (int w4 = tid; w4 < kept * NQ; w4 += NT) {
+      for (int w4 = tid; !DIRECT && w4 < kept * NQ; w4 += NT) {
         const int k = w4 / NQ, q4 = w4 % NQ;
         float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
@@ -728,11 +755,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
           s0 += s_part[ww][k][4 * q4]; s1 += s_part[ww][k][4 * q4 + 1];
           s2 += s_part[ww][k][4 * q4 + 2]; s3 += s_part[ww][k][4 * q4 + 3];
         }
-        if (DET) {
-          reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[q4] = make_float4(s0, s1, s2, s3);
-        } else if (s0 != 0.f || s1 != 0.f || s2 != 0.f || s3 != 0.f) {
-          red_add_v4(a.grad_geom + (size_t)s_item[k] * GG_STRIDE + 4 * q4, s0, s1, s2, s3);
-        }
+        emit4(k, q4, s0, s1, s2, s3);
       }
       __syncthreads();
       hi = lo;
