@@ -106,6 +106,10 @@ struct gs_rasterizer {
   // groups it composited into (read by the matching backward)
   uint8_t* gmask = nullptr;
   bool gmask_valid = false;
+  // persistent raster kernels: tiles in heaviest-first order (from the ranges
+  // of the last persistent forward)
+  uint32_t* tile_order = nullptr;
+  bool order_valid = false;
 
   // device scalars: [0] entry total u64, then u32 words
   unsigned long long* entry_total = nullptr;
@@ -357,6 +361,8 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
                                         r->sort_scratch, &r->ent_in1, st, r->ranges, (uint32_t)tiles));
   mark(prof, 3, st);
   TRY_LAUNCH(r, launch_ranges_fix(r->ranges, (uint32_t)tiles, st));
+  r->order_valid = persistent;
+  if (persistent) TRY_LAUNCH(r, launch_tile_order(r->ranges, (uint32_t)tiles, r->tile_order, st));
   mark(prof, 4, st);
   RasterArgs ra{};
   ra.views = vdev; ra.n_views = (int)nv; ra.total_tiles = tiles;
@@ -364,6 +370,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ra.records = r->records;
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.tile_counter = r->words + 2;
+  ra.tile_order = persistent ? r->tile_order : nullptr;
   r->mask_valid = r->stored_state && color && persistent && r->tile == 16;
   r->gmask_valid = color && persistent && r->tile == 16 && !r->mask_valid && r->gmask != nullptr;
   if (r->gmask_valid) ra.gmask = r->gmask;
@@ -396,6 +403,7 @@ RasterArgs bwd_args(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, int til
   ra.grad_geom = r->grad_geom; ra.partials = r->partials;
   ra.lambda_dist = r->lambda_dist;
   ra.tile_counter = r->words + 3;
+  ra.tile_order = r->order_valid ? r->tile_order : nullptr;
   return ra;
 }
 
@@ -692,6 +700,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
     ALLOC(r->entry_offset, I);
   }
   ALLOC(r->ranges, r->max_tiles);
+  ALLOC(r->tile_order, r->max_tiles);
   if (r->stored_state) {
     // One bit per (pixel, tile entry): 32 bytes per entry, whole 32-entry words per tile.
     ALLOC(r->mask, ((size_t)E / 32 + r->max_tiles) * 256);
@@ -750,7 +759,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->dl_dcolor, r->dl_dnormal, r->target, r->out_nc, r->coef, r->loss_sums, r->grad_geom,
                   r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
                   r->accum_norm, r->dyn_dev, r->dens_flags, r->dens_slots, r->dens_tmp, r->views_dev,
-                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask,
+                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask, r->tile_order,
                   r->normal_loss_sums,
                   r->mask_words,
                   r->scan_scratch, r->sort_scratch};

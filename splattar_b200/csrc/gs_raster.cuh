@@ -258,7 +258,11 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
   int tile = blockIdx.x;
   for (;;) {
     if (PERSIST) {
-      if (tid == 0) s_tile = (int)atomicAdd(a.tile_counter, 1u);
+      if (tid == 0) {
+        const uint32_t slot = atomicAdd(a.tile_counter, 1u);
+        // heaviest tiles first when an order is given (a shorter tail)
+        s_tile = (int)(a.tile_order != nullptr && slot < (uint32_t)a.total_tiles ? __ldg(a.tile_order + slot) : slot);
+      }
       __syncthreads();
       tile = s_tile;
       if (tile >= a.total_tiles) return;
@@ -473,7 +477,11 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
   int tile = blockIdx.x;
   for (;;) {
     if (PERSIST) {
-      if (tid == 0) s_tile = (int)atomicAdd(a.tile_counter, 1u);
+      if (tid == 0) {
+        const uint32_t slot = atomicAdd(a.tile_counter, 1u);
+        // heaviest tiles first when an order is given (a shorter tail)
+        s_tile = (int)(a.tile_order != nullptr && slot < (uint32_t)a.total_tiles ? __ldg(a.tile_order + slot) : slot);
+      }
       __syncthreads();
       tile = s_tile;
       if (tile >= a.total_tiles) return;

@@ -505,6 +505,39 @@ int launch_ranges_fix(uint2* ranges, uint32_t num_tiles, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+namespace {
+__global__ void __launch_bounds__(1024) k_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order) {
+  __shared__ uint32_t s_cnt[33];
+  const int tid = threadIdx.x;
+  if (tid < 33) s_cnt[tid] = 0u;
+  __syncthreads();
+  for (uint32_t t = tid; t < num_tiles; t += blockDim.x) {
+    const uint2 r = ranges[t];
+    atomicAdd(&s_cnt[32 - __clz(r.y - r.x + 1u)], 1u);  // bucket ⌊log2(len + 1)⌋ + 1 ∈ [1, 32]
+  }
+  __syncthreads();
+  if (tid == 0) {  // exclusive offsets, heaviest bucket first
+    uint32_t run = 0;
+    for (int b = 32; b >= 0; --b) {
+      const uint32_t c = s_cnt[b];
+      s_cnt[b] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  for (uint32_t t = tid; t < num_tiles; t += blockDim.x) {
+    const uint2 r = ranges[t];
+    order[atomicAdd(&s_cnt[32 - __clz(r.y - r.x + 1u)], 1u)] = t;
+  }
+}
+}  // namespace
+
+int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, cudaStream_t st) {
+  if (num_tiles == 0) return 0;
+  k_tile_order<<<1, 1024, 0, st>>>(ranges, num_tiles, order);
+  return (int)cudaGetLastError();
+}
+
 int launch_mask_offsets(const uint2* ranges, uint32_t num_tiles, uint32_t* words, uint32_t* mask_off, void* scratch,
                         cudaStream_t st) {
   if (num_tiles == 0) return 0;
