@@ -210,14 +210,15 @@ def launches_per_step(n_tiles: int, nv: int, form: str) -> int:
     upsweep + 3-kernel histogram scan + downsweep); entry scan (3) and entry
     guard; expansion; tile sort (same passes over the tile-id bits); ranges;
     forward raster; L1+SSIM (2); backward raster; projection backward + Adam
-    (chosen form, which also orders its tiles heaviest first: one more launch).
-    Matches the ncu launch list (43 per step on ring8_1m)."""
+    (chosen form, which also orders its tiles heaviest first before each
+    raster pass: two more launches). Matches the ncu launch list (44 per step
+    on ring8_1m)."""
     bits = max(1, math.ceil(math.log2(max(n_tiles, 2))))
     tile_passes = math.ceil(bits / 8)
     per_pass = 5
     fwd = 1 + 4 * per_pass + 3 + 1 + 1 + tile_passes * per_pass + 1 + 1
     if form == "chosen":
-        return fwd + 1 + 2 + 1 + 1
+        return fwd + 1 + 2 + 1 + 1 + 1
     return nv * (fwd + 2 + 1 + 1) + 5
 
 

@@ -110,6 +110,9 @@ struct gs_rasterizer {
   // of the last persistent forward)
   uint32_t* tile_order = nullptr;
   bool order_valid = false;
+  // per tile, the largest contributor count of the last persistent forward:
+  // the backward's work, used to order its tiles
+  uint32_t* tile_walk = nullptr;
 
   // device scalars: [0] entry total u64, then u32 words
   unsigned long long* entry_total = nullptr;
@@ -362,7 +365,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   mark(prof, 3, st);
   TRY_LAUNCH(r, launch_ranges_fix(r->ranges, (uint32_t)tiles, st));
   r->order_valid = persistent;
-  if (persistent) TRY_LAUNCH(r, launch_tile_order(r->ranges, (uint32_t)tiles, r->tile_order, st));
+  if (persistent) TRY_LAUNCH(r, launch_tile_order(r->ranges, nullptr, (uint32_t)tiles, r->tile_order, st));
   mark(prof, 4, st);
   RasterArgs ra{};
   ra.views = vdev; ra.n_views = (int)nv; ra.total_tiles = tiles;
@@ -371,6 +374,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ra.out_color = r->out_color; ra.out_aux = r->out_aux; ra.out_normal = r->out_normal; ra.out_nc = r->out_nc;
   ra.tile_counter = r->words + 2;
   ra.tile_order = persistent ? r->tile_order : nullptr;
+  ra.tile_walk = persistent ? r->tile_walk : nullptr;
   r->mask_valid = r->stored_state && color && persistent && r->tile == 16;
   r->gmask_valid = color && persistent && r->tile == 16 && !r->mask_valid && r->gmask != nullptr;
   if (r->gmask_valid) ra.gmask = r->gmask;
@@ -403,7 +407,7 @@ RasterArgs bwd_args(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, int til
   ra.grad_geom = r->grad_geom; ra.partials = r->partials;
   ra.lambda_dist = r->lambda_dist;
   ra.tile_counter = r->words + 3;
-  ra.tile_order = r->order_valid ? r->tile_order : nullptr;
+  ra.tile_order = nullptr;
   return ra;
 }
 
@@ -421,6 +425,10 @@ gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t n
     TRY_CUDA(r, cudaMemsetAsync(r->words + 3, 0, sizeof(uint32_t), st));
     grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(r->tile, prec, aux, r->bwd_ppt, r->bwd_batch, r->det,
                                                               ra.mask != nullptr));
+    if (r->order_valid) {  // heaviest first by how far each tile's walk goes
+      TRY_LAUNCH(r, launch_tile_order(r->ranges, r->tile_walk, (uint32_t)tiles, r->tile_order, st));
+      ra.tile_order = r->tile_order;
+    }
   }
   TRY_LAUNCH(r, launch_raster_bwd(ra, r->tile, prec, aux, r->bwd_ppt, r->bwd_batch, r->det, persistent, grid, st));
   return GS_OK;
@@ -701,6 +709,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   }
   ALLOC(r->ranges, r->max_tiles);
   ALLOC(r->tile_order, r->max_tiles);
+  ALLOC(r->tile_walk, r->max_tiles);
   if (r->stored_state) {
     // One bit per (pixel, tile entry): 32 bytes per entry, whole 32-entry words per tile.
     ALLOC(r->mask, ((size_t)E / 32 + r->max_tiles) * 256);
@@ -759,7 +768,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->dl_dcolor, r->dl_dnormal, r->target, r->out_nc, r->coef, r->loss_sums, r->grad_geom,
                   r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
                   r->accum_norm, r->dyn_dev, r->dens_flags, r->dens_slots, r->dens_tmp, r->views_dev,
-                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask, r->tile_order,
+                  r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask, r->tile_order, r->tile_walk,
                   r->normal_loss_sums,
                   r->mask_words,
                   r->scan_scratch, r->sort_scratch};

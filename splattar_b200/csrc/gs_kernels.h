@@ -90,6 +90,7 @@ struct RasterArgs {
   float lambda_dist;
   uint32_t* tile_counter;       // persistent kernels: zeroed before each launch
   const uint32_t* tile_order;   // persistent kernels: the tile taken at each counter value (null: identity)
+  uint32_t* tile_walk;          // forward (optional): per tile, the largest contributor count of its pixels
   // Stored-state mode (16-pixel tiles): per-pixel contributor bitmasks. Word w of
   // pixel i (0..255, row-major in the tile) of tile t is mask[(mask_off[t] + w)·256 + i];
   // bit b of word w is set when list position 32w + b composited into the pixel.
@@ -150,10 +151,12 @@ int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_
 // [start, end) per key ((0, 0) for absent keys) — the tile ranges without a
 // separate pass over the sorted entries.
 int launch_ranges_fix(uint2* ranges, uint32_t num_tiles, cudaStream_t st);
-// Tile order for the persistent raster kernels: tiles bucketed by
-// ⌊log2(entries + 1)⌋, heaviest bucket first (order within a bucket is
-// arbitrary; results do not depend on it).
-int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, cudaStream_t st);
+// Tile order for the persistent raster kernels: tiles bucketed by the
+// logarithm of their work (four buckets per octave; the work is lengths[t]
+// when given, else the tile's entry count), heaviest bucket first. Order
+// within a bucket is arbitrary; results do not depend on it.
+int launch_tile_order(const uint2* ranges, const uint32_t* lengths, uint32_t num_tiles, uint32_t* order,
+                      cudaStream_t st);
 // dst[i] = src[i].y for i < min(*n, capacity).
 int launch_pair_values(const uint2* src, uint32_t* dst, const unsigned long long* n, uint64_t capacity,
                        cudaStream_t st);

@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
   __shared__ uint32_t s_gw[GM ? 4 : 1][GM ? GW : 1];
   __shared__ int s_wcount[2][NW];
   __shared__ int s_tile;
+  __shared__ uint32_t s_walk;  // tile_walk: the tile's largest contributor count
   const int tid = threadIdx.x, lane = tid & 31;
   const bool gm_on = GM && a.gmask != nullptr;
   const int g0 = L::row(tid) >> 2;  // first row group of this lane's pixels
@@ -416,6 +417,17 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
         a.out_normal[pix] = make_float4(nx[p], ny[p], nz[p], 0.f);
       }
       a.out_nc[pix] = nc[p];
+    }
+    if (a.tile_walk != nullptr) {  // how far the backward will walk this tile's list
+      uint32_t m = 0;
+#pragma unroll
+      for (int p = 0; p < PPT; ++p) m = max(m, nc[p]);
+      m = __reduce_max_sync(FULL, m);
+      if (tid == 0) s_walk = 0u;
+      __syncthreads();
+      if (lane == 0) atomicMax(&s_walk, m);
+      __syncthreads();
+      if (tid == 0) a.tile_walk[tile] = s_walk;
     }
     if (!PERSIST) return;
     __syncthreads();

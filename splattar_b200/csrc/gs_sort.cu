@@ -506,35 +506,46 @@ int launch_ranges_fix(uint2* ranges, uint32_t num_tiles, cudaStream_t st) {
 }
 
 namespace {
-__global__ void __launch_bounds__(1024) k_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order) {
-  __shared__ uint32_t s_cnt[33];
+// Bucket of a work amount w: 4·⌊log2(w + 1)⌋ plus the two bits below the
+// leading one, so four buckets per octave (0..127).
+__device__ __forceinline__ uint32_t work_bucket(uint32_t w) {
+  const uint32_t x = w + 1u > w ? w + 1u : w;
+  const int e = 31 - __clz(x);
+  const uint32_t frac = e >= 2 ? (x >> (e - 2)) & 3u : (x << (2 - e)) & 3u;
+  return 4u * (uint32_t)e + frac;
+}
+
+__global__ void __launch_bounds__(1024) k_tile_order(const uint2* ranges, const uint32_t* lengths, uint32_t num_tiles,
+                                                     uint32_t* order) {
+  constexpr int NB = 128;
+  __shared__ uint32_t s_cnt[NB];
   const int tid = threadIdx.x;
-  if (tid < 33) s_cnt[tid] = 0u;
+  if (tid < NB) s_cnt[tid] = 0u;
   __syncthreads();
-  for (uint32_t t = tid; t < num_tiles; t += blockDim.x) {
+  auto work = [&](uint32_t t) {
+    if (lengths) return lengths[t];
     const uint2 r = ranges[t];
-    atomicAdd(&s_cnt[32 - __clz(r.y - r.x + 1u)], 1u);  // bucket ⌊log2(len + 1)⌋ + 1 ∈ [1, 32]
-  }
+    return r.y - r.x;
+  };
+  for (uint32_t t = tid; t < num_tiles; t += blockDim.x) atomicAdd(&s_cnt[work_bucket(work(t))], 1u);
   __syncthreads();
   if (tid == 0) {  // exclusive offsets, heaviest bucket first
     uint32_t run = 0;
-    for (int b = 32; b >= 0; --b) {
+    for (int b = NB - 1; b >= 0; --b) {
       const uint32_t c = s_cnt[b];
       s_cnt[b] = run;
       run += c;
     }
   }
   __syncthreads();
-  for (uint32_t t = tid; t < num_tiles; t += blockDim.x) {
-    const uint2 r = ranges[t];
-    order[atomicAdd(&s_cnt[32 - __clz(r.y - r.x + 1u)], 1u)] = t;
-  }
+  for (uint32_t t = tid; t < num_tiles; t += blockDim.x) order[atomicAdd(&s_cnt[work_bucket(work(t))], 1u)] = t;
 }
 }  // namespace
 
-int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, cudaStream_t st) {
+int launch_tile_order(const uint2* ranges, const uint32_t* lengths, uint32_t num_tiles, uint32_t* order,
+                      cudaStream_t st) {
   if (num_tiles == 0) return 0;
-  k_tile_order<<<1, 1024, 0, st>>>(ranges, num_tiles, order);
+  k_tile_order<<<1, 1024, 0, st>>>(ranges, lengths, num_tiles, order);
   return (int)cudaGetLastError();
 }
 
