@@ -36,8 +36,8 @@ sys.path.insert(0, ROOT)
 METRIC = "fwd+bwd+Adam steps/s, 1M surfels 1080p: chosen vs plain form; HBM roofline frac"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel,
 # from one ncu capture of the same workload and launch shapes
-# (profile_step --workload ring8_1m --shapes 64,4,64,8).
-TRAFFIC = {("ring8_1m", "raster_bwd"): 849_430_272}
+# (profile_step --workload ring8_1m --shapes 64,4,128,8).
+TRAFFIC = {("ring8_1m", "raster_bwd"): 1_551_134_976}
 # Launch shapes (fwd batch, fwd pixels/thread, bwd batch, bwd pixels/thread)
 # tried for the plain form at 16-pixel tiles before it is timed.
 PLAIN_SHAPES = [(128, 2, 128, 2), (128, 2, 64, 4), (128, 1, 128, 2), (64, 4, 64, 8)]
