@@ -265,3 +265,28 @@ def test_async_copies_take_device_pointers():
     r.write_async("target", host.data_ptr(), host.numel() * 4, 0, 0)
     r.check()
     assert np.all(r.read("target", 4 * P) == 7.0)
+
+
+def test_chosen_step_with_no_tile_entries():
+    """Every surfel behind every camera: no tile entries, empty ranges, a
+    black image, zero gradients, so the Adam step leaves the parameters as
+    they were; nothing is reported as an error."""
+    scene, cams = multi_view_setup(77, 200)
+    rc = [raster_camera(c, 3) for c in cams]
+    # The three cameras share a centre and look at the scene: move the scene
+    # 50 units behind that centre, away from where they look.
+    moved = scene.copy()
+    c0 = np.asarray(cams[0].center, np.float64)
+    away = (c0 - scene.pos.mean(0)) / np.linalg.norm(c0 - scene.pos.mean(0))
+    moved.pos = c0 + 50.0 * away[None, :] + 0.01 * scene.pos
+    r = _trainer(moved, cams)
+    before = _params(r, moved.n)
+    for _ in range(2):
+        r.train_step(rc, moved.n, StepSettings(0.8, 0.2, AdamSettings(eps=1e-15), "chosen"))
+    r.check()
+    assert r.entry_count() == 0
+    P = sum(c.width * c.height for c in cams)
+    assert np.all(r.read("out_color", 4 * P) == 0)
+    after = _params(r, moved.n)
+    for k in before:
+        assert np.array_equal(before[k], after[k]), k
