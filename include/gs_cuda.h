@@ -229,6 +229,23 @@ gs_status gs_camera_adam6(float m[6], float v[6], uint32_t t, const float grad[6
                           float step[6]);
 gs_status gs_camera_apply_step(gs_camera* cam, const float step[6]);
 
+/* Trainer schedule (first_attempt/crates/gs-train/src/trainer.rs), host-only.
+ * gs_scene_extent = the position-LR scale of trainer.rs:740-746: half the
+ * diagonal of the bounding box of n positions (stride floats apart, xyz
+ * first), at least 1e-3. gs_schedule_t = schedule_t (trainer.rs:407-416):
+ * iter/iters, or with an anneal (start, len, t0) t0 + (1 − t0)·min(1,
+ * (iter − start)/len) (iter before start counts as start). gs_position_lr =
+ * the exponential decay of trainer.rs:1150: lr_pos·extent·final_factor^t
+ * (the defaults are lr_pos 1.6e-4, final_factor 0.01, trainer.rs:470-471). */
+typedef struct {
+  uint32_t start;
+  uint32_t len;
+  float t0;
+} gs_anneal;
+gs_status gs_scene_extent(const float* positions, uint32_t n, uint32_t stride, float* extent);
+gs_status gs_schedule_t(uint32_t iter, uint32_t iters, const gs_anneal* anneal, float* t);
+gs_status gs_position_lr(float lr_pos, float extent, float final_factor, float t, float* lr);
+
 /* Optimizer (first_attempt/crates/gs-train/src/optim.rs:50-242) over the five
  * classes the trainer registers (trainer.rs:757-761): pos (identity, 4 per
  * surfel incl. pad lane), scales (exp), quat (identity), opacity (sigmoid),

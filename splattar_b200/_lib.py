@@ -69,6 +69,10 @@ class StepConfig(C.Structure):
     _fields_ = [("w_l1", C.c_float), ("w_ssim", C.c_float), ("adam", AdamConfig), ("form", C.c_uint32)]
 
 
+class Anneal(C.Structure):
+    _fields_ = [("start", C.c_uint32), ("len", C.c_uint32), ("t0", C.c_float)]
+
+
 class DensifyConfig(C.Structure):
     _fields_ = [("grad_threshold", C.c_float), ("opacity_threshold", C.c_float)]
 
@@ -124,6 +128,9 @@ def lib():
         "gs_camera_step_grad": [C.POINTER(f32), C.POINTER(f32), C.POINTER(f32)],
         "gs_camera_adam6": [C.POINTER(f32), C.POINTER(f32), u32, C.POINTER(f32), f32, f32, C.POINTER(f32)],
         "gs_camera_apply_step": [C.POINTER(Camera), C.POINTER(f32)],
+        "gs_scene_extent": [C.POINTER(f32), u32, u32, C.POINTER(f32)],
+        "gs_schedule_t": [u32, u32, C.POINTER(Anneal), C.POINTER(f32)],
+        "gs_position_lr": [f32, f32, f32, f32, C.POINTER(f32)],
         "gs_mcmc_seed": [vp, u64, vp],
         "gs_mcmc_relocate": [vp, C.POINTER(McmcConfig), u32, vp],
         "gs_mcmc_stats": [vp, C.POINTER(u32), C.POINTER(u64), vp],
@@ -168,6 +175,6 @@ def exported_symbols() -> list[str]:
         "gs_binner_destroy", "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_radix_sort_pairs_noalloc",
         "gs_exclusive_scan_u32",
         "gs_camera_rotation", "gs_shutdown", "gs_loss_normal", "gs_camera_step_grad", "gs_camera_adam6",
-        "gs_camera_apply_step", "gs_mcmc_seed", "gs_mcmc_relocate", "gs_mcmc_stats", "gs_mcmc_noise",
+        "gs_camera_apply_step", "gs_scene_extent", "gs_schedule_t", "gs_position_lr", "gs_mcmc_seed", "gs_mcmc_relocate", "gs_mcmc_stats", "gs_mcmc_noise",
         "gs_ply_write", "gs_ply_info", "gs_ply_read", "gs_rasterizer_save_ply",
         "gs_rasterizer_load_ply"]

@@ -1034,6 +1034,42 @@ gs_status gs_camera_adam6(float m[6], float v[6], uint32_t t, const float grad[6
   return GS_OK;
 }
 
+// ------------------------------------------------------- trainer schedule
+// first_attempt/crates/gs-train/src/trainer.rs:740-746, 407-416, 1150.
+gs_status gs_scene_extent(const float* positions, uint32_t n, uint32_t stride, float* extent) {
+  if (!extent || (n && !positions) || stride < 3) return GS_ERR_INVALID_ARG;
+  if (n == 0) { *extent = 1e-3f; return GS_OK; }
+  float lo[3], hi[3];
+  for (int c = 0; c < 3; ++c) lo[c] = hi[c] = positions[c];
+  for (uint32_t i = 1; i < n; ++i)
+    for (int c = 0; c < 3; ++c) {
+      const float v = positions[(size_t)i * stride + c];
+      lo[c] = std::min(lo[c], v);
+      hi[c] = std::max(hi[c], v);
+    }
+  const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+  *extent = std::max(std::sqrt(dx * dx + dy * dy + dz * dz), 1e-3f) * 0.5f;
+  return GS_OK;
+}
+
+gs_status gs_schedule_t(uint32_t iter, uint32_t iters, const gs_anneal* anneal, float* t) {
+  if (!t) return GS_ERR_INVALID_ARG;
+  if (!anneal) {
+    *t = (float)iter / (float)std::max(iters, 1u);
+    return GS_OK;
+  }
+  const uint32_t since = iter > anneal->start ? iter - anneal->start : 0u;
+  const float done = std::min((float)since / (float)std::max(anneal->len, 1u), 1.0f);
+  *t = anneal->t0 + (1.0f - anneal->t0) * done;
+  return GS_OK;
+}
+
+gs_status gs_position_lr(float lr_pos, float extent, float final_factor, float t, float* lr) {
+  if (!lr) return GS_ERR_INVALID_ARG;
+  *lr = lr_pos * extent * std::pow(final_factor, t);
+  return GS_OK;
+}
+
 gs_status gs_camera_apply_step(gs_camera* cam, const float step[6]) {
   if (!cam || !step) return GS_ERR_INVALID_ARG;
   // R' = R·exp([δ]×) with δ = −step[0..3]: q' = normalize(q · from_scaled_axis(δ)).

@@ -389,6 +389,31 @@ def camera_apply_step(cam: "RasterCamera", step6) -> "RasterCamera":
     return RasterCamera(tuple(c.center[:]), tuple(c.quat[:]), c.focal, cam.sh_degree, cam.width, cam.height)
 
 
+def scene_extent(positions) -> float:
+    """Position-LR scale (first_attempt/crates/gs-train/src/trainer.rs:740-746):
+    half the bounding-box diagonal of (n, >=3) positions, at least 1e-3."""
+    p = np.ascontiguousarray(positions, np.float32)
+    out = C.c_float()
+    check(lib().gs_scene_extent(p.ctypes.data_as(C.POINTER(C.c_float)), p.shape[0], p.shape[1], C.byref(out)))
+    return out.value
+
+
+def schedule_t(iteration: int, iters: int, anneal=None) -> float:
+    """schedule_t (trainer.rs:407-416); anneal = (start, len, t0) or None."""
+    from ._lib import Anneal
+    out = C.c_float()
+    a = None if anneal is None else C.byref(Anneal(*anneal))
+    check(lib().gs_schedule_t(iteration, iters, a, C.byref(out)))
+    return out.value
+
+
+def position_lr(lr_pos: float, extent: float, final_factor: float, t: float) -> float:
+    """The exponential position-LR decay of trainer.rs:1150."""
+    out = C.c_float()
+    check(lib().gs_position_lr(lr_pos, extent, final_factor, t, C.byref(out)))
+    return out.value
+
+
 def write_ply(path: str, positions4, scales2, quats4, opacities, sh48):
     """write_3dgs_ply (first_attempt/crates/gs-io/src/ply/writer.rs) from host
     arrays of activated values: positions (n,4), scales (n,2), quats xyzw
