@@ -211,14 +211,17 @@ def launches_per_step(n_tiles: int, nv: int, form: str) -> int:
     guard; expansion; tile sort (same passes over the tile-id bits); ranges;
     forward raster; L1+SSIM (2); backward raster; projection backward + Adam
     (chosen form, which also orders its tiles heaviest first before each
-    raster pass: two more launches). Matches the ncu launch list (44 per step
-    on ring8_1m)."""
+    raster pass: two more launches, and runs the occlusion cut's completion
+    pass: gate, flagged counts, entry scan (3), guard, range reset,
+    expansion, tile sort, range fix and forward raster, each finding zero work
+    when no tile needs it)."""
     bits = max(1, math.ceil(math.log2(max(n_tiles, 2))))
     tile_passes = math.ceil(bits / 8)
     per_pass = 5
     fwd = 1 + 4 * per_pass + 3 + 1 + 1 + tile_passes * per_pass + 1 + 1
     if form == "chosen":
-        return fwd + 1 + 2 + 1 + 1 + 1
+        completion = 1 + 1 + 3 + 1 + 1 + 1 + tile_passes * per_pass + 1 + 1
+        return fwd + 1 + 2 + 1 + 1 + 1 + completion
     return nv * (fwd + 2 + 1 + 1) + 5
 
 
@@ -278,6 +281,7 @@ def run_ours(args, ws, rank, local):
     ms_chosen = timed(chosen, args.steps, args.warmup)
     clk = clocks.stop()
     E = rast.entry_count()
+    redone = None if args.stored_state else int(rast.read("incomplete_tiles", 1)[0])
     ms_plain = None
     plain_shapes = None
     if not args.no_plain:
@@ -354,7 +358,7 @@ def run_ours(args, ws, rank, local):
     stages = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
     n_tiles = sum(((c.width + tile - 1) // tile) * ((c.height + tile - 1) // tile) for c in cams)
     rast.check(sp)
-    result = dict(tuned=tuned, wl=wl, n=n, nv=nv, P=P, E=E, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
+    result = dict(tuned=tuned, wl=wl, n=n, nv=nv, P=P, E=E, redone=redone, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
                   plain_shapes=plain_shapes,
                   handle_bytes=int(free0 - free1),
                   stages=stages, n_tiles=n_tiles, loss=loss_vals, h2d=tgt_host.numel() * 4,
@@ -479,6 +483,11 @@ def main():
             "resolutions": [f"{c.width}x{c.height}" for c in r["wl"].cameras],
             "pixels_per_step": P,
             "tile_entries_per_step": E,
+            "occlusion_cut": None if r["redone"] is None else {
+                "tiles_rendered_again_in_last_step": r["redone"],
+                "what": "each tile binned down to the depth its pixels needed in the previous step plus a margin; "
+                        "tiles whose truncated list ran out re-binned and re-rendered in full within the step; "
+                        "images and gradients equal to full lists"},
             "form": "chosen: views batched per pass, persistent raster kernels, projection backward fused with Adam, "
                     f"{args.precision} storage of SH and projected colour/normal, CUDA-graph replay, "
                     f"{r['tuned']['tile']}-pixel tiles",

@@ -55,10 +55,18 @@ enum {
   GS_FLAG_TIGHT_BINNING = 1u << 3, /* bin a surfel only into the tiles its alpha >= 1/255 box overlaps: images and
                                       gradients are unchanged; tile lists, ranges and OUT_NCONTRIB then refer to the
                                       shorter lists instead of the reference's conservative rects */
-  GS_FLAG_STORED_STATE = 1u << 4   /* stored-state backward for the chosen-form step (with GS_FLAG_COLOR_ONLY): the
+  GS_FLAG_STORED_STATE = 1u << 4,  /* stored-state backward for the chosen-form step (with GS_FLAG_COLOR_ONLY): the
                                       forward records which tile entries composited into each pixel (one bit per
                                       pixel and entry, 32 bytes per entry of max_entries held by the handle) and
                                       the backward evaluates only those; results are identical */
+  GS_FLAG_FULL_LISTS = 1u << 5     /* turn off the chosen-form step's occlusion cut. With the cut (the default,
+                                      except in deterministic and stored-state modes) each tile is binned only down
+                                      to the depth its pixels needed in the previous step with the same views, plus
+                                      a margin (GS_BUF_TILE_CUT); a tile whose truncated list runs out before all its
+                                      pixels terminate is binned and rendered again in full within the same step
+                                      (counted in GS_BUF_INCOMPLETE_TILES). Images, contributor indices and
+                                      gradients are those of the full lists; tile lists, ranges and the entry
+                                      count then cover the truncated lists */
 };
 
 /* Rasterizer::new(ctx, capacity, width, height, max_entries)
@@ -154,7 +162,10 @@ typedef enum {
   GS_BUF_V_QUAT = 38,
   GS_BUF_V_OPACITY = 39,
   GS_BUF_V_SH = 40,
-  GS_BUF_NORMAL_LOSS = 41 /* double per view: sum over pixels of alpha (1 - n.N_d) of the last gs_loss_normal */
+  GS_BUF_NORMAL_LOSS = 41,/* double per view: sum over pixels of alpha (1 - n.N_d) of the last gs_loss_normal */
+  GS_BUF_INCOMPLETE_TILES = 42,/* u32: tiles the last chosen-form step rendered again with full lists (occlusion cut) */
+  GS_BUF_TILE_CUT = 43    /* u32 per tile: f32 bits of the deepest centre depth the next chosen-form step bins into
+                             the tile (all ones: no cut); reset when the step's views or shape change */
 } gs_buffer_id;
 
 typedef struct gs_rasterizer gs_rasterizer;

@@ -21,6 +21,7 @@ FLAG_PERSISTENT = 2
 FLAG_COLOR_ONLY = 4
 FLAG_TIGHT_BINNING = 8
 FLAG_STORED_STATE = 16
+FLAG_FULL_LISTS = 32
 
 BUF = {
     "positions": 0, "scales": 1, "quats": 2, "opacities": 3, "sh": 4, "out_color": 5, "out_aux": 6,
@@ -30,6 +31,7 @@ BUF = {
     "raw_opacity": 25, "raw_sh": 26, "rects": 27, "depth_keys": 28, "depth_order": 29,
     "grad_norm_sum": 30, "m_pos": 31, "m_scales": 32, "m_quat": 33, "m_opacity": 34, "m_sh": 35, "v_pos": 36,
     "v_scales": 37, "v_quat": 38, "v_opacity": 39, "v_sh": 40, "normal_loss": 41,
+    "incomplete_tiles": 42, "tile_cut": 43,
 }
 
 

@@ -113,6 +113,21 @@ struct gs_rasterizer {
   // per tile, the largest contributor count of the last persistent forward:
   // the backward's work, used to order its tiles
   uint32_t* tile_walk = nullptr;
+  // Occlusion cut of the chosen-form step (off with GS_FLAG_FULL_LISTS and
+  // in deterministic and stored-state modes): per tile the deepest depth key
+  // the next step bins (all ones: the whole list), the tiles a truncated list
+  // left unfinished, the items' depth keys and the completion pass's counts.
+  bool cut_on = false;
+  uint32_t* tile_cut = nullptr;
+  uint32_t* inc_list = nullptr;
+  uint32_t* inc_skip = nullptr;
+  uint32_t* inc_src = nullptr;
+  uint8_t* inc_flag = nullptr;
+  uint32_t* item_key = nullptr;
+  uint32_t* counts2 = nullptr;
+  uint32_t* cutw = nullptr;  // [0] unfinished tiles [1] completion items [2] completion entries (u32) [3] tile counter
+  unsigned long long* entry_total2 = nullptr;
+  std::vector<uint32_t> cut_sig;  // step shape and views the cuts were recorded for
 
   // device scalars: [0] entry total u64, then u32 words
   unsigned long long* entry_total = nullptr;
@@ -322,11 +337,22 @@ const void* sh_for(gs_rasterizer* r, int prec) { return prec == 0 ? (const void*
 
 // Projection + binning + forward raster for `nv` views starting at views_dev
 // (already uploaded), `tiles` tiles in total, storage precision `prec`.
+// cut: bin each tile only up to the depth recorded by the previous step's
+// forward (tile_cut), then bin in full every tile whose truncated list ran
+// out before all its pixels terminated and continue rendering it. A truncated list
+// is a prefix of the full one (entries are ordered by depth), and a tile
+// whose pixels all terminate inside it never reads past it, so images,
+// contributor indices and gradients are those of the full lists.
 gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vhost, uint32_t nv, int tiles, uint32_t n,
                       int prec, bool persistent, bool tight, cudaStream_t st, Prof* prof = nullptr,
-                      bool color = false) {
+                      bool color = false, bool cut = false) {
   const uint32_t items = nv * n;
+  const bool cut_active = cut && r->cut_on && persistent;
   mark(prof, -1, st);
+  if (cut_active) {
+    TRY_CUDA(r, cudaMemsetAsync(r->cutw, 0, sizeof(uint32_t) * 4, st));
+    TRY_CUDA(r, cudaMemsetAsync(r->inc_flag, 0, (size_t)tiles, st));
+  }
   ProjectArgs pa{};
   pa.views = vdev; pa.n = n;
   pa.pos = r->positions; pa.scales = r->scales; pa.quats = r->quats; pa.opac = r->opacities;
@@ -334,6 +360,8 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   pa.records = r->records; pa.rects = r->rects;
   pa.keys = r->item_keys[0]; pa.vals = r->item_vals[0]; pa.counts = r->counts;
   pa.tight = tight ? 1 : 0;
+  pa.cut = cut_active ? r->tile_cut : nullptr;
+  pa.item_key = cut_active ? r->item_key : nullptr;
   TRY_LAUNCH(r, launch_project(pa, prec, nv, st));
   mark(prof, 0, st);
   int in1 = 0;
@@ -354,7 +382,18 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ea.exp_item = r->exp_item;
   ea.entry_offset = r->det ? r->entry_offset : nullptr;
   ea.error_word = r->words + 1;
-  TRY_LAUNCH(r, launch_expand(ea, st));
+  ExpandFilterArgs fa{};
+  fa.perm = perm; fa.counts = r->counts; fa.offsets = r->offsets; fa.rects = r->rects;
+  fa.views = vdev; fa.items_per_view = n; fa.n_items_host = items;
+  fa.total = r->entry_total; fa.capacity = r->max_entries; fa.pairs = r->ent_pairs[0];
+  fa.error_word = r->words + 1;
+  if (cut_active) {
+    fa.cut = r->tile_cut;
+    fa.key_by_item = r->item_key;
+    TRY_LAUNCH(r, launch_expand_filtered(fa, st));
+  } else {
+    TRY_LAUNCH(r, launch_expand(ea, st));
+  }
   mark(prof, 2, st);
   const int bits = tile_key_bits((uint32_t)std::max(tiles, 1));
   // The tile sort's final pass also records each tile's range; the fix-up
@@ -390,8 +429,49 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
     grid = std::min(tiles, r->num_sms * raster_fwd_occupancy(r->tile, prec, batch, ppt, r->det, color,
                                                               ra.mask != nullptr));
   }
+  if (cut_active) {
+    ra.tile_cut = r->tile_cut; ra.cut_pass = 1; ra.item_key = r->item_key;
+    ra.inc_count = r->cutw; ra.inc_list = r->inc_list; ra.inc_flag = r->inc_flag;
+    ra.inc_skip = r->inc_skip; ra.inc_src = r->inc_src;
+  }
   TRY_LAUNCH(r, launch_raster_fwd(ra, r->tile, prec, batch, ppt, r->det, persistent, color && persistent, grid, st));
   mark(prof, 5, st);
+  if (cut_active) {
+    // Completion pass (every kernel finds zero work when no tile is listed):
+    // the listed tiles' full lists are binned after the entries in use,
+    // sorted there and their ranges replaced; each tile's rendering then
+    // continues after the prefix pass 1 composited.
+    TRY_LAUNCH(r, launch_cut_gate(r->cutw, items, r->cutw + 1, st));
+    TRY_LAUNCH(r, launch_count_flagged(r->rects, vdev, nv, n, items, r->cutw, r->inc_list, r->inc_flag, r->counts2,
+                                       st));
+    TRY_LAUNCH(r, launch_scan(r->counts2, perm, r->offsets, items, r->cutw + 1, r->cutw + 2, r->entry_total2,
+                              r->scan_scratch, st));
+    TRY_LAUNCH(r, launch_entry_guard2(r->entry_total, r->entry_total2, r->cutw + 2, r->max_entries, r->words + 1, st));
+    TRY_LAUNCH(r, launch_ranges_reset_list(r->inc_list, r->cutw, r->ranges, (uint32_t)tiles, st));
+    mark(prof, 1, st);
+    ExpandFilterArgs fb = fa;
+    fb.counts = r->counts2; fb.n_items_dev = r->cutw + 1;
+    fb.total = r->entry_total2; fb.base = r->entry_total;
+    fb.cut = nullptr; fb.key_by_item = nullptr; fb.flag = r->inc_flag;
+    TRY_LAUNCH(r, launch_expand_filtered(fb, st));
+    mark(prof, 2, st);
+    int in1b = 0;
+    TRY_LAUNCH(r, launch_radix_sort_pairs(r->ent_pairs[0], r->ent_pairs[1], r->max_entries, r->cutw + 2, bits,
+                                          r->sort_scratch, &in1b, st, r->ranges, (uint32_t)tiles, r->entry_total));
+    if (in1b != r->ent_in1) return fail(r, GS_ERR_STATE, "completion sort ended in the other buffer");
+    mark(prof, 3, st);
+    TRY_LAUNCH(r, launch_ranges_fix_list(r->inc_list, r->cutw, r->ranges, (uint32_t)tiles, r->entry_total,
+                                         r->entry_total2, r->gmask_valid ? r->gmask : nullptr, r->inc_skip,
+                                         r->inc_src, st));
+    mark(prof, 4, st);
+    RasterArgs rb = ra;
+    rb.cut_pass = 2;
+    rb.tile_order = r->inc_list;
+    rb.tile_limit = r->cutw;
+    rb.tile_counter = r->cutw + 3;
+    TRY_LAUNCH(r, launch_raster_fwd(rb, r->tile, prec, batch, ppt, r->det, persistent, color && persistent, grid, st));
+    mark(prof, 5, st);
+  }
   r->last_nv = nv; r->last_n = n; r->last_tiles = tiles; r->last_views_dev = vdev; r->last_views_host = vhost;
   r->have_forward = true;
   return GS_OK;
@@ -538,6 +618,25 @@ gs_status adam_plain(gs_rasterizer* r, const gs_adam_config* c, uint32_t n, cuda
   return refresh_half(r, n, st);
 }
 
+// The cuts hold for the step shape and views they were recorded with; any
+// other step starts from full lists (results are exact either way; this only
+// keeps stale cuts from sending most tiles through the completion pass).
+gs_status cut_refresh(gs_rasterizer* r, uint32_t nv, uint32_t n, cudaStream_t st) {
+  if (!r->cut_on) return GS_OK;
+  std::vector<uint32_t> sig = {nv, n, (uint32_t)r->tile};
+  for (const ViewInfo& v : r->views_batched) {
+    const size_t w = sizeof(ViewInfo) / sizeof(uint32_t);
+    const size_t at = sig.size();
+    sig.resize(at + w);
+    std::memcpy(sig.data() + at, &v, w * sizeof(uint32_t));
+  }
+  if (sig != r->cut_sig) {
+    TRY_CUDA(r, cudaMemsetAsync(r->tile_cut, 0xff, sizeof(uint32_t) * (size_t)r->max_tiles, st));
+    r->cut_sig = sig;
+  }
+  return GS_OK;
+}
+
 gs_status ensure_graph_stream(gs_rasterizer* r) {
   if (!r->cap_stream) TRY_CUDA(r, cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking));
   return GS_OK;
@@ -552,7 +651,8 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   int tiles = 0;
   for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
   // With GS_FLAG_COLOR_ONLY the step's forward leaves depth and normal unwritten (nothing reads them).
-  gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, prof, r->color_only);
+  gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, prof, r->color_only,
+                            true);
   if (s) return s;
   TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
   s = run_loss(r, vdev, r->views_batched.data(), nv, cfg->w_l1, cfg->w_ssim, r->loss_sums, st);
@@ -665,6 +765,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   r->color_only = (c.flags & GS_FLAG_COLOR_ONLY) != 0;
   r->tight = (c.flags & GS_FLAG_TIGHT_BINNING) != 0;
   r->stored_state = (c.flags & GS_FLAG_STORED_STATE) != 0;
+  r->cut_on = (c.flags & GS_FLAG_FULL_LISTS) == 0 && !r->det && !r->stored_state;
   r->fwd_batch = (int)c.batch;
   r->fwd_ppt = (int)c.pixels_per_thread;
   r->tile = (int)c.tile;
@@ -710,6 +811,17 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   ALLOC(r->ranges, r->max_tiles);
   ALLOC(r->tile_order, r->max_tiles);
   ALLOC(r->tile_walk, r->max_tiles);
+  if (r->cut_on) {
+    ALLOC(r->tile_cut, r->max_tiles);
+    ALLOC(r->inc_list, r->max_tiles);
+    ALLOC(r->inc_skip, r->max_tiles);
+    ALLOC(r->inc_src, r->max_tiles);
+    ALLOC(r->inc_flag, r->max_tiles);
+    ALLOC(r->item_key, I);
+    ALLOC(r->counts2, I);
+    ALLOC(r->cutw, 4);
+    ALLOC(r->entry_total2, 1);
+  }
   if (r->stored_state) {
     // One bit per (pixel, tile entry): 32 bytes per entry, whole 32-entry words per tile.
     ALLOC(r->mask, ((size_t)E / 32 + r->max_tiles) * 256);
@@ -752,6 +864,8 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   if (e == cudaSuccess) e = cudaMemset(r->entry_total, 0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(r->grad_cam, 0, 16 * sizeof(float) * c.max_views);
   if (e == cudaSuccess) e = cudaMemset(r->accum_norm, 0, sizeof(float) * N);
+  if (e == cudaSuccess && r->cut_on) e = cudaMemset(r->tile_cut, 0xff, sizeof(uint32_t) * (size_t)r->max_tiles);
+  if (e == cudaSuccess && r->cut_on) e = cudaMemset(r->cutw, 0, sizeof(uint32_t) * 4);
   if (e != cudaSuccess) return bail(e, "initial memset");
   *out = r;
   return GS_OK;
@@ -771,6 +885,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask, r->tile_order, r->tile_walk,
                   r->normal_loss_sums,
                   r->mask_words,
+                  r->tile_cut, r->inc_list, r->inc_skip, r->inc_src, r->inc_flag, r->item_key, r->counts2, r->cutw, r->entry_total2,
                   r->scan_scratch, r->sort_scratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -807,6 +922,7 @@ gs_status gs_rasterizer_upload_scene(gs_rasterizer* r, const gs_scene_input* s, 
   TRY_CUDA(r, cudaStreamSynchronize(st));
   r->n_uploaded = s->n;
   r->optim_ready = false;
+  r->cut_sig.clear();
   return GS_OK;
 }
 
@@ -878,6 +994,12 @@ static gs_status buffer_info(gs_rasterizer* r, gs_buffer_id id, void** p, size_t
     case GS_BUF_DEPTH_ORDER: *p = r->item_vals[0]; *bytes = 4 * I; break;
     case GS_BUF_GRAD_NORM_SUM: *p = r->accum_norm; *bytes = 4 * N; break;
     case GS_BUF_NORMAL_LOSS: *p = r->normal_loss_sums; *bytes = 8 * (size_t)r->max_views; break;
+    case GS_BUF_INCOMPLETE_TILES:
+    case GS_BUF_TILE_CUT:
+      if (!r->cut_on) return fail(r, GS_ERR_STATE, "the occlusion cut is off for this handle");
+      if (id == GS_BUF_INCOMPLETE_TILES) { *p = r->cutw; *bytes = 4; }
+      else { *p = r->tile_cut; *bytes = 4 * (size_t)r->max_tiles; }
+      break;
     case GS_BUF_M_POS: case GS_BUF_M_SCALES: case GS_BUF_M_QUAT: case GS_BUF_M_OPACITY: case GS_BUF_M_SH: {
       const int k = (int)id - (int)GS_BUF_M_POS;
       *p = r->mom1[k]; *bytes = 4 * N * WIDTH[k];
@@ -1139,6 +1261,8 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, ui
   if (cfg->form == 0) return plain_body(r, nv, n, cfg, st);
   // Chosen form: batched step replayed from a CUDA graph; per-step values
   // (cameras, learning rates, bias corrections) are uploaded before replay.
+  s = cut_refresh(r, nv, n, st);
+  if (s) return s;
   r->t += 1;
   DynParams dp{};
   for (int k = 0; k < 5; ++k) { dp.lr[k] = cfg->adam.lr[k]; dp.reg[k] = cfg->adam.reg[k]; }
@@ -1189,6 +1313,8 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
   if (cfg->form == 0) {
     s = plain_body(r, nv, n, cfg, st, &prof);
   } else {
+    s = cut_refresh(r, nv, n, st);
+    if (s) return s;
     r->t += 1;
     DynParams dp{};
     for (int k = 0; k < 5; ++k) { dp.lr[k] = cfg->adam.lr[k]; dp.reg[k] = cfg->adam.reg[k]; }
@@ -1399,6 +1525,7 @@ gs_status gs_densify_prune(gs_rasterizer* r, const gs_densify_config* c, uint32_
   if (!r || !c || !n_out) return GS_ERR_INVALID_ARG;
   if (!r->optim_ready) return fail(r, GS_ERR_STATE, "gs_optimizer_init first");
   if (n > r->cap) return fail(r, GS_ERR_CAPACITY, "num_surfels exceeds capacity");
+  r->cut_sig.clear();  // the surfel set changes: the next step starts from full lists
   cudaStream_t st = S(stream);
   const size_t N = r->cap;
   if (!r->dens_flags) {
@@ -1468,6 +1595,7 @@ gs_status gs_mcmc_relocate(gs_rasterizer* r, const gs_mcmc_config* c, uint32_t n
   if (!r->optim_ready) return fail(r, GS_ERR_STATE, "gs_optimizer_init first");
   if (n > r->cap) return fail(r, GS_ERR_CAPACITY, "num_surfels exceeds capacity");
   if (n == 0) return GS_OK;
+  r->cut_sig.clear();  // relocated surfels: the next step starts from full lists
   cudaStream_t st = S(stream);
   gs_status s = mcmc_ready(r, st);
   if (s) return s;

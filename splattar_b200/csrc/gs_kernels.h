@@ -28,6 +28,11 @@ struct ProjectArgs {
   uint32_t* vals;
   uint32_t* counts;
   int tight;              // bin only tiles the α-box overlaps (contributor indices then refer to that list)
+  // Occlusion cut (null: off): per global tile id, the largest depth key
+  // binned into the tile; counts[item] then covers only the rect's tiles with
+  // key <= cut[tile]. item_key receives every item's depth key by item index.
+  const uint32_t* cut;
+  uint32_t* item_key;
 };
 
 struct ProjectBwdArgs {
@@ -100,6 +105,27 @@ struct RasterArgs {
   uint8_t* gmask;
   uint32_t* mask;               // null: the backward re-evaluates every entry
   const uint32_t* mask_off;     // per tile, in 256-word groups
+  // Persistent kernels: number of tile_order entries to take (device count);
+  // null: total_tiles.
+  const uint32_t* tile_limit;
+  // Occlusion cut bookkeeping (persistent forward with tile_walk): null: off.
+  // cut_pass 1 renders lists truncated at tile_cut and records every tile
+  // that ran out of its truncated list with pixels still alive (inc_flag[t]
+  // = 1; slot i of inc_count holds the tile in inc_list, its truncated
+  // length in inc_skip and start in inc_src). cut_pass 2 takes the listed
+  // tiles (tile_order = inc_list) and resumes each after its first inc_skip
+  // entries from the pixel state pass 1 left in the outputs (their gmask
+  // bytes are moved by launch_ranges_fix_list). Both write each
+  // finished tile's next cut: the depth key (item_key) at list position
+  // walk + walk/4 + 32, or past the list's end when it is shorter.
+  uint32_t* tile_cut;
+  int cut_pass;
+  const uint32_t* item_key;
+  uint32_t* inc_count;
+  uint32_t* inc_list;
+  uint32_t* inc_skip;
+  uint32_t* inc_src;
+  uint8_t* inc_flag;
 };
 // Raster launch shapes built for a tile size (8, 16, 32): (staging batch,
 // pixels per thread). Returns the count and points *out at the table.
@@ -145,11 +171,14 @@ int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, ui
                       int key_bits, void* scratch, int* result_in_1, cudaStream_t st);
 // The same sort on interleaved (key, val) pairs, ping-ponging between p0 and p1.
 int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch,
-                            int* result_in_1, cudaStream_t st, uint2* ranges = nullptr, uint32_t num_ranges = 0);
+                            int* result_in_1, cudaStream_t st, uint2* ranges = nullptr, uint32_t num_ranges = 0,
+                            const unsigned long long* base = nullptr);
 // With `ranges` (zero-filled, num_ranges entries) the sort's final pass also
 // records each key's output range; launch_ranges_fix then converts it to
 // [start, end) per key ((0, 0) for absent keys) — the tile ranges without a
-// separate pass over the sorted entries.
+// separate pass over the sorted entries. With `base` (device), the sort
+// covers elements [*base, *base + n) of both buffers and the recorded ranges
+// are positions in the whole buffer.
 int launch_ranges_fix(uint2* ranges, uint32_t num_tiles, cudaStream_t st);
 // Tile order for the persistent raster kernels: tiles bucketed by the
 // logarithm of their work (four buckets per octave; the work is lengths[t]
@@ -183,6 +212,52 @@ struct ExpandArgs {
   uint32_t* error_word;
 };
 int launch_expand(const ExpandArgs& a, cudaStream_t st);
+
+// Expansion restricted to some tiles of each item's rect, in the same order
+// as launch_expand (items in depth order, a rect's tiles row-major): a tile
+// is taken when key_by_item[item] <= cut[tile] (cut != null) or when
+// flag[tile] != 0 (flag != null). counts/offsets hold the restricted counts.
+// Entries go to pairs[*base + offset] (base null: 0) as (tile, item).
+struct ExpandFilterArgs {
+  const uint32_t* perm;
+  const uint32_t* counts;
+  const uint32_t* offsets;
+  const uint4* rects;
+  const ViewInfo* views;
+  uint32_t items_per_view;
+  const uint32_t* n_items_dev;       // null: n_items_host
+  uint32_t n_items_host;
+  const unsigned long long* total;   // entries of this expansion
+  const unsigned long long* base;    // entries already in pairs, or null
+  uint64_t capacity;
+  uint2* pairs;
+  const uint32_t* cut;
+  const uint32_t* key_by_item;
+  const uint8_t* flag;
+  uint32_t* error_word;
+};
+int launch_expand_filtered(const ExpandFilterArgs& a, cudaStream_t st);
+// Completion pass of the occlusion cut. gate_n = *inc_count ? n_items : 0.
+int launch_cut_gate(const uint32_t* inc_count, uint32_t n_items, uint32_t* gate_n, cudaStream_t st);
+// counts[item] = tiles of rects[item] that are listed (inc_list, *inc_count
+// of them; flag[t] set for each). The kernel returns at once when the list
+// is empty (the counts are then not read).
+int launch_count_flagged(const uint4* rects, const ViewInfo* views, uint32_t n_views, uint32_t items_per_view,
+                         uint32_t n_items, const uint32_t* inc_count, const uint32_t* inc_list, const uint8_t* flag,
+                         uint32_t* counts, cudaStream_t st);
+// When base + total2 exceeds the capacity: flag the entry-capacity error and
+// zero total2 and count2.
+int launch_entry_guard2(const unsigned long long* base, unsigned long long* total2, uint32_t* count2,
+                        uint64_t capacity, uint32_t* error_word, cudaStream_t st);
+// ranges[list[i]] = (0, 0) for i < *count.
+int launch_ranges_reset_list(const uint32_t* list, const uint32_t* count, uint2* ranges, uint32_t max_list,
+                             cudaStream_t st);
+// launch_ranges_fix for the listed tiles only, then *entry_total += *total2.
+// With gmask, the first skip[i] bytes of listed tile i's summary move from
+// gmask[src[i]] to the tile's new start.
+int launch_ranges_fix_list(const uint32_t* list, const uint32_t* count, uint2* ranges, uint32_t max_list,
+                           unsigned long long* entry_total, const unsigned long long* total2, uint8_t* gmask,
+                           const uint32_t* skip, const uint32_t* src, cudaStream_t st);
 // ranges[t] = [start, end) of tile t in the sorted pairs (ranges zeroed by the callee).
 // mask_off[t] = Σ_{t' < t} ⌈len(t')/32⌉ over the tiles' entry ranges.
 int launch_mask_offsets(const uint2* ranges, uint32_t num_tiles, uint32_t* words, uint32_t* mask_off, void* scratch,

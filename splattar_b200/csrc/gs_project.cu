@@ -3,7 +3,8 @@
 // normal, projected centre, conservative 3σ pixel radius capped at 64 px, tile
 // rect by truncation, depth key = f32 bits of the centre depth. One thread
 // per (surfel, view); the tile count of the rect is written for the binner
-// (the reference's separate count_tiles pass, tile_binning.wgsl:30-43).
+// (the reference's separate count_tiles pass, tile_binning.wgsl:30-43),
+// restricted under the occlusion cut to the tiles whose cut the key reaches.
 //
 // This translation unit is compiled with --fmad=false: the rect and key
 // arithmetic is evaluated in the reference's operation order without
@@ -93,6 +94,7 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   if (g.depth < NEAR_DEPTH) {
     a.rects[item] = rect;
     a.keys[item] = 0u;
+    if (a.item_key != nullptr) a.item_key[item] = 0u;
     a.counts[item] = 0u;
     return;
   }
@@ -157,7 +159,29 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     }
   }
   a.rects[item] = rect;
-  a.keys[item] = __float_as_uint(depth);
+  const uint32_t key = __float_as_uint(depth);
+  a.keys[item] = key;
+  if (a.item_key != nullptr) a.item_key[item] = key;
+  if (a.cut != nullptr && count) {
+    // Occlusion cut: only the rect's tiles whose binned depth reaches this key.
+    // Four independent loads per round, walking the rect row-major.
+    const uint32_t tb = (uint32_t)__ldg(&a.views[v].tile_base), txs = (uint32_t)k.tiles_x;
+    uint32_t kept = 0, x = rect.x, y = rect.y;
+    for (uint32_t j = 0; j < count; j += 4) {
+      uint32_t idx[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        idx[u] = tb + y * txs + x;
+        if (++x > rect.z) { x = rect.x; ++y; }
+      }
+      uint32_t c[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) c[u] = j + u < count ? __ldg(a.cut + idx[u]) : 0u;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) kept += (j + u < count && key <= c[u]) ? 1u : 0u;
+    }
+    count = kept;
+  }
   a.counts[item] = count;
 
   const float3 Bu = cross3(tv, c);

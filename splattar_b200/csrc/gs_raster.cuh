@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
   __shared__ int s_wcount[2][NW];
   __shared__ int s_tile;
   __shared__ uint32_t s_walk;  // tile_walk: the tile's largest contributor count
+  __shared__ uint32_t s_slot;  // counter value the tile was taken at
   const int tid = threadIdx.x, lane = tid & 31;
   const bool gm_on = GM && a.gmask != nullptr;
   const int g0 = L::row(tid) >> 2;  // first row group of this lane's pixels
@@ -261,8 +262,10 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
     if (PERSIST) {
       if (tid == 0) {
         const uint32_t slot = atomicAdd(a.tile_counter, 1u);
+        const uint32_t lim = a.tile_limit != nullptr ? *a.tile_limit : (uint32_t)a.total_tiles;
         // heaviest tiles first when an order is given (a shorter tail)
-        s_tile = (int)(a.tile_order != nullptr && slot < (uint32_t)a.total_tiles ? __ldg(a.tile_order + slot) : slot);
+        s_tile = slot >= lim ? a.total_tiles : (int)(a.tile_order != nullptr ? __ldg(a.tile_order + slot) : slot);
+        s_slot = slot;
       }
       __syncthreads();
       tile = s_tile;
@@ -270,6 +273,16 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
     }
     const TileGeo<PPT> g = tile_geo<TS, PPT>(a, tile);
     const uint2 range = __ldg(&a.ranges[tile]);
+    // Completion pass of the occlusion cut: the tile's full list begins with
+    // the skip entries pass 1 composited (their row-group summary was moved
+    // along with the range); continue after them from the pixel state pass 1
+    // wrote.
+    const bool resume = PERSIST && a.cut_pass == 2;
+    uint32_t skip = 0;
+    if (resume) {
+      skip = a.inc_skip[s_slot];
+      if (range.y - range.x < skip) skip = 0;  // list not rebuilt (entry capacity error already flagged)
+    }
     float T[PPT], cr[PPT], cg[PPT], cb[PPT], aa[PPT], ad[PPT], nx[PPT], ny[PPT], nz[PPT];
     uint32_t nc[PPT];
     bool done[PPT];
@@ -286,11 +299,24 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
       T[p] = 1.f; cr[p] = cg[p] = cb[p] = aa[p] = ad[p] = nx[p] = ny[p] = nz[p] = 0.f;
       nc[p] = 0;
       done[p] = !g.inside[p];
+      if (resume && g.inside[p]) {
+        const long long pix = g.row0 + (long long)p * g.W;
+        const float4 c = a.out_color[pix], x = a.out_aux[pix];
+        cr[p] = c.x; cg[p] = c.y; cb[p] = c.z; aa[p] = c.w;
+        T[p] = x.x;
+        if (!COLOR) {
+          ad[p] = x.y;
+          const float4 nn = a.out_normal[pix];
+          nx[p] = nn.x; ny[p] = nn.y; nz[p] = nn.z;
+        }
+        nc[p] = a.out_nc[pix];
+        done[p] = T[p] < T_TERMINATE;
+      }
       tdone &= done[p];
       mw[p] = 0u;
       mi[p] = 0;
     }
-    for (uint32_t base = range.x; base < range.y; base += BATCH) {
+    for (uint32_t base = range.x + skip; base < range.y; base += BATCH) {
       if (__syncthreads_count(tdone) == NT) break;
       const int count = (int)min((uint32_t)BATCH, range.y - base);
       int kept = 0;
@@ -429,6 +455,42 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
       __syncthreads();
       if (tid == 0) a.tile_walk[tile] = s_walk;
     }
+    if (a.tile_cut != nullptr) {  // occlusion cut bookkeeping (set together with tile_walk)
+      const bool complete = __syncthreads_count(tdone) == NT;  // every pixel terminated
+      if (tid == 0) {
+        const uint32_t used = a.cut_pass == 1 ? a.tile_cut[tile] : 0xffffffffu;
+        const uint32_t len = range.y - range.x;
+        if (!complete && used != 0xffffffffu) {
+          // the truncated list ran out first: the completion pass continues the tile
+          a.inc_flag[tile] = 1u;
+          const uint32_t slot = atomicAdd(a.inc_count, 1u);
+          a.inc_list[slot] = (uint32_t)tile;
+          a.inc_skip[slot] = len;
+          a.inc_src[slot] = range.x;
+        } else {
+          // next cut: the depth key at list position walk + walk/4 + 32 (the
+          // last contributor plus a margin for the next step's changes). A
+          // truncated list shorter than that extends its cut past its last
+          // key by the key span from the last contributor to the list's end
+          // (at least 2^14 units in the last place, about 0.2 % of depth).
+          uint32_t next = 0xffffffffu;
+          if (complete) {
+            const uint32_t walk = s_walk, keep = walk + walk / 4u + 32u;
+            if (keep < len) {
+              next = __ldg(a.item_key + a.sorted_pairs[range.x + keep - 1u].y);
+            } else if (used == 0xffffffffu || walk == 0u || len == 0u) {
+              next = used;
+            } else {
+              const uint32_t kl = __ldg(a.item_key + a.sorted_pairs[range.y - 1u].y);
+              const uint32_t kw = __ldg(a.item_key + a.sorted_pairs[range.x + walk - 1u].y);
+              const uint32_t span = max(kl - kw, 1u << 14);
+              next = kl < 0x7f7fffffu - span ? kl + span : 0x7f7fffffu;
+            }
+          }
+          a.tile_cut[tile] = next;
+        }
+      }
+    }
     if (!PERSIST) return;
     __syncthreads();
   }
@@ -491,8 +553,9 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
     if (PERSIST) {
       if (tid == 0) {
         const uint32_t slot = atomicAdd(a.tile_counter, 1u);
+        const uint32_t lim = a.tile_limit != nullptr ? *a.tile_limit : (uint32_t)a.total_tiles;
         // heaviest tiles first when an order is given (a shorter tail)
-        s_tile = (int)(a.tile_order != nullptr && slot < (uint32_t)a.total_tiles ? __ldg(a.tile_order + slot) : slot);
+        s_tile = slot >= lim ? a.total_tiles : (int)(a.tile_order != nullptr ? __ldg(a.tile_order + slot) : slot);
       }
       __syncthreads();
       tile = s_tile;

@@ -137,12 +137,14 @@ __device__ __forceinline__ uint32_t match_digit(uint32_t d, int nbits, uint32_t 
 // Element access: two arrays, or one interleaved uint2 array.
 struct SplitIO {
   const uint32_t* kin; const uint32_t* vin; uint32_t* kout; uint32_t* vout;
+  __device__ __forceinline__ void skip(uint64_t b) { kin += b; vin += b; kout += b; vout += b; }
   __device__ __forceinline__ uint32_t key(uint64_t i) const { return __ldg(kin + i); }
   __device__ __forceinline__ uint2 load(uint64_t i) const { return make_uint2(__ldg(kin + i), __ldg(vin + i)); }
   __device__ __forceinline__ void store(size_t g, uint2 e) const { kout[g] = e.x; vout[g] = e.y; }
 };
 struct PairIO {
   const uint2* in; uint2* out;
+  __device__ __forceinline__ void skip(uint64_t b) { in += b; out += b; }
   __device__ __forceinline__ uint32_t key(uint64_t i) const {
     return __ldg(reinterpret_cast<const uint32_t*>(in + i));
   }
@@ -152,8 +154,10 @@ struct PairIO {
 
 template <class IO>
 __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(IO io, uint64_t n_host, const uint32_t* n_dev, int shift,
-                                                           int nbits, uint32_t* __restrict__ hist) {
+                                                           int nbits, uint32_t* __restrict__ hist,
+                                                           const unsigned long long* base) {
   __shared__ uint32_t s_hist[RS_WARPS][RS_BINS];
+  if (base != nullptr) io.skip(*base);
   const int tid = threadIdx.x, warp = tid >> 5;
   for (int k = tid; k < RS_WARPS * RS_BINS; k += RS_THREADS) (&s_hist[0][0])[k] = 0;
   __syncthreads();
@@ -192,7 +196,8 @@ template <class IO>
 __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_downsweep(IO io, uint64_t n_host, const uint32_t* n_dev,
                                                                 int shift, int nbits,
                                                                 const uint32_t* __restrict__ hist,
-                                                                uint2* ranges, uint32_t num_ranges) {
+                                                                uint2* ranges, uint32_t num_ranges,
+                                                                const unsigned long long* base) {
   __shared__ uint2 s_e[RS_TILE];
   __shared__ uint32_t s_wh[RS_WARPS][RS_BINS];
   __shared__ uint32_t s_start[RS_BINS], s_gofs[RS_BINS], s_run[RS_BINS];
@@ -203,6 +208,8 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_downsweep(IO io, uint64_t 
   const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
   const uint64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
   if (beg >= end) return;
+  const uint32_t b0 = base != nullptr ? (uint32_t)*base : 0u;  // range positions are whole-buffer positions
+  if (b0) io.skip(b0);
   const uint32_t mask = (1u << nbits) - 1u;
   s_run[tid] = hist[(size_t)tid * gridDim.x + blockIdx.x];  // RS_THREADS == RS_BINS
   uint2 e[RS_ROUNDS];
@@ -275,8 +282,8 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_downsweep(IO io, uint64_t 
       const uint32_t pos = s_gofs[(v.x >> shift) & mask] + (uint32_t)i;
       io.store((size_t)pos, v);
       if (ranges != nullptr && v.x < num_ranges) {
-        if (i == 0 || s_e[i - 1].x != v.x) atomicMax(&ranges[v.x].x, ~pos);
-        if (i == tn - 1 || s_e[i + 1].x != v.x) atomicMax(&ranges[v.x].y, pos + 1u);
+        if (i == 0 || s_e[i - 1].x != v.x) atomicMax(&ranges[v.x].x, ~(b0 + pos));
+        if (i == tn - 1 || s_e[i + 1].x != v.x) atomicMax(&ranges[v.x].y, b0 + pos + 1u);
       }
     }
     __syncthreads();
@@ -356,6 +363,168 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   }
 }
 
+// Filtered expansion (occlusion cut and its completion pass): the warp walks
+// the candidate tiles of its 32 items' rects in launch_expand's order and
+// keeps those the filter accepts, compacted by ballot, so each item's kept
+// tiles land at its restricted offset in rect order.
+__global__ void __launch_bounds__(256) k_expand_filtered(ExpandFilterArgs a) {
+  const uint64_t n = read_n(a.n_items_host, a.n_items_dev);
+  const uint64_t tot = *a.total;
+  const uint64_t b = a.base != nullptr ? *a.base : 0ull;
+  if (tot == 0 || b + tot > a.capacity) return;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps_total = (uint64_t)gridDim.x * (blockDim.x / 32);
+  for (uint64_t w = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); w * 32 < n; w += warps_total) {
+    const uint64_t k0 = w * 32, k = k0 + lane;
+    uint32_t item = 0, cnt = 0, full = 0, x0 = 0, y0 = 0, wd = 1, tb = 0, tx = 0, key = 0;
+    if (k < n) {
+      item = a.perm[k];
+      cnt = a.counts[item];
+      if (cnt) {
+        const uint4 r = a.rects[item];
+        x0 = r.x; y0 = r.y; wd = r.z - r.x + 1u;
+        full = wd * (r.w - r.y + 1u);
+        const ViewInfo* V = a.views + item / a.items_per_view;
+        tb = (uint32_t)__ldg(&V->tile_base);
+        tx = (uint32_t)__ldg(&V->tiles_x);
+        if (a.cut != nullptr) key = a.key_by_item[item];
+      }
+    }
+    uint32_t incl = full, incl_c = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, incl, o), tc = __shfl_up_sync(FULL, incl_c, o);
+      if (lane >= o) { incl += t; incl_c += tc; }
+    }
+    const uint32_t excl = incl - full;
+    const uint32_t total_full = __shfl_sync(FULL, incl, 31), total_cnt = __shfl_sync(FULL, incl_c, 31);
+    if (total_cnt == 0) continue;
+    const uint32_t off0 = a.offsets[k0];
+    if ((uint64_t)off0 + total_cnt > tot) {
+      if (lane == 0) atomicOr(a.error_word, ERR_ENTRY_CAPACITY);
+      continue;
+    }
+    uint32_t run = 0;
+    for (uint32_t basej = 0; basej < total_full; basej += 32) {
+      const uint32_t j = basej + lane;
+      int owner = 0;
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) {
+        const int c = owner + s;
+        const uint32_t ec = __shfl_sync(FULL, excl, c < 32 ? c : 31);
+        if (c < 32 && ec <= j) owner = c;
+      }
+      const uint32_t o_excl = __shfl_sync(FULL, excl, owner);
+      const uint32_t o_wd = __shfl_sync(FULL, wd, owner);
+      const uint32_t o_x0 = __shfl_sync(FULL, x0, owner);
+      const uint32_t o_y0 = __shfl_sync(FULL, y0, owner);
+      const uint32_t o_item = __shfl_sync(FULL, item, owner);
+      const uint32_t o_tb = __shfl_sync(FULL, tb, owner);
+      const uint32_t o_tx = __shfl_sync(FULL, tx, owner);
+      const uint32_t o_key = __shfl_sync(FULL, key, owner);
+      bool take = false;
+      uint32_t tile = 0;
+      if (j < total_full) {
+        const uint32_t local = j - o_excl;
+        const uint32_t ly = local / o_wd, lx = local - ly * o_wd;
+        tile = o_tb + (o_y0 + ly) * o_tx + (o_x0 + lx);
+        take = a.cut != nullptr ? o_key <= __ldg(a.cut + tile) : __ldg(a.flag + tile) != 0;
+      }
+      const uint32_t bal = __ballot_sync(FULL, take);
+      if (take) {
+        const uint32_t slot = run + __popc(bal & lanemask_lt());
+        if (slot < total_cnt) a.pairs[b + off0 + slot] = make_uint2(tile, o_item);
+        else atomicOr(a.error_word, ERR_ENTRY_CAPACITY);  // counts disagree with the filter: never written past them
+      }
+      run += __popc(bal);
+    }
+  }
+}
+
+__global__ void k_cut_gate(const uint32_t* inc_count, uint32_t n_items, uint32_t* gate_n) {
+  *gate_n = *inc_count ? n_items : 0u;
+}
+
+// Listed tiles are held in shared memory as (view, x, y) when there are few
+// of them; each item then checks its rect against the list instead of
+// reading the flags of every tile in the rect.
+constexpr int FLAG_LIST_SMEM = 512;
+__global__ void __launch_bounds__(256) k_count_flagged(const uint4* rects, const ViewInfo* views, uint32_t nv,
+                                                       uint32_t ipv, uint32_t n, const uint32_t* inc_count,
+                                                       const uint32_t* inc_list, const uint8_t* flag,
+                                                       uint32_t* counts) {
+  const uint32_t m = *inc_count;
+  if (m == 0) return;
+  __shared__ uint32_t s_v[FLAG_LIST_SMEM], s_x[FLAG_LIST_SMEM], s_y[FLAG_LIST_SMEM];
+  const bool listed = m <= (uint32_t)FLAG_LIST_SMEM;
+  if (listed) {
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+      const uint32_t t = inc_list[i];
+      uint32_t v = 0;
+      while (v + 1 < nv && t >= (uint32_t)__ldg(&views[v + 1].tile_base)) ++v;
+      const uint32_t lt = t - (uint32_t)__ldg(&views[v].tile_base), tx = (uint32_t)__ldg(&views[v].tiles_x);
+      s_v[i] = v; s_y[i] = lt / tx; s_x[i] = lt - (lt / tx) * tx;
+    }
+    __syncthreads();
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint4 r = rects[i];
+    uint32_t c = 0;
+    if (r.z >= r.x && r.w >= r.y) {
+      const uint32_t v = i / ipv;
+      if (listed) {
+        for (uint32_t k = 0; k < m; ++k)
+          c += (s_v[k] == v && s_x[k] >= r.x && s_x[k] <= r.z && s_y[k] >= r.y && s_y[k] <= r.w) ? 1u : 0u;
+      } else {
+        const ViewInfo* V = views + v;
+        const uint32_t tb = (uint32_t)__ldg(&V->tile_base), tx = (uint32_t)__ldg(&V->tiles_x);
+        for (uint32_t y = r.y; y <= r.w; ++y)
+          for (uint32_t x = r.x; x <= r.z; ++x) c += __ldg(flag + tb + y * tx + x) != 0 ? 1u : 0u;
+      }
+    }
+    counts[i] = c;
+  }
+}
+
+__global__ void k_entry_guard2(const unsigned long long* base, unsigned long long* total2, uint32_t* count2,
+                               uint64_t capacity, uint32_t* error_word) {
+  if (*base + *total2 > capacity) {
+    atomicOr(error_word, ERR_ENTRY_CAPACITY);
+    *total2 = 0;
+    *count2 = 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ranges_reset_list(const uint32_t* list, const uint32_t* count, uint2* ranges,
+                                                           uint32_t max_list) {
+  const uint32_t m = min(*count, max_list);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    ranges[list[i]] = make_uint2(0u, 0u);
+}
+
+// One block per listed tile: the range recorded by the completion sort
+// becomes [start, end), and the row-group summary of the first skip[i]
+// entries (those pass 1 composited) moves from src[i] to the new start.
+__global__ void __launch_bounds__(256) k_ranges_fix_list(const uint32_t* list, const uint32_t* count, uint2* ranges,
+                                                         uint32_t max_list, unsigned long long* entry_total,
+                                                         const unsigned long long* total2, uint8_t* gmask,
+                                                         const uint32_t* skip, const uint32_t* src) {
+  const uint32_t m = min(*count, max_list);
+  for (uint32_t i = blockIdx.x; i < m; i += gridDim.x) {
+    const uint32_t t = list[i];
+    const uint2 r = ranges[t];
+    __syncthreads();  // every thread holds the recorded range before it is replaced
+    const uint2 f = r.y ? make_uint2(~r.x, r.y) : make_uint2(0u, 0u);
+    if (threadIdx.x == 0) ranges[t] = f;
+    if (gmask != nullptr) {
+      const uint32_t sk = skip[i], from = src[i];
+      if (f.y - f.x >= sk)
+        for (uint32_t j = threadIdx.x; j < sk; j += blockDim.x) gmask[f.x + j] = gmask[from + j];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *entry_total += *total2;
+}
+
 __global__ void __launch_bounds__(256) k_ranges(const uint2* pairs, const unsigned long long* total,
                                                 uint64_t capacity, uint2* ranges, uint32_t num_tiles) {
   const uint64_t n = min((uint64_t)*total, capacity);
@@ -428,18 +597,19 @@ int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_
 
 template <class IO, class SWAP>
 int radix_passes(IO io, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch, int* result_in_1,
-                 cudaStream_t st, SWAP swap, uint2* ranges = nullptr, uint32_t num_ranges = 0) {
+                 cudaStream_t st, SWAP swap, uint2* ranges = nullptr, uint32_t num_ranges = 0,
+                 const unsigned long long* base = nullptr) {
   auto* hist = reinterpret_cast<uint32_t*>(scratch);
   int in1 = 0;
   for (int shift = 0; shift < key_bits; shift += 8) {
     const int nbits = key_bits - shift < 8 ? key_bits - shift : 8;
-    k_rs_upsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist);
+    k_rs_upsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist, base);
     const int e = launch_scan(hist, nullptr, hist, (uint64_t)RS_BINS * SORT_GRID, nullptr, nullptr, nullptr,
                               hist + RS_BINS * SORT_GRID, st);
     if (e) return e;
     const bool last = shift + 8 >= key_bits;
     k_rs_downsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist,
-                                                         last ? ranges : nullptr, num_ranges);
+                                                         last ? ranges : nullptr, num_ranges, base);
     swap(io);
     in1 ^= 1;
   }
@@ -457,7 +627,8 @@ int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, ui
 }
 
 int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch,
-                            int* result_in_1, cudaStream_t st, uint2* ranges, uint32_t num_ranges) {
+                            int* result_in_1, cudaStream_t st, uint2* ranges, uint32_t num_ranges,
+                            const unsigned long long* base) {
   PairIO io{p0, p1};
   return radix_passes(
       io, n_host, n_dev, key_bits, scratch, result_in_1, st,
@@ -465,12 +636,52 @@ int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_
         PairIO y{x.out, const_cast<uint2*>(x.in)};
         x = y;
       },
-      ranges, num_ranges);
+      ranges, num_ranges, base);
 }
 
 int launch_expand(const ExpandArgs& a, cudaStream_t st) {
   const int grid = grid_for((uint64_t)a.n_items_host, 256, 148 * 16);
   k_expand<<<grid, 256, 0, st>>>(a);
+  return (int)cudaGetLastError();
+}
+
+int launch_expand_filtered(const ExpandFilterArgs& a, cudaStream_t st) {
+  const int grid = grid_for((uint64_t)a.n_items_host, 256, 148 * 16);
+  k_expand_filtered<<<grid, 256, 0, st>>>(a);
+  return (int)cudaGetLastError();
+}
+
+int launch_cut_gate(const uint32_t* inc_count, uint32_t n_items, uint32_t* gate_n, cudaStream_t st) {
+  k_cut_gate<<<1, 1, 0, st>>>(inc_count, n_items, gate_n);
+  return (int)cudaGetLastError();
+}
+
+int launch_count_flagged(const uint4* rects, const ViewInfo* views, uint32_t n_views, uint32_t items_per_view,
+                         uint32_t n_items, const uint32_t* inc_count, const uint32_t* inc_list, const uint8_t* flag,
+                         uint32_t* counts, cudaStream_t st) {
+  if (n_items == 0) return 0;
+  k_count_flagged<<<grid_for(n_items, 256, 148 * 4), 256, 0, st>>>(rects, views, n_views, items_per_view, n_items,
+                                                                    inc_count, inc_list, flag, counts);
+  return (int)cudaGetLastError();
+}
+
+int launch_entry_guard2(const unsigned long long* base, unsigned long long* total2, uint32_t* count2,
+                        uint64_t capacity, uint32_t* error_word, cudaStream_t st) {
+  k_entry_guard2<<<1, 1, 0, st>>>(base, total2, count2, capacity, error_word);
+  return (int)cudaGetLastError();
+}
+
+int launch_ranges_reset_list(const uint32_t* list, const uint32_t* count, uint2* ranges, uint32_t max_list,
+                             cudaStream_t st) {
+  if (max_list == 0) return 0;
+  k_ranges_reset_list<<<grid_for(max_list, 256, 148), 256, 0, st>>>(list, count, ranges, max_list);
+  return (int)cudaGetLastError();
+}
+
+int launch_ranges_fix_list(const uint32_t* list, const uint32_t* count, uint2* ranges, uint32_t max_list,
+                           unsigned long long* entry_total, const unsigned long long* total2, uint8_t* gmask,
+                           const uint32_t* skip, const uint32_t* src, cudaStream_t st) {
+  k_ranges_fix_list<<<148, 256, 0, st>>>(list, count, ranges, max_list, entry_total, total2, gmask, skip, src);
   return (int)cudaGetLastError();
 }
 

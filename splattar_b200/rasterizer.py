@@ -17,7 +17,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import (BUF, FLAG_COLOR_ONLY, FLAG_DETERMINISTIC, FLAG_PERSISTENT, FLAG_STORED_STATE, FLAG_TIGHT_BINNING, PREC,
+from ._lib import (BUF, FLAG_COLOR_ONLY, FLAG_DETERMINISTIC, FLAG_FULL_LISTS, FLAG_PERSISTENT, FLAG_STORED_STATE,
+                   FLAG_TIGHT_BINNING, PREC,
                    AdamConfig, Camera,
                    DensifyConfig, GsError, McmcConfig, RasterConfig, SceneInputC, StepConfig, check, lib)
 
@@ -91,7 +92,7 @@ class SceneInput:
 _DTYPES = {
     "out_ncontrib": np.uint32, "ranges": np.uint32, "sorted_items": np.uint32, "entry_count": np.uint64,
     "loss": np.float64, "rects": np.uint32, "depth_keys": np.uint32, "depth_order": np.uint32,
-    "normal_loss": np.float64,
+    "normal_loss": np.float64, "incomplete_tiles": np.uint32, "tile_cut": np.uint32,
 }
 
 
@@ -102,11 +103,11 @@ class Rasterizer:
     def __init__(self, capacity: int, width: int, height: int, max_entries: int = 0, *, max_views: int = 1,
                  max_pixels: int = 0, precision: str = "f32", deterministic: bool = False,
                  persistent: bool = False, color_only: bool = False, tight: bool = False, batch: int = 128,
-                 pixels_per_thread: int = 0, stored_state: bool = False, tile: int = 16):
+                 pixels_per_thread: int = 0, stored_state: bool = False, tile: int = 16, full_lists: bool = False):
         self._h = None
         flags = (FLAG_DETERMINISTIC if deterministic else 0) | (FLAG_PERSISTENT if persistent else 0) | (
             FLAG_COLOR_ONLY if color_only else 0) | (FLAG_TIGHT_BINNING if tight else 0) | (
-            FLAG_STORED_STATE if stored_state else 0)
+            FLAG_STORED_STATE if stored_state else 0) | (FLAG_FULL_LISTS if full_lists else 0)
         cfg = RasterConfig(capacity, width, height, max_views, max_pixels, max_entries, tile, batch, PREC[precision],
                            flags, pixels_per_thread)
         h = C.c_void_p()
