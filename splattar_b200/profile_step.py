@@ -10,7 +10,9 @@ shapes (or autotunes when none are given), runs ``--warmup`` steps, then
 milliseconds per step and the tile-entry count. Every step is a complete
 forward + loss + backward + Adam pass; nothing is skipped. Launch order per
 chosen step: projection, depth sort, entry scan, expansion, tile sort, ranges,
-forward raster, L1+SSIM, backward raster, projection backward + Adam.
+forward raster, the occlusion cut's completion pass (gate, flagged counts,
+entry scan, guard, range reset, expansion, tile sort, range fix, forward
+raster), L1+SSIM, backward raster, projection backward + Adam.
 """
 from __future__ import annotations
 
