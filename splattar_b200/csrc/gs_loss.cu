@@ -105,19 +105,23 @@ __device__ __forceinline__ void slide11x2(const float (&w)[6], In in, Out out) {
 }
 
 // Moments → SSIM, its coefficient maps and the per-view loss sums.
-// Per channel: (μx, μy), (E[x²], E[y²]) as packed pairs and E[xy] scalar.
+// Eight blurred maps, seven of them packed pairs: per channel (μx, μy) and
+// (E[x²], E[y²]), then (E[xy]_r, E[xy]_g), and E[xy]_b scalar. Eight maps
+// give 208 horizontal row items and 256 vertical items (16 columns, two
+// halves of 8 rows), so both passes occupy the block in a single round.
 // Coefficient planes (scratch, coef_stride pixels each): float2 planes
 // (Cμ_r, Cμ_g), (Cx²_r, Cx²_g), (Cxy_r, Cxy_g), (Cμ_b, Cx²_b) at
 // coef + 2k·stride, and Cxy_b at coef + 8·stride.
+constexpr int NM2 = 7;  // packed maps
 __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
   __shared__ float2 s_in[3][EXT][IN_PITCH];     // (x, y) per channel, with halo
-  __shared__ float2 s_h2[3][2][EXT * H_ROW];    // horizontal: [ch][(μx,μy) | (x²,y²)][row][col]
-  __shared__ float s_h1[3][EXT * H_ROW];        // horizontal: [ch] E[xy]
+  __shared__ float2 s_h2[NM2][EXT * H_ROW];     // horizontal results of the packed maps [map][row][col]
+  __shared__ float s_h1[EXT * H_ROW];           // horizontal E[xy]_b
   __shared__ double s_red[2][8];
   // Vertical results reuse s_in after the horizontal pass.
-  float2* s_v2 = &s_in[0][0][0];                 // [ch][2][16×16]
-  float* s_v1 = reinterpret_cast<float*>(s_v2 + 3 * 2 * V_PLANE);  // [ch][16×16]
-  static_assert(3 * 2 * V_PLANE * 2 + 3 * V_PLANE <= 3 * EXT * IN_PITCH * 2, "vertical results fit in s_in");
+  float2* s_v2 = &s_in[0][0][0];                          // [map][16×16]
+  float* s_v1 = reinterpret_cast<float*>(s_v2 + NM2 * V_PLANE);  // [16×16]
+  static_assert(NM2 * V_PLANE * 2 + V_PLANE <= 3 * EXT * IN_PITCH * 2, "vertical results fit in s_in");
   const int tid = threadIdx.x;
   const TileLoc L = locate(a, blockIdx.x);
   for (int k = tid; k < EXT * EXT; k += 256) {
@@ -137,20 +141,26 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
 #pragma unroll
   for (int k = 0; k < 6; ++k) w[k] = a.w[k];
   __syncthreads();
-  // Horizontal: item = (channel, map kind, row): kind 0 (μx, μy) and kind 1
-  // (E[x²], E[y²]) packed, kind 2 E[xy] scalar.
-  for (int it = tid; it < 9 * EXT; it += 256) {
-    const int km = it / EXT, r = it - km * EXT, ch = km / 3, kind = km - ch * 3;
-    const float2* XY = &s_in[ch][r][0];
-    if (kind == 0) {
-      float2* O = &s_h2[ch][0][r * H_ROW];
-      slide11x2<T16>(w, [&](int i) { return XY[i]; }, [&](int o, float2 v) { O[o] = v; });
-    } else if (kind == 1) {
-      float2* O = &s_h2[ch][1][r * H_ROW];
-      slide11x2<T16>(w, [&](int i) { const float2 v = XY[i]; return __fmul2_rn(v, v); }, [&](int o, float2 v) { O[o] = v; });
+  // Horizontal: item = (map, row).
+  for (int it = tid; it < (NM2 + 1) * EXT; it += 256) {
+    const int m = it / EXT, r = it - m * EXT;
+    if (m < 6) {
+      const float2* XY = &s_in[m >> 1][r][0];
+      float2* O = &s_h2[m][r * H_ROW];
+      if (m & 1)
+        slide11x2<T16>(w, [&](int i) { const float2 v = XY[i]; return __fmul2_rn(v, v); }, [&](int o, float2 v) { O[o] = v; });
+      else
+        slide11x2<T16>(w, [&](int i) { return XY[i]; }, [&](int o, float2 v) { O[o] = v; });
+    } else if (m == 6) {
+      const float2* R = &s_in[0][r][0];
+      const float2* G = &s_in[1][r][0];
+      float2* O = &s_h2[6][r * H_ROW];
+      slide11x2<T16>(w, [&](int i) { const float2 u = R[i], v = G[i]; return make_float2(u.x * u.y, v.x * v.y); },
+                     [&](int o, float2 v) { O[o] = v; });
     } else {
-      float* O = &s_h1[ch][r * H_ROW];
-      slide11<T16>(w, [&](int i) { const float2 v = XY[i]; return v.x * v.y; }, [&](int o, float v) { O[o] = v; });
+      const float2* B = &s_in[2][r][0];
+      float* O = &s_h1[r * H_ROW];
+      slide11<T16>(w, [&](int i) { const float2 v = B[i]; return v.x * v.y; }, [&](int o, float v) { O[o] = v; });
     }
   }
   // L1 of this thread's pixel, read before s_in is reused.
@@ -164,17 +174,17 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
     if (inside) l1 += fabsf(v.x - v.y);
   }
   __syncthreads();
-  // Vertical: item = (channel, map kind, column): kinds 0, 1 packed, 2 scalar.
-  if (tid < 3 * 3 * T16) {
-    const int c = tid % T16, km = tid / T16, ch = km / 3, kind = km % 3;
-    if (kind < 2) {
-      const float2* I = &s_h2[ch][kind][c];
-      float2* O = s_v2 + (ch * 2 + kind) * V_PLANE + c;
-      slide11x2<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float2 v) { O[o * T16] = v; });
+  // Vertical: item = (map, column, half): rows 8h..8h+7 from input rows 8h..8h+17.
+  {
+    const int m = tid >> 5, c = tid & 15, h = (tid >> 4) & 1;
+    if (m < NM2) {
+      const float2* I = &s_h2[m][c + 8 * h * H_ROW];
+      float2* O = s_v2 + m * V_PLANE + c + 8 * h * T16;
+      slide11x2<8>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float2 v) { O[o * T16] = v; });
     } else {
-      const float* I = &s_h1[ch][c];
-      float* O = s_v1 + ch * V_PLANE + c;
-      slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+      const float* I = &s_h1[c + 8 * h * H_ROW];
+      float* O = s_v1 + c + 8 * h * T16;
+      slide11<8>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
     }
   }
   __syncthreads();
@@ -189,17 +199,20 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
     for (int ch = 0; ch < 3; ++ch) {
       const int q = oy * T16 + ox;
       const float2 mu = s_v2[(ch * 2) * V_PLANE + q], b2 = s_v2[(ch * 2 + 1) * V_PLANE + q];
-      const float bxy = s_v1[ch * V_PLANE + q];
+      const float bxy = ch == 0 ? s_v2[6 * V_PLANE + q].x : (ch == 1 ? s_v2[6 * V_PLANE + q].y : s_v1[q]);
       const float mu_x = mu.x, mu_y = mu.y;
       const float sx2 = b2.x - mu_x * mu_x, sy2 = b2.y - mu_y * mu_y, sxy = bxy - mu_x * mu_y;
       const float p = mu_x * mu_x + mu_y * mu_y + C1;
       const float qd = sx2 + sy2 + C2;
-      const float l = (2.0f * mu_x * mu_y + C1) / p;
-      const float cs = (2.0f * sxy + C2) / qd;
+      // p >= C1 and qd ~>= C2: one approximate reciprocal each (about 1 ulp)
+      // replaces the four IEEE divisions of the expressions.
+      const float ip = __fdividef(1.0f, p), iq = __fdividef(1.0f, qd);
+      const float l = (2.0f * mu_x * mu_y + C1) * ip;
+      const float cs = (2.0f * sxy + C2) * iq;
       ss += l * cs;
-      cm[ch] = (cs * (2.0f * mu_y - 2.0f * mu_x * l) / p + l * (-2.0f * mu_y + 2.0f * mu_x * cs) / qd) * dw;
-      cx2[ch] = (-l * cs / qd) * dw;
-      cxy[ch] = (2.0f * l / qd) * dw;
+      cm[ch] = (cs * (2.0f * mu_y - 2.0f * mu_x * l) * ip + l * (-2.0f * mu_y + 2.0f * mu_x * cs) * iq) * dw;
+      cx2[ch] = (-l * cs * iq) * dw;
+      cxy[ch] = (2.0f * l * iq) * dw;
     }
     float2* P2 = reinterpret_cast<float2*>(a.coef);
     const size_t st2 = a.coef_stride;  // float2 plane k starts at float offset 2k·stride
@@ -262,16 +275,19 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
     }
   }
   __syncthreads();
-  if (tid < 5 * T16) {
-    const int m = tid / T16, c = tid - m * T16;
+  // Vertical: item = (map, column, segment), segments of 6 rows starting at
+  // rows 0, 5 and 10 (rows 5 and 10 are computed twice, identically).
+  if (tid < 5 * T16 * 3) {
+    const int m = tid / (3 * T16), rem = tid - m * 3 * T16, sg = rem / T16, c = rem - sg * T16;
+    const int r0 = 5 * sg;
     if (m < 4) {
-      const float2* I = &s_h2[m][c];
-      float2* O = s_v2 + m * V_PLANE + c;
-      slide11x2<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float2 v) { O[o * T16] = v; });
+      const float2* I = &s_h2[m][c + r0 * H_ROW];
+      float2* O = s_v2 + m * V_PLANE + c + r0 * T16;
+      slide11x2<6>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float2 v) { O[o * T16] = v; });
     } else {
-      const float* I = &s_h1[c];
-      float* O = s_v1 + c;
-      slide11<T16>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+      const float* I = &s_h1[c + r0 * H_ROW];
+      float* O = s_v1 + c + r0 * T16;
+      slide11<6>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
     }
   }
   __syncthreads();
