@@ -185,6 +185,34 @@ __device__ __forceinline__ bool box_hits_tile(const float4& b, const TileGeo<PPT
   return b.x <= g.bx1 && b.y >= g.bx0 && b.z <= g.by1 && b.w >= g.by0;
 }
 
+// Bits r (0 <= r < TS) with c0 + r in [z0, z1], for pixel centres c0 + r.
+// The candidate ends come from the float differences (off by at most one
+// for |z - c0| < 2^23; larger values are clamped) and are corrected with the
+// same comparisons the per-pixel test makes, so the result is exact.
+template <int TS>
+__device__ __forceinline__ uint32_t span_bits(float c0, float z0, float z1) {
+  int lo = (int)ceilf(fminf(fmaxf(z0 - c0, -1.0f), (float)TS));
+  if (lo < TS && !(c0 + (float)lo >= z0)) ++lo;
+  if (lo > 0 && c0 + (float)(lo - 1) >= z0) --lo;
+  int hi = (int)floorf(fminf(fmaxf(z1 - c0, -1.0f), (float)TS));
+  if (hi >= 0 && !(c0 + (float)hi <= z1)) --hi;
+  if (hi < TS - 1 && c0 + (float)(hi + 1) <= z1) ++hi;
+  lo = max(lo, 0);
+  hi = min(hi, TS - 1);
+  if (hi < lo) return 0u;
+  return ((2u << hi) - 1u) & ~((1u << lo) - 1u);
+}
+
+// Pixel masks of an entry's α-box over the tile: bit r of .x when pixel row r
+// of the tile (centre by0 + r) lies in [b.z, b.w], bit c of .y when column c
+// (centre bx0 + c) lies in [b.x, b.y]: the per-pixel box test, decided once
+// per staged entry (backward); a lane then tests bits instead of comparing per
+// pixel.
+template <int TS, int PPT>
+__device__ __forceinline__ uint2 box_masks(const float4& b, const TileGeo<PPT>& g) {
+  return make_uint2(span_bits<TS>(g.by0, b.z, b.w), span_bits<TS>(g.bx0, b.x, b.y));
+}
+
 // Compaction of one staging round: returns this thread's slot among the kept
 // entries of the round (valid when keep) and the number kept. Order is
 // preserved. Rounds alternate between two s_wcount rows, so the next round's
@@ -513,7 +541,8 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
   // gather them by shuffles and emit the vector reduction (or ordered store)
   // at once, without staging them in shared memory.
   constexpr bool DIRECT = !AUX && NW == 1;
-  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
+  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH];
+  __shared__ uint2 s_msk[BATCH];  // box_masks of the staged entry
   __shared__ float4 s_r4[AUX ? BATCH : 1];
   __shared__ uint32_t s_item[BATCH];
   __shared__ uint32_t s_q[DET ? BATCH : 1];
@@ -661,7 +690,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
           load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (AUX) s_r4[slot] = r4;
-          s_bb[slot] = bb;
+          s_msk[slot] = box_masks<TS, PPT>(bb, g);
           s_item[slot] = item;
           if (DET) s_q[slot] = q;
           s_j[slot] = j;
@@ -705,12 +734,13 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             continue;
           }
         }
-        const float4 bbk = s_bb[k];
+        const uint2 mk = s_msk[k];
+        const uint32_t rows = mk.x >> L::row(tid);  // bit p: pixel p's row is inside the box
         float gg[NG];
 #pragma unroll
         for (int c = 0; c < NG; ++c) gg[c] = 0.f;
         bool contrib = false;
-        if (masks ? anybit : ((gm & thread_gbits) && g.pxc >= bbk.x && g.pxc <= bbk.y)) {
+        if (masks ? anybit : ((gm & thread_gbits) && ((mk.y >> L::col(tid)) & 1u))) {
           const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
@@ -727,7 +757,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
 #pragma unroll
           for (int q = 0; q < PS; ++q) {
             const int p = pp + q;
-            need[q] = masks ? bit[p] : (cidx < nc[p] && (gm & pbit[p]) && g.pyc[p] >= bbk.z && g.pyc[p] <= bbk.w);
+            need[q] = masks ? bit[p] : (cidx < nc[p] && (gm & pbit[p]) && ((rows >> p) & 1u));
           }
           if constexpr (PS == 2) {
             if (!need[0] && !need[1]) continue;
