@@ -27,9 +27,11 @@ MOMENTS = ("m_pos", "m_scales", "m_quat", "m_opacity", "m_sh")
 WIDTH = {"m_pos": 4, "m_scales": 2, "m_quat": 4, "m_opacity": 1, "m_sh": 48}
 
 
-def _pair(lr_zero: bool, tile: int = 16, extra_full: bool = False):
+def _pair(lr_zero: bool, tile: int = 16, extra_full: bool = False, big: bool = False):
     s = make_surfels(N, 7, True, 3, 0.1)
     t = make_surfels(N, 8, True, 3, 0.1)
+    if big:  # 2 % of the surfels eight times larger: tile rects of more than 32 tiles
+        s.scales[::50] *= 8.0
     cams = ring_cameras(RES)
     P = sum(w * h for w, h in RES)
     out = []
@@ -70,8 +72,12 @@ def _same_step(a, b, P):
         assert np.abs(ma - mb).max() <= 1e-4 * scale, k
 
 
-def test_reused_cuts_give_full_list_results():
-    a, b, cams, P, step = _pair(lr_zero=True)
+@pytest.mark.parametrize("big", [False, True])
+def test_reused_cuts_give_full_list_results(big):
+    """Binning under the cut takes kept-tile bits for rects of up to 32 tiles
+    and tests each tile for larger rects; `big` adds surfels whose rects are
+    larger."""
+    a, b, cams, P, step = _pair(lr_zero=True, big=big)
     for k in range(4):
         a.train_step(cams, N, step)
         b.train_step(cams, N, step)
