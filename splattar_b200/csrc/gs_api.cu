@@ -185,6 +185,10 @@ struct gs_rasterizer {
 
   // graph of the chosen-form step
   cudaStream_t cap_stream = nullptr;
+  // side stream of the chosen step: clears grad_geom and orders the
+  // backward's tiles while the forward and the loss run
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_fwd = nullptr, ev_side = nullptr;
   cudaGraphExec_t graph = nullptr;
   std::vector<uint64_t> graph_key;
 };
@@ -491,9 +495,12 @@ RasterArgs bwd_args(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, int til
   return ra;
 }
 
+// prepared: grad_geom already cleared and the tile order already computed
+// (the chosen step does both on its side stream).
 gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, int tiles, uint32_t n, int prec,
-                              bool aux, bool persistent, cudaStream_t st) {
-  if (!r->det) TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)nv * n, st));
+                              bool aux, bool persistent, cudaStream_t st, bool prepared = false) {
+  if (!r->det && !prepared)
+    TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)nv * n, st));
   RasterArgs ra = bwd_args(r, vdev, nv, tiles);
   if (r->gmask_valid && !aux && r->tile == 16) ra.gmask = r->gmask;  // summary of the matching forward
   if (r->mask_valid && !aux) {  // masks of the matching colour-only forward
@@ -506,7 +513,7 @@ gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t n
     grid = std::min(tiles, r->num_sms * raster_bwd_occupancy(r->tile, prec, aux, r->bwd_ppt, r->bwd_batch, r->det,
                                                               ra.mask != nullptr));
     if (r->order_valid) {  // heaviest first by how far each tile's walk goes
-      TRY_LAUNCH(r, launch_tile_order(r->ranges, r->tile_walk, (uint32_t)tiles, r->tile_order, st));
+      if (!prepared) TRY_LAUNCH(r, launch_tile_order(r->ranges, r->tile_walk, (uint32_t)tiles, r->tile_order, st));
       ra.tile_order = r->tile_order;
     }
   }
@@ -642,6 +649,13 @@ gs_status ensure_graph_stream(gs_rasterizer* r) {
   return GS_OK;
 }
 
+gs_status ensure_side_stream(gs_rasterizer* r) {
+  if (!r->side_stream) TRY_CUDA(r, cudaStreamCreateWithFlags(&r->side_stream, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&r->ev_fork, &r->ev_fwd, &r->ev_side})
+    if (!*e) TRY_CUDA(r, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  return GS_OK;
+}
+
 // The chosen-form step body: batched forward, loss, backward raster, fused
 // projection backward + Adam. Recorded into a graph by train_step.
 gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_config* cfg, cudaStream_t st,
@@ -650,15 +664,28 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   const ViewInfo* vdev = r->views_dev;
   int tiles = 0;
   for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
+  // Side stream (forked from and joined into st, so it is part of a captured
+  // graph): grad_geom is cleared during the forward; the backward's tile
+  // order is computed during the loss.
+  cudaStream_t side = r->side_stream;
+  TRY_CUDA(r, cudaEventRecord(r->ev_fork, st));
+  TRY_CUDA(r, cudaStreamWaitEvent(side, r->ev_fork, 0));
+  if (!r->det) TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)nv * n, side));
   // With GS_FLAG_COLOR_ONLY the step's forward leaves depth and normal unwritten (nothing reads them).
   gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, prof, r->color_only,
                             true);
   if (s) return s;
+  TRY_CUDA(r, cudaEventRecord(r->ev_fwd, st));
+  TRY_CUDA(r, cudaStreamWaitEvent(side, r->ev_fwd, 0));
+  if (r->order_valid)
+    TRY_LAUNCH(r, launch_tile_order(r->ranges, r->tile_walk, (uint32_t)tiles, r->tile_order, side));
+  TRY_CUDA(r, cudaEventRecord(r->ev_side, side));
   TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
   s = run_loss(r, vdev, r->views_batched.data(), nv, cfg->w_l1, cfg->w_ssim, r->loss_sums, st);
   if (s) return s;
   mark(prof, 6, st);
-  s = run_backward_raster(r, vdev, nv, tiles, n, prec, false, true, st);
+  TRY_CUDA(r, cudaStreamWaitEvent(st, r->ev_side, 0));
+  s = run_backward_raster(r, vdev, nv, tiles, n, prec, false, true, st, true);
   if (s) return s;
   mark(prof, 7, st);
   TRY_CUDA(r, cudaMemsetAsync(r->grad_cam, 0, sizeof(float) * 16 * nv, st));
@@ -875,6 +902,9 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
   if (!r) return GS_OK;
   if (r->graph) cudaGraphExecDestroy(r->graph);
   if (r->cap_stream) cudaStreamDestroy(r->cap_stream);
+  if (r->side_stream) cudaStreamDestroy(r->side_stream);
+  for (cudaEvent_t e : {r->ev_fork, r->ev_fwd, r->ev_side})
+    if (e) cudaEventDestroy(e);
   void* ptrs[] = {r->positions, r->scales, r->quats, r->opacities, r->sh, r->sh_half, r->records, r->rects,
                   r->item_keys[0], r->item_keys[1], r->item_vals[0], r->item_vals[1], r->counts, r->offsets,
                   r->entry_offset, r->ent_pairs[0], r->ent_pairs[1], r->exp_item,
@@ -1282,6 +1312,7 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, ui
   if (!r->graph || key != r->graph_key) {
     if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
     s = ensure_graph_stream(r);
+    if (!s) s = ensure_side_stream(r);
     if (s) return s;
     TRY_CUDA(r, cudaStreamSynchronize(st));
     TRY_CUDA(r, cudaStreamBeginCapture(r->cap_stream, cudaStreamCaptureModeThreadLocal));
@@ -1320,7 +1351,8 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
     for (int k = 0; k < 5; ++k) { dp.lr[k] = cfg->adam.lr[k]; dp.reg[k] = cfg->adam.reg[k]; }
     bias_corrections(cfg->adam.beta1, cfg->adam.beta2, r->t, dp.bc1, dp.bc2);
     TRY_CUDA(r, cudaMemcpyAsync(r->dyn_dev, &dp, sizeof(dp), cudaMemcpyHostToDevice, st));
-    s = chosen_body(r, nv, n, cfg, st, &prof);
+    s = ensure_side_stream(r);
+    if (!s) s = chosen_body(r, nv, n, cfg, st, &prof);
     r->accum_steps += 1;
   }
   if (s) return s;
