@@ -2,8 +2,9 @@
 (crates/gs-cpu-ref/tests/gradcheck.rs:109-326): central differences with an
 absolute step of 1e-6 against the analytic backward for every parameter class
 including the camera, tolerance 1e-7 + 1e-3·|g|, on the same seeded scenes.
-Plus the north_star's relative-step variant (step 1e-4·max(|x|, 1e-3)) on
-sampled parameters."""
+Plus a relative-step variant (step 1e-4·max(|x|, 1e-3), the finite-difference
+protocol of the FP64 gradient check at 1,024 surfels and 128×128) on sampled
+parameters."""
 import numpy as np
 import pytest
 
@@ -131,7 +132,7 @@ def test_gradcheck_aux_losses(seed, n, size):
 
 def test_relative_step_fd_sampled():
     """Central differences with relative step 1e-4 on sampled parameters of a
-    larger micro-scene (the north_star's FD protocol at CPU-friendly size)."""
+    larger micro-scene (the relative-step protocol at CPU-friendly size)."""
     scene, cam = make_scene(97, 64, 3, 48)
     w = make_weights(97 ^ 0x5A5A, 48 * 48)
     g = oracle.gradients(scene, cam, w)
