@@ -150,5 +150,37 @@ __device__ __forceinline__ float3 sh_raw_color(const void* sh, size_t i, int deg
   return sh_raw_color_with([&](int k) { return sh_coeff<PREC>(sh, i, k); }, deg, dir, b, nb);
 }
 
+// A surfel's 48 SH values held in registers, fetched with 16-byte loads
+// (12 for f32 storage, 6 for 16-bit); value j is taken from word j (f32) or
+// half j (16-bit). With compile-time j (unrolled loops) the selection is free.
+template <int PREC>
+struct ShRow {
+  static constexpr int Q = PREC == 0 ? SH_FLOATS / 4 : SH_FLOATS / 8;
+  uint4 q[Q];
+  __device__ __forceinline__ void load(const void* sh, size_t i) {
+    const uint4* p = reinterpret_cast<const uint4*>(sh) + i * Q;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) q[k] = __ldg(p + k);
+  }
+  __device__ __forceinline__ uint32_t word(int w) const {
+    const uint4& u = q[w >> 2];
+    const int c = w & 3;
+    return c == 0 ? u.x : (c == 1 ? u.y : (c == 2 ? u.z : u.w));
+  }
+  __device__ __forceinline__ float value(int j) const {
+    if constexpr (PREC == 0) {
+      return __uint_as_float(word(j));
+    } else {
+      using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
+      const uint32_t w = word(j >> 1);
+      const unsigned short bits = (unsigned short)((j & 1) ? (w >> 16) : (w & 0xffffu));
+      H h;
+      memcpy(&h, &bits, 2);
+      return h2f<H>(h);
+    }
+  }
+  __device__ __forceinline__ float3 coeff(int k) const { return f3(value(3 * k), value(3 * k + 1), value(3 * k + 2)); }
+};
+
 }  // namespace
 }  // namespace gs

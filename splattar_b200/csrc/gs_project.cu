@@ -107,7 +107,9 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float3 dir = f3(g.x.x / lx, g.x.y / lx, g.x.z / lx);
   float b[16];
   int nb;
-  float3 raw = sh_raw_color<PREC>(a.sh, i, k.deg, dir, b, nb);
+  ShRow<PREC> row;
+  row.load(a.sh, i);
+  float3 raw = sh_raw_color_with([&](int kk) { return row.coeff(kk); }, k.deg, dir, b, nb);
   float3 color = f3(fmaxf(raw.x, 0.0f), fmaxf(raw.y, 0.0f), fmaxf(raw.z, 0.0f));
 
   // Normal facing the camera (surfel_prep_fwd.wgsl:188-194).
