@@ -405,6 +405,39 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
               if (!need[0]) continue;
               hh[0] = eval_hit(cp, r0, r1, r2, r4.w, g.sy[pp], g.pyc[pp]);
             }
+            if constexpr (PS == 2 && COLOR && !MASK) {
+              // Both pixels of the pair composited at once in packed FP32: a
+              // pixel that does not take the entry gets α = 0, so its weight is
+              // 0 and its T is multiplied by 1 (both exact); each component
+              // rounds as the scalar code below would.
+              const float a0 = fminf(__fmul_rn(r3.w, hh[0].ghat), ALPHA_CLAMP);
+              const float a1 = fminf(__fmul_rn(r3.w, hh[PS - 1].ghat), ALPHA_CLAMP);
+              const bool c0 = need[0] && !(a0 < ALPHA_SKIP), c1 = need[PS - 1] && !(a1 < ALPHA_SKIP);
+              if (c0 || c1) {
+                const float2 al = make_float2(c0 ? a0 : 0.f, c1 ? a1 : 0.f);
+                const float2 Tp = make_float2(T[pp], T[pp + 1]);
+                const float2 w = __fmul2_rn(Tp, al);
+                float2 vr = __ffma2_rn(make_float2(r3.x, r3.x), w, make_float2(cr[pp], cr[pp + 1]));
+                float2 vg = __ffma2_rn(make_float2(r3.y, r3.y), w, make_float2(cg[pp], cg[pp + 1]));
+                float2 vb = __ffma2_rn(make_float2(r3.z, r3.z), w, make_float2(cb[pp], cb[pp + 1]));
+                float2 va = __fadd2_rn(make_float2(aa[pp], aa[pp + 1]), w);
+                const float2 Tn = __fmul2_rn(Tp, __fadd2_rn(make_float2(1.0f, 1.0f), make_float2(-al.x, -al.y)));
+                cr[pp] = vr.x; cr[pp + 1] = vr.y; cg[pp] = vg.x; cg[pp + 1] = vg.y;
+                cb[pp] = vb.x; cb[pp + 1] = vb.y; aa[pp] = va.x; aa[pp + 1] = va.y;
+                T[pp] = Tn.x; T[pp + 1] = Tn.y;
+                if (c0) {
+                  nc[pp] = idx1;
+                  if (GM) gcur[(((L::row(tid) & 3) + pp) >> 2) & (GPL - 1)] |= kbit;
+                  if (Tn.x < T_TERMINATE) done[pp] = true;
+                }
+                if (c1) {
+                  nc[pp + 1] = idx1;
+                  if (GM) gcur[(((L::row(tid) & 3) + pp + 1) >> 2) & (GPL - 1)] |= kbit;
+                  if (Tn.y < T_TERMINATE) done[pp + 1] = true;
+                }
+              }
+              continue;
+            }
 #pragma unroll
             for (int q = 0; q < PS; ++q) {
               const int p = pp + q;

@@ -157,3 +157,30 @@ def test_cut_is_off_where_documented():
         r = Rasterizer(1000, 64, 64, **kw)
         with pytest.raises(Exception, match="GS_ERR_STATE"):
             r.read("incomplete_tiles", 1)
+
+
+def test_chosen_forward_launch_shapes_agree():
+    """The colour-only forward of the training step composites pixel pairs in
+    packed FP32 (2, 4 and 8 pixels per thread) and single pixels in scalar
+    code (1 pixel per thread): every shape gives bit-identical colour, final
+    T and contributor indices."""
+    s = make_surfels(20_000, 11, True, 3, 0.1)
+    cams = ring_cameras(RES)
+    P = sum(w * h for w, h in RES)
+    adam = AdamSettings(eps=1e-15)
+    adam.lr = {k: 0.0 for k in adam.lr}
+    step = StepSettings(0.8, 0.2, adam, "chosen")
+    outs = []
+    for fb, fp in [(64, 1), (128, 2), (64, 4), (64, 8)]:
+        r = Rasterizer(20_000, 0, 0, 20_000 * len(RES) * 64, max_views=len(RES), max_pixels=P, precision="f16",
+                       color_only=True)
+        r.upload_scene(s.scene_input())
+        r.write("target", np.full(4 * P, 0.5, np.float32))
+        r.optimizer_init(20_000)
+        r.set_launch_shapes(fb, fp, 128, 8)
+        r.train_step(cams, 20_000, step)
+        r.check()
+        outs.append(_images(r, P))
+    for o in outs[1:]:
+        for x, y in zip(outs[0], o):
+            assert np.array_equal(x, y)
