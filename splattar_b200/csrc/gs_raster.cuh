@@ -836,7 +836,11 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             }
             suf_c[p] += dc * w;
             T[p] = t_before;
-            gg[11] += dlc[p].x * w; gg[12] += dlc[p].y * w; gg[13] += dlc[p].z * w;
+            {  // packed pairs round per component as the scalar FFMAs (x·1 is exact)
+              const float2 c2 = __ffma2_rn(make_float2(dlc[p].x, dlc[p].y), make_float2(w, w), make_float2(gg[11], gg[12]));
+              gg[11] = c2.x; gg[12] = c2.y;
+              gg[13] += dlc[p].z * w;
+            }
             if (raw_alpha <= ALPHA_CLAMP) {
               // dL/dĝ·ĝ = dL/dα·o·ĝ; ray branch: ĝ = exp(−(u²+v²)/2) with
               // u = (s·Bu)/det, v = (s·Bv)/det, det = s·M, so dL/d(s·Bu) = −u·K/det,
@@ -847,12 +851,14 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
               const float K = dg * r3.w;
               if (h.ray) {
                 const float Ki = K * h.inv_det;
-                const float gun = -h.u * Ki, gvn = -h.v * Ki;
+                const float2 guv = __fmul2_rn(make_float2(-h.u, -h.v), make_float2(Ki, Ki));
                 float gdet = h.q2 * Ki;
                 if (AUX) gdet -= h.t * dl_dt * h.inv_det;
-                gg[1] += gdet * g.sy[p]; gg[2] += gdet;
-                gg[4] += gun * g.sy[p]; gg[5] += gun;
-                gg[7] += gvn * g.sy[p]; gg[8] += gvn;
+                const float2 sy1 = make_float2(g.sy[p], 1.0f);
+                const float2 m0 = __ffma2_rn(make_float2(gdet, gdet), sy1, make_float2(gg[1], gg[2]));
+                const float2 m1 = __ffma2_rn(make_float2(guv.x, guv.x), sy1, make_float2(gg[4], gg[5]));
+                const float2 m2 = __ffma2_rn(make_float2(guv.y, guv.y), sy1, make_float2(gg[7], gg[8]));
+                gg[1] = m0.x; gg[2] = m0.y; gg[4] = m1.x; gg[5] = m1.y; gg[7] = m2.x; gg[8] = m2.y;
                 if (AUX) gg[15] += dl_dt * h.inv_det;
               } else {
                 const float kk = K * (1.0f / LOWPASS_SIGMA2);
