@@ -80,8 +80,10 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
   Hit h;
   const float det = fmaf(r0.y, sy, c.det0);
   const float inv = rcp_approx(det);
-  const float u = __fmul_rn(fmaf(r1.y, sy, c.un0), inv);
-  const float v = __fmul_rn(fmaf(r2.y, sy, c.vn0), inv);
+  // (u·det, v·det) and (u, v) as packed pairs, rounding per component as fmaf / __fmul_rn.
+  const float2 uvn = __ffma2_rn(make_float2(r1.y, r2.y), make_float2(sy, sy), make_float2(c.un0, c.vn0));
+  const float2 uv = __fmul2_rn(uvn, make_float2(inv, inv));
+  const float u = uv.x, v = uv.y;
   const float t = __fmul_rn(r0.w, inv);
   const bool ray_ok = fabsf(det) > 1e-12f && t > NEAR_DEPTH;
   h.q2 = fmaf(u, u, __fmul_rn(v, v));
@@ -405,7 +407,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
               if (!need[0]) continue;
               hh[0] = eval_hit(cp, r0, r1, r2, r4.w, g.sy[pp], g.pyc[pp]);
             }
-            if constexpr (PS == 2 && COLOR && !MASK) {
+            if constexpr (PS == 2 && COLOR && !MASK && PPT <= 4) {  // (8 pixels per thread would spill)
               // Both pixels of the pair composited at once in packed FP32: a
               // pixel that does not take the entry gets α = 0, so its weight is
               // 0 and its T is multiplied by 1 (both exact); each component
@@ -862,8 +864,9 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
                 if (AUX) gg[15] += dl_dt * h.inv_det;
               } else {
                 const float kk = K * (1.0f / LOWPASS_SIGMA2);
-                gg[9] += cp.dx * kk;
-                gg[10] += h.dy * kk;
+                const float2 sd = __ffma2_rn(make_float2(cp.dx, h.dy), make_float2(kk, kk), make_float2(gg[9], gg[10]));
+                gg[9] = sd.x;
+                gg[10] = sd.y;
                 if (AUX) gg[16] += dl_dt;
               }
             }
