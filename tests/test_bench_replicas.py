@@ -62,3 +62,13 @@ def test_reference_arm_prints_on_rank0_only():
     r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_launch_count_matches_the_profiled_step():
+    """gpu_launches counts 64 kernels per chosen step on ring8_1m (35,392 tiles of 16 px over 8 views), the
+    number the ncu launch list of that step shows; the plain form launches per view."""
+    import bench
+    assert bench.launches_per_step(35392, 8, "chosen") == 64
+    # two tile-sort passes for up to 65,536 tiles; a third beyond that
+    assert bench.launches_per_step(70000, 16, "chosen") == 64 + 2 * 5
+    assert bench.launches_per_step(35392, 8, "plain") == 8 * (38 + 2 + 1 + 1) + 5
