@@ -66,7 +66,9 @@ enum {
                                       pixels terminate is binned and rendered again in full within the same step
                                       (counted in GS_BUF_INCOMPLETE_TILES). Images, contributor indices and
                                       gradients are those of the full lists; tile lists, ranges and the entry
-                                      count then cover the truncated lists */
+                                      count then cover the truncated lists, and the full lists of completed
+                                      tiles follow them in GS_BUF_SORTED_ITEMS (find a tile's list through
+                                      GS_BUF_RANGES) */
 };
 
 /* Rasterizer::new(ctx, capacity, width, height, max_entries)
