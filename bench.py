@@ -36,12 +36,31 @@ sys.path.insert(0, ROOT)
 METRIC = "fwd+bwd+Adam steps/s, 1M surfels 1080p: chosen vs plain form; HBM roofline frac"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel,
 # from one ncu capture of the same workload and launch shapes
-# (profile_step --workload ring8_1m --shapes 64,4,128,8).
+# (python profile_step.py --workload ring8_1m --shapes 64,4,128,8).
 TRAFFIC = {("ring8_1m", "raster_bwd"): 1_552_203_008}
 # Launch shapes (fwd batch, fwd pixels/thread, bwd batch, bwd pixels/thread)
 # tried for the plain form at 16-pixel tiles before it is timed.
 PLAIN_SHAPES = [(128, 2, 128, 2), (128, 2, 64, 4), (128, 1, 128, 2), (64, 4, 64, 8)]
 FALLBACK_HBM_GBS = 6650.0
+# FP32 arithmetic of the raster kernels (an FMA counts 2), counted from
+# splattar_b200/csrc/gs_raster.cuh, as (per hit evaluation, per contributing
+# pair, MUFU ops per hit evaluation, MUFU ops per contributing pair):
+#   hit test eval_hit / eval_hit2: det 1 FMA, u.det and v.det 2 FMA, u and v
+#     2 MUL, t 1 MUL, u^2+v^2 1 MUL + 1 FMA, q_ray 1 MUL, dy 1 ADD, q_screen
+#     1 FMA, exp 1 MUL + 1 EX2, 1/det 1 RCP (17 flops, 2 MUFU), alpha 1 MUL,
+#     plus the column partial sums (3 FMA, 1 ADD, 1 MUL = 8 flops per entry
+#     and thread, over 4 forward / 8 backward pixels per thread);
+#   forward composite: w 1 MUL, colour 3 FMA, alpha sum 1 ADD, T 1 ADD + 1 MUL;
+#   backward per contributor: 1 - alpha 1 ADD + 1 RCP, T_before 1 MUL, w 1 MUL,
+#     dL/dcolour.colour 1 MUL + 2 FMA, dL/dalpha 1 MUL + 1 FMA, suffix 1 FMA,
+#     colour gradient 3 FMA, dL/dghat, opacity sum, K 3 MUL/ADD, ray-branch
+#     record moments 1 + 2 + 1 MUL and 6 FMA (38 flops, 1 MUFU).
+RASTER_OPS = {"raster_fwd": (20, 10, 2, 0), "raster_bwd": (19, 38, 2, 1)}
+# Nominal B200 rates per SM per clock: 128 FP32 lanes (FMA = 2 flops), 16 MUFU.
+SM_COUNT, FP32_PER_SM_CLK, MUFU_PER_SM_CLK = 148, 256, 16
+# Issue-slot activity of the raster kernels measured by ncu on ring2_200k
+# (profiles/raster_fwd_bwd_ring2_200k.md).
+ISSUE_ACTIVE_NCU = {"raster_fwd": 0.800, "raster_bwd": 0.683}
 
 
 def parse(argv=None):
@@ -53,6 +72,8 @@ def parse(argv=None):
     p.add_argument("--workload", default="ring8_1m")
     p.add_argument("--precision", default="f16", choices=["f32", "f16", "bf16"])
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-full-lists", action="store_true",
+                   help="skip timing the chosen form without the occlusion cut")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU-baseline sample time")
     p.add_argument("--densify-every", type=int, default=0,
@@ -205,6 +226,62 @@ def algorithmic_bytes(stage: str, n: int, views, E: int, P: int) -> float:
     return 0.0
 
 
+def raster_compute(stage: str, work: dict, kernel_ms: float, sm_mhz) -> dict:
+    """Compute side of a raster kernel's roofline: FP32 flops and MUFU ops
+    from the device-counted hit evaluations and contributing pairs, over the
+    kernel's measured time, against the nominal rates at the sampled SM
+    clock."""
+    f_eval, f_contrib, m_eval, m_contrib = RASTER_OPS[stage]
+    evals = work["fwd_evals"] if stage == "raster_fwd" else work["bwd_evals"]
+    flops = f_eval * evals + f_contrib * work["contrib_pairs"]
+    mufu = m_eval * evals + m_contrib * work["contrib_pairs"]
+    hz = (sm_mhz or 1965.0) * 1e6
+    peak_tf = SM_COUNT * FP32_PER_SM_CLK * hz / 1e12
+    peak_mufu = SM_COUNT * MUFU_PER_SM_CLK * hz / 1e12
+    sec = kernel_ms * 1e-3
+    return {"bound": "issue", "hit_evaluations": evals, "contributing_pairs": work["contrib_pairs"],
+            "fp32_flops": flops, "achieved_tflops": round(flops / sec / 1e12, 3),
+            "peak_tflops": round(peak_tf, 2), "frac": round(flops / sec / 1e12 / peak_tf, 4),
+            "mufu_ops": mufu, "mufu_frac": round(mufu / sec / 1e12 / peak_mufu, 4),
+            "issue_active_ncu": ISSUE_ACTIVE_NCU.get(stage),
+            "peak_source": f"nominal B200: {SM_COUNT} SMs x {FP32_PER_SM_CLK} FP32 flops and {MUFU_PER_SM_CLK} MUFU "
+                           f"ops per clock at the sampled {hz / 1e6:.0f} MHz",
+            "ops_per_unit": {"flops_per_hit": f_eval, "flops_per_contributor": f_contrib, "mufu_per_hit": m_eval,
+                             "mufu_per_contributor": m_contrib}}
+
+
+def literal_baselines() -> dict:
+    """The reference CPU renderer's own O(P·N) per-pixel walk
+    (crates/gs-cpu-ref/src/forward.rs:207-246: every sorted surfel tested
+    against every pixel's tile), single-threaded, at the 16,384-surfel 256x256
+    scene and the 1,024-surfel 128x128 scene, and the binned step at the
+    16,384-surfel scene in full (no sampling), all host threads."""
+    import oracle
+    from splattar_b200.synthetic import look_at, make_surfels, workload
+    f64 = lambda a: np.asarray(a, np.float64)  # noqa: E731
+    out = {}
+    wl0 = workload("small_1view_256")
+    s0, c0 = wl0.surfels, wl0.cameras[0]
+    sc0 = oracle.Scene(f64(s0.positions), f64(s0.scales), f64(s0.quats), f64(s0.opacities), f64(s0.sh48()), 0)
+    cam0 = oracle.Camera(f64(c0.center), f64(c0.quat), float(c0.focal), c0.width, c0.height)
+    t = time.time()
+    oracle.render(sc0, cam0, literal=True)
+    out["literal_forward_16k_256px_s"] = round(time.time() - t, 3)
+    s1 = make_surfels(1024, 0, False, 0, 0.3)
+    c1 = look_at((0, 0, -3), (0, 0, 0), 128, 128, focal=128.0)
+    sc1 = oracle.Scene(f64(s1.positions), f64(s1.scales), f64(s1.quats), f64(s1.opacities), f64(s1.sh48()), 0)
+    cam1 = oracle.Camera(f64(c1.center), f64(c1.quat), float(c1.focal), 128, 128)
+    t = time.time()
+    oracle.render(sc1, cam1, literal=True)
+    out["literal_forward_1k_128px_s"] = round(time.time() - t, 3)
+    tgt = np.zeros((c0.width * c0.height, 4))
+    t = time.time()
+    oracle.cpu_step_timed(sc0, cam0, tgt, tile_stride=1, threads=oracle.max_threads())
+    out["binned_step_16k_256px_s"] = round(time.time() - t, 3)
+    out["threads"] = {"literal": 1, "binned": oracle.max_threads()}
+    return out
+
+
 def launches_per_step(n_tiles: int, nv: int, form: str) -> int:
     """Kernel launches of one step: projection; depth sort (4 radix passes of
     upsweep + 3-kernel histogram scan + downsweep); entry scan (3) and entry
@@ -260,20 +337,21 @@ def run_ours(args, ws, rank, local):
     chosen = StepSettings(0.8, 0.2, adam, "chosen")
     plain = StepSettings(0.8, 0.2, adam, "plain")
 
-    def timed(step_cfg, steps, warmup):
+    def timed(step_cfg, steps, warmup, h=None):
+        h = rast if h is None else h
         for _ in range(warmup):
-            rast.train_step(cams, n, step_cfg, sp)
-        rast.check(sp)
+            h.train_step(cams, n, step_cfg, sp)
+        h.check(sp)
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
-            rast.train_step(cams, n, step_cfg, sp)
+            h.train_step(cams, n, step_cfg, sp)
         e1.record(stream)
         torch.cuda.synchronize()
-        rast.check(sp)
+        h.check(sp)
         return max_over_ranks(e0.elapsed_time(e1) / steps, ws)
 
     clocks = ClockSampler(local)
@@ -353,17 +431,35 @@ def run_ours(args, ws, rank, local):
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps, ws)
     loss_vals = loss_host.numpy().copy()
 
-    # Stage timing (CUDA events between stages on the launch stream).
+    # Stage timing (CUDA events between stages on the launch stream), then
+    # the raster kernels' work on the last of those steps (counted on the
+    # device, outside every timed region).
     prof = [rast.train_step_profiled(cams, n, chosen, sp) for _ in range(3)]
     stages = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
+    work = rast.raster_work(sp)
     n_tiles = sum(((c.width + tile - 1) // tile) * ((c.height + tile - 1) // tile) for c in cams)
     rast.check(sp)
-    result = dict(tuned=tuned, wl=wl, n=n, nv=nv, P=P, E=E, redone=redone, ms_chosen=ms_chosen, ms_plain=ms_plain, ms_e2e=ms_e2e, clk=clk,
-                  plain_shapes=plain_shapes,
-                  handle_bytes=int(free0 - free1),
-                  stages=stages, n_tiles=n_tiles, loss=loss_vals, h2d=tgt_host.numel() * 4,
-                  d2h=loss_host.numel() * 8)
+    handle_bytes = int(free0 - free1)
     rast.close()
+
+    # The chosen form without the occlusion cut (full tile lists every step):
+    # its speed does not depend on the views repeating from step to step.
+    ms_full = None
+    if not args.no_full_lists and not args.stored_state:
+        rf = Rasterizer(n, 0, 0, max_entries, max_views=nv, max_pixels=P, precision=args.precision, color_only=True,
+                        full_lists=True)
+        rf.upload_scene(wl.surfels.scene_input())
+        rf.write("target", target)
+        rf.optimizer_init(n)
+        rf.tile = tile
+        rf.set_launch_shapes(tuned["fwd_batch"], tuned["fwd_pixels_per_thread"], tuned["bwd_batch"],
+                             tuned["bwd_pixels_per_thread"])
+        ms_full = timed(chosen, args.steps, args.warmup, rf)
+        rf.close()
+    result = dict(tuned=tuned, wl=wl, n=n, nv=nv, P=P, E=E, redone=redone, ms_chosen=ms_chosen, ms_plain=ms_plain,
+                  ms_e2e=ms_e2e, ms_full=ms_full, clk=clk, plain_shapes=plain_shapes, handle_bytes=handle_bytes,
+                  stages=stages, work=work, n_tiles=n_tiles, loss=loss_vals, h2d=tgt_host.numel() * 4,
+                  d2h=loss_host.numel() * 8)
     return result
 
 
@@ -463,6 +559,8 @@ def main():
     dom = max(stages, key=stages.get)
     alg = algorithmic_bytes(dom, n, r["wl"].cameras, E, P)
     achieved = alg / (stages[dom] * 1e-3) / 1e9 if stages[dom] > 0 else 0.0
+    sm_mhz = r["clk"].get("sm_mhz")
+    compute = {k: raster_compute(k, r["work"], stages[k], sm_mhz) for k in ("raster_fwd", "raster_bwd")}
     line = {
         "metric": METRIC,
         "value": round(job_steps_s, 4),
@@ -474,7 +572,10 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "f32" if args.precision == "f32" else f"f32 compute, {args.precision} storage",
+        "storage": None if args.precision == "f32" else
+        f"{args.precision}: SH coefficients and the projected record's normal and depth; geometry, colour, opacity, "
+        "compositing, gradients and Adam moments f32",
         "data": "synthetic",
         "config": {
             "workload": args.workload,
@@ -506,17 +607,26 @@ def main():
                     "16-pixel tiles",
             "launch_shapes": r["plain_shapes"]},
         "chosen_over_plain": None if r["ms_plain"] is None else round(r["ms_plain"] / r["ms_chosen"], 3),
+        "full_lists": None if r["ms_full"] is None else {
+            "steps_per_s": round(aggregate_steps_per_s(r["ms_full"], ws), 4), "ms_per_step": round(r["ms_full"], 4),
+            "over_plain": None if r["ms_plain"] is None else round(r["ms_plain"] / r["ms_full"], 3),
+            "form": "the chosen form with GS_FLAG_FULL_LISTS: no occlusion cut, full tile lists every step (its speed "
+                    "does not depend on the views repeating between steps)"},
         "e2e": {"value": round(aggregate_steps_per_s(r["ms_e2e"], ws), 4), "unit": "steps/s", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "ms_per_step": round(r["ms_e2e"], 4),
                 "path": "per step: pinned host target -> device staging (side stream, prefetched one step ahead) -> "
                         "Rasterizer.write_async(target) + gs_train_step + read_async(loss -> pinned host)"},
         "gpu_launches": launches_per_step(r["n_tiles"], nv, "chosen") * args.steps,
-        "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+        "roofline": {"kernel": dom, "bound": compute[dom]["bound"] if dom in compute else "hbm",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": TRAFFIC.get((args.workload, dom)),
-                     "traffic_unit": "DRAM bytes read + written per launch (ncu, profiles/raster_traffic_ring8_1m.md)",
+                     "traffic_unit": "DRAM bytes read + written per launch (ncu capture of this workload)",
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
                      else "fallback 6.65 TB/s",
-                     "algorithmic_bytes": alg, "kernel_ms": round(stages[dom], 4)},
+                     "algorithmic_bytes": alg, "kernel_ms": round(stages[dom], 4),
+                     "compute": compute.get(dom)},
+        "raster_compute": compute,
+        "raster_work": r["work"],
         "stages_ms": {k: round(v, 4) for k, v in stages.items()},
         "clocks": r["clk"],
         "loss": [float(x) for x in r["loss"][:4]],
@@ -526,11 +636,14 @@ def main():
         cores = oracle.max_threads()
         t0 = time.time()
         step_s, stride, detail = cpu_step_estimate(r["wl"], args.cpu_seconds, threads=cores)
+        spent = time.time() - t0
         line["cpu_baseline"] = {"value": round(1.0 / step_s, 6), "unit": "steps/s", "cores": cores, "kind": "port",
                                 "sample": f"all {nv} views; projection, tile lists, L1+SSIM, parameter chain and Adam "
                                           f"in full; per-pixel forward/backward on every {stride}th tile, scaled by "
-                                          f"{stride} ({time.time() - t0:.1f} s of CPU time)",
-                                "seconds_per_step": round(step_s, 3)}
+                                          f"{stride}",
+                                "extrapolated": True, "sample_fraction_of_pixel_walks": round(1.0 / stride, 5),
+                                "seconds_spent": round(spent, 2), "seconds_per_step": round(step_s, 3),
+                                "literal": literal_baselines()}
     print(json.dumps(line))
 
 
@@ -545,11 +658,13 @@ def main_reference(args, ws, rank):
     cores = oracle.max_threads()
     nv = len(wl.cameras)
     times = []
+    t0 = time.time()
     for k in range(args.warmup + args.steps):
         v = k % nv
         step_s, stride, _ = cpu_step_estimate(wl, 0, threads=cores, view_ids=[v])
         if k >= args.warmup:
             times.append(step_s)
+    spent = time.time() - t0
     step_s = statistics.mean(times)
     val = 1.0 / step_s
     line = {"metric": METRIC, "value": round(val, 6), "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
@@ -559,7 +674,9 @@ def main_reference(args, ws, rank):
             "cpu_baseline": {"value": round(val, 6), "unit": "steps/s", "cores": cores, "kind": "port",
                              "sample": f"each step one view (rotating) of {nv}: projection, tile lists, L1+SSIM, "
                                        f"parameter chain in full, per-pixel walks on every {stride}th tile scaled by "
-                                       f"{stride}, extrapolated to all {nv} views; Adam over all parameters"},
+                                       f"{stride}, extrapolated to all {nv} views; Adam over all parameters",
+                             "extrapolated": True, "sample_fraction_of_pixel_walks": round(1.0 / (stride * nv), 6),
+                             "seconds_spent": round(spent, 2)},
             "e2e": {"value": round(val, 6), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference (Rust + WGSL on wgpu/Vulkan) cannot be built or run here; this is its CPU "
                     "renderer's algorithm restated in C++"}

@@ -47,7 +47,10 @@ typedef enum {
 typedef enum { GS_PREC_F32 = 0, GS_PREC_F16 = 1, GS_PREC_BF16 = 2 } gs_precision;
 
 enum {
-  GS_FLAG_DETERMINISTIC = 1u << 0, /* ordered per-entry gradient reduction, no float atomics */
+  GS_FLAG_DETERMINISTIC = 1u << 0, /* ordered reductions, no float atomics on any gradient: per-entry record
+                                      gradients summed in entry order, parameter gradients in view order, camera
+                                      gradients as per-block partials summed in block order; results are bitwise
+                                      reproducible run to run */
   GS_FLAG_PERSISTENT = 1u << 1,    /* persistent raster kernels over a global tile queue */
   GS_FLAG_COLOR_ONLY = 1u << 2,    /* backward ignores dl_dcolor.w, dl_dnormal and lambda_dist; the chosen-form
                                       training step's forward writes colour, alpha and final T only (OUT_NORMAL and
@@ -179,6 +182,16 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r);
 gs_status gs_rasterizer_upload_scene(gs_rasterizer* r, const gs_scene_input* scene, void* stream);
 /* Rasterizer::lambda_dist (rasterizer.rs:60) */
 gs_status gs_rasterizer_set_lambda_dist(gs_rasterizer* r, float lambda_dist);
+/* No reference counterpart (the reference's device code has no waits). The
+ * chosen-form step's fused projection backward + Adam kernel copies each
+ * block's optimizer rows into shared memory with bulk copies and waits for
+ * them with two bounded waits: copy_wait_cycles before the block's Adam update
+ * (on expiry the block skips its update and sets the sticky error word, which
+ * gs_rasterizer_check reports as GS_ERR_DEVICE_TIMEOUT; 0 gives up at once)
+ * and drain_wait_cycles for the copies to land before an expired block exits
+ * (at least 1e8 cycles, else GS_ERR_INVALID_ARG). Defaults 2e9 and 2e9 SM
+ * cycles (about 1 s each at 1.965 GHz). Host-only; later steps use them. */
+gs_status gs_rasterizer_set_wait_limits(gs_rasterizer* r, uint64_t copy_wait_cycles, uint64_t drain_wait_cycles);
 /* Rasterizer::forward (rasterizer.rs:389-448): projection, binning, forward
  * raster for n_views cameras (1 = the reference's single-view call). */
 gs_status gs_rasterizer_forward(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
@@ -292,12 +305,21 @@ gs_status gs_adam_flat(float* raw, const float* grad_act, float* m, float* v, fl
  * form 1 = chosen: all views batched in one pass per stage, tight binning
  *          (GS_FLAG_TIGHT_BINNING), persistent raster kernels, projection
  *          backward fused with Adam, storage precision from the config, the
- *          whole step replayed as one CUDA graph. */
+ *          whole step replayed as one CUDA graph.
+ * loss 0 = L1+SSIM against TARGET with weights w_l1, w_ssim (Trainer::step).
+ * loss 1 = the image gradient the caller wrote into DL_DCOLOR (rgb; the
+ *          depth channel and DL_DNORMAL are not read) is used as it is: no
+ *          loss kernel runs and GS_BUF_LOSS is zero. This is the reference's
+ *          split between a loss producer that writes dl_dcolor (SsimLoss,
+ *          NormalLoss, the tracker's photometric loss,
+ *          crates/gs-track/src/lib.rs:134-142) and Rasterizer::backward. */
+enum { GS_LOSS_L1_SSIM = 0, GS_LOSS_GIVEN = 1 };
 typedef struct {
   float w_l1;
   float w_ssim;
   gs_adam_config adam;
   uint32_t form;
+  uint32_t loss;  /* GS_LOSS_* */
 } gs_step_config;
 gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
                         const gs_step_config* cfg, void* stream);
@@ -309,6 +331,15 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t n_view
  * 7 backward raster, 8 projection backward + Adam. */
 gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32_t n_views, uint32_t num_surfels,
                                  const gs_step_config* cfg, void* stream, float stage_ms[9], uint32_t* n_stages);
+
+/* No reference counterpart: the work of the raster kernels on the last
+ * forward, counted on the device by replaying each pixel's walk (for the
+ * compute side of their roofline; not meant for a timed region). out =
+ * {forward hit evaluations (list entries whose alpha box holds the pixel,
+ * up to the pixel's termination), contributing pairs (alpha >= 1/255, the
+ * forward's own decisions), backward hit evaluations (entries before the
+ * pixel's last contributor that the backward evaluates), pixels}. Blocking. */
+gs_status gs_raster_work(gs_rasterizer* r, uint64_t out[4], void* stream);
 
 /* Raster launch shapes (staging batch, pixels per thread) built per tile size:
  *   forward   tile 8:  ppt 1 or 2 with batch 64/128/256

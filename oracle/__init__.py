@@ -63,6 +63,10 @@ def lib():
         L.orc_render.restype = i32
         L.orc_gradients.argtypes = [vp, vp, i32, vp, vp, vp, f64, i32, vp]
         L.orc_gradients.restype = i32
+        L.orc_render_sampled.argtypes = [vp, vp, i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_render_sampled.restype = i32
+        L.orc_gradients_sampled.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, f64, i32, vp]
+        L.orc_gradients_sampled.restype = i32
         L.orc_distortion_loss.argtypes = [vp, vp, i32]
         L.orc_distortion_loss.restype = f64
         L.orc_project_f32.argtypes = [i32, vp, vp, vp, vp, vp, C.c_float, i32, i32, i32, vp, vp, vp]
@@ -161,20 +165,48 @@ def project(scene: Scene, cam: Camera, tile: int = 16):
     return rects, keys, marg.astype(bool), pos
 
 
-def render(scene: Scene, cam: Camera, tile: int = 16, literal: bool = False, threads: int = 0):
+def render(scene: Scene, cam: Camera, tile: int = 16, literal: bool = False, threads: int = 0,
+           tile_stride: int = 1, tile_offset: int = 0):
+    """Per-pixel forward outputs. With tile_stride > 1 only the pixels of
+    tiles t with t % tile_stride == tile_offset (row-major tile ids) are
+    rendered (the others stay zero, `sampled` marks the rendered ones).
+    Except for the literal walk, `last` holds each rendered pixel's last
+    contributing surfel (input index, -1 if none) and `count` its number of
+    contributing surfels."""
     P = cam.width * cam.height
     out = dict(color=np.zeros((P, 3)), alpha=np.zeros(P), depth=np.zeros(P), normal=np.zeros((P, 3)),
-               trans=np.zeros(P), ncontrib=np.zeros(P, np.int32), marginal=np.zeros(P, np.uint8))
+               trans=np.zeros(P), ncontrib=np.zeros(P, np.int32), marginal=np.zeros(P, np.uint8),
+               last=np.full(P, -1, np.int32), count=np.zeros(P, np.int32))
     s, c = scene.c(), cam.c()
-    lib().orc_render(C.byref(s), C.byref(c), tile, int(literal), threads, _p(out["color"]), _p(out["alpha"]),
-                     _p(out["depth"]), _p(out["normal"]), _p(out["trans"]), _p(out["ncontrib"]),
-                     _p(out["marginal"]))
+    if not literal:
+        rc = lib().orc_render_sampled(C.byref(s), C.byref(c), tile, tile_stride, tile_offset, threads,
+                                      _p(out["color"]), _p(out["alpha"]), _p(out["depth"]), _p(out["normal"]),
+                                      _p(out["trans"]), _p(out["ncontrib"]), _p(out["marginal"]), _p(out["last"]),
+                                      _p(out["count"]))
+        assert rc == 0, "bad tile sample"
+    else:
+        lib().orc_render(C.byref(s), C.byref(c), tile, int(literal), threads, _p(out["color"]), _p(out["alpha"]),
+                         _p(out["depth"]), _p(out["normal"]), _p(out["trans"]), _p(out["ncontrib"]),
+                         _p(out["marginal"]))
     out["marginal"] = out["marginal"].astype(bool)
+    out["sampled"] = sampled_pixels(cam, tile, tile_stride, tile_offset)
     return out
 
 
+def sampled_pixels(cam: Camera, tile: int = 16, tile_stride: int = 1, tile_offset: int = 0) -> np.ndarray:
+    """Mask (P,) of the pixels whose row-major tile id t has t % tile_stride == tile_offset."""
+    tiles_x = (cam.width + tile - 1) // tile
+    ys, xs = np.divmod(np.arange(cam.width * cam.height), cam.width)
+    t = (ys // tile) * tiles_x + xs // tile
+    return (t % tile_stride) == tile_offset
+
+
 def gradients(scene: Scene, cam: Camera, dl_dcolor, dl_ddepth=None, dl_dnormal=None, lambda_dist: float = 0.0,
-              tile: int = 16, threads: int = 0):
+              tile: int = 16, threads: int = 0, tile_stride: int = 1, tile_offset: int = 0):
+    """Parameter and camera gradients of a loss with the given per-pixel image
+    gradients. With tile_stride > 1 only the pixels of the sampled tiles
+    (t % tile_stride == tile_offset) are walked: the exact gradient of a loss
+    whose image gradient is zero elsewhere."""
     n = scene.n
     g = dict(pos=np.zeros((n, 3)), scales=np.zeros((n, 2)), quat=np.zeros((n, 4)), opacity=np.zeros(n),
              sh=np.zeros((n, 48)), cam_center=np.zeros(3), cam_quat=np.zeros(4), focal=np.zeros(1),
@@ -185,8 +217,13 @@ def gradients(scene: Scene, cam: Camera, dl_dcolor, dl_ddepth=None, dl_dnormal=N
     dld = None if dl_ddepth is None else np.ascontiguousarray(dl_ddepth, np.float64).reshape(-1)
     dln = None if dl_dnormal is None else np.ascontiguousarray(dl_dnormal, np.float64).reshape(-1, 3)
     s, c = scene.c(), cam.c()
-    lib().orc_gradients(C.byref(s), C.byref(c), tile, _p(dlc), _p(dld), _p(dln), float(lambda_dist), threads,
-                        C.byref(gs))
+    if tile_stride > 1:
+        rc = lib().orc_gradients_sampled(C.byref(s), C.byref(c), tile, tile_stride, tile_offset, _p(dlc), _p(dld),
+                                         _p(dln), float(lambda_dist), threads, C.byref(gs))
+        assert rc == 0, "bad tile sample"
+    else:
+        lib().orc_gradients(C.byref(s), C.byref(c), tile, _p(dlc), _p(dld), _p(dln), float(lambda_dist), threads,
+                            C.byref(gs))
     g["focal"] = float(g["focal"][0])
     return g
 

@@ -120,6 +120,33 @@ int orc_render(const orc_scene* s_, const orc_camera* c_, int tile, int literal,
   return 0;
 }
 
+// Forward render of a bounded sample of the image: only the pixels of tiles t
+// with t % stride == offset (row-major tile ids of this camera) are written;
+// the arrays are full-size and the other pixels are left as the caller set
+// them. last_idx receives the input index of each pixel's last contributing
+// surfel (-1 if none), which identifies the contributor independently of how
+// a tile list was binned, and count its number of contributing surfels.
+int orc_render_sampled(const orc_scene* s_, const orc_camera* c_, int tile, int stride, int offset, int nthreads,
+                       double* color, double* alpha, double* depth, double* normal, double* trans, int32_t* ncontrib,
+                       uint8_t* marginal, int32_t* last_idx, int32_t* count) {
+  Scene s = to_scene(s_);
+  Camera cam = to_cam(c_);
+  if (stride < 1 || offset < 0 || offset >= stride) return -1;
+  auto sc = prepare(s, cam, tile);
+  RenderOut o{color, alpha, depth, normal, trans, ncontrib, marginal, last_idx, count};
+  const int tiles_x = (cam.width + tile - 1) / tile, tiles_y = (cam.height + tile - 1) / tile;
+  auto lists = tile_lists(sc, cam, tile, stride, offset);
+  set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int t = offset; t < tiles_x * tiles_y; t += stride) {
+    const int tx = t % tiles_x, ty = t / tiles_x;
+    for (int y = ty * tile; y < std::min(cam.height, (ty + 1) * tile); ++y)
+      for (int x = tx * tile; x < std::min(cam.width, (tx + 1) * tile); ++x)
+        render_pixel(sc, lists[(size_t)t], cam, x, y, (size_t)y * cam.width + x, o);
+  }
+  return 0;
+}
+
 struct orc_grads {
   double* pos;
   double* scales;
@@ -136,13 +163,14 @@ struct orc_grads {
 // are ACCUMULATED into the caller's (zeroed) arrays. Per-tile partial
 // accumulators are merged in tile order, so the result is deterministic for
 // any thread count.
-int orc_gradients(const orc_scene* s_, const orc_camera* c_, int tile, const double* dl_dcolor,
-                  const double* dl_ddepth, const double* dl_dnormal, double lambda_dist, int nthreads,
-                  const orc_grads* g_) {
+static int gradients_tiles(const orc_scene* s_, const orc_camera* c_, int tile, int stride, int offset,
+                           const double* dl_dcolor, const double* dl_ddepth, const double* dl_dnormal,
+                           double lambda_dist, int nthreads, const orc_grads* g_) {
   Scene s = to_scene(s_);
   Camera cam = to_cam(c_);
+  if (stride < 1 || offset < 0 || offset >= stride) return -1;
   auto sc = prepare(s, cam, tile);
-  auto lists = tile_lists(sc, cam, tile);
+  auto lists = tile_lists(sc, cam, tile, stride, offset);
   int tiles_x = (cam.width + tile - 1) / tile, tiles_y = (cam.height + tile - 1) / tile;
   LossIn L{dl_dcolor, dl_ddepth, dl_dnormal, lambda_dist};
   int n_tiles = tiles_x * tiles_y;
@@ -150,7 +178,7 @@ int orc_gradients(const orc_scene* s_, const orc_camera* c_, int tile, const dou
   std::vector<double> tile_dfocal(n_tiles, 0.0);
   set_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 1)
-  for (int t = 0; t < n_tiles; ++t) {
+  for (int t = offset; t < n_tiles; t += stride) {
     const auto& list = lists[t];
     if (list.empty()) continue;
     // Local accumulators indexed by position in the tile list: backward_pixel
@@ -186,6 +214,21 @@ int orc_gradients(const orc_scene* s_, const orc_camera* c_, int tile, const dou
   Grads g{g_->pos, g_->scales, g_->quat, g_->opacity, g_->sh, g_->cam_center, g_->cam_quat, g_->focal, g_->dl_dr_cam};
   chain_to_params(s, cam, sc, acc, dfocal, g);
   return 0;
+}
+
+int orc_gradients(const orc_scene* s_, const orc_camera* c_, int tile, const double* dl_dcolor,
+                  const double* dl_ddepth, const double* dl_dnormal, double lambda_dist, int nthreads,
+                  const orc_grads* g_) {
+  return gradients_tiles(s_, c_, tile, 1, 0, dl_dcolor, dl_ddepth, dl_dnormal, lambda_dist, nthreads, g_);
+}
+
+// The backward restricted to the pixels of tiles t with t % stride == offset:
+// the exact gradient of a loss whose image gradient is zero on every other
+// pixel (the caller's dl_* arrays are full-size; other pixels are not read).
+int orc_gradients_sampled(const orc_scene* s_, const orc_camera* c_, int tile, int stride, int offset,
+                          const double* dl_dcolor, const double* dl_ddepth, const double* dl_dnormal,
+                          double lambda_dist, int nthreads, const orc_grads* g_) {
+  return gradients_tiles(s_, c_, tile, stride, offset, dl_dcolor, dl_ddepth, dl_dnormal, lambda_dist, nthreads, g_);
 }
 
 double orc_distortion_loss(const orc_scene* s_, const orc_camera* c_, int tile) {

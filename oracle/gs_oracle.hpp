@@ -381,15 +381,22 @@ inline Hit evaluate(const SurfelCam& sc, const V3& d, double pix_x, double pix_y
 
 // Per-tile entry lists in depth order: list[tile] = indices into the sorted
 // SurfelCam vector. Identical to filtering the sorted vector with
-// covers_pixel, which is what the reference's render loop does.
-inline std::vector<std::vector<int>> tile_lists(const std::vector<SurfelCam>& sc, const Camera& cam, int tile) {
+// covers_pixel, which is what the reference's render loop does. With
+// stride > 1 only the tiles t with t % stride == offset (row-major tile ids)
+// get their lists; the others stay empty (a bounded sample of the image).
+inline std::vector<std::vector<int>> tile_lists(const std::vector<SurfelCam>& sc, const Camera& cam, int tile,
+                                                int stride = 1, int offset = 0) {
   int tiles_x = (cam.width + tile - 1) / tile, tiles_y = (cam.height + tile - 1) / tile;
   std::vector<std::vector<int>> lists((size_t)tiles_x * tiles_y);
   for (int k = 0; k < (int)sc.size(); ++k) {
     const SurfelCam& s = sc[k];
     if (!s.visible) continue;
     for (int ty = s.y0; ty <= s.y1; ++ty)
-      for (int tx = s.x0; tx <= s.x1; ++tx) lists[(size_t)ty * tiles_x + tx].push_back(k);
+      for (int tx = s.x0; tx <= s.x1; ++tx) {
+        const int t = ty * tiles_x + tx;
+        if (stride > 1 && t % stride != offset) continue;
+        lists[(size_t)t].push_back(k);
+      }
   }
   return lists;
 }
@@ -402,6 +409,8 @@ struct RenderOut {
   double* trans;      // P final transmittance (may be null)
   int32_t* ncontrib;  // P (may be null)
   uint8_t* marginal;  // P (may be null)
+  int32_t* last_idx = nullptr;  // P: input index of the last contributing surfel, -1 if none (may be null)
+  int32_t* count = nullptr;     // P: number of contributing surfels (alpha >= 1/255) (may be null)
 };
 
 // One pixel's forward walk over its tile list (forward.rs:218-244).
@@ -412,7 +421,7 @@ inline void render_pixel(const std::vector<SurfelCam>& sc, const std::vector<int
   double T = 1.0;
   V3 col, nrm;
   double a = 0, dep = 0;
-  int nc = 0;
+  int nc = 0, last = -1, cnt = 0;
   bool marg = false;
   for (int li = 0; li < (int)list.size(); ++li) {
     const SurfelCam& s = sc[list[li]];
@@ -436,6 +445,8 @@ inline void render_pixel(const std::vector<SurfelCam>& sc, const std::vector<int
     nrm += s.normal * w;
     T *= 1.0 - alpha;
     nc = li + 1;
+    last = s.idx;
+    ++cnt;
     if (std::fabs(T - T_TERMINATE) < MARGIN_T * T_TERMINATE) marg = true;
     if (T < T_TERMINATE) break;
   }
@@ -446,6 +457,8 @@ inline void render_pixel(const std::vector<SurfelCam>& sc, const std::vector<int
   if (o.trans) o.trans[i] = T;
   if (o.ncontrib) o.ncontrib[i] = nc;
   if (o.marginal) o.marginal[i] = marg ? 1 : 0;
+  if (o.last_idx) o.last_idx[i] = last;
+  if (o.count) o.count[i] = cnt;
 }
 
 // forward.rs:174-205 — Σ_rays Σ_i Σ_j w_i w_j |t_i − t_j|.

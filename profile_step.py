@@ -1,13 +1,14 @@
 """Runs training steps of a synthetic workload for a profiler to capture.
 
-    python -m splattar_b200.profile_step --workload ring2_200k --steps 2 \
-        --shapes 128,2,64,4
+    python profile_step.py --workload ring2_200k --steps 2 --shapes 128,2,64,4
 
 Sets up the workload exactly as the benchmark does (target images rendered
 from the seed-1 scene, optimizer initialised), applies the given raster launch
 shapes (or autotunes when none are given), runs ``--warmup`` steps, then
 ``--steps`` steps of the requested form, and prints one JSON line with the
-milliseconds per step and the tile-entry count. Every step is a complete
+milliseconds per step, the tile-entry count and the raster kernels' work
+on the last step (gs_raster_work, counted after the timed steps). Every step
+is a complete
 forward + loss + backward + Adam pass; nothing is skipped. Launch order per
 chosen step: projection, depth sort, entry scan, expansion, tile sort, ranges,
 forward raster, the occlusion cut's completion pass (gate, flagged counts,
@@ -18,6 +19,10 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 
 def main(argv=None):
@@ -32,8 +37,8 @@ def main(argv=None):
 
     import torch
 
-    from .rasterizer import AdamSettings, Rasterizer, StepSettings
-    from .synthetic import workload
+    from splattar_b200.rasterizer import AdamSettings, Rasterizer, StepSettings
+    from splattar_b200.synthetic import workload
 
     wl = workload(a.workload)
     cams, n, nv, P = wl.cameras, wl.surfels.n, len(wl.cameras), wl.pixels
@@ -65,7 +70,7 @@ def main(argv=None):
     rast.check(stream.cuda_stream)
     print(json.dumps({"workload": a.workload, "form": a.form, "steps": a.steps, "shapes": shapes,
                       "ms_per_step": round(e0.elapsed_time(e1) / max(1, a.steps), 4),
-                      "tile_entries": rast.entry_count()}))
+                      "tile_entries": rast.entry_count(), "raster_work": rast.raster_work(stream.cuda_stream)}))
     rast.close()
 
 

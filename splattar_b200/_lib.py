@@ -68,7 +68,8 @@ class AdamConfig(C.Structure):
 
 
 class StepConfig(C.Structure):
-    _fields_ = [("w_l1", C.c_float), ("w_ssim", C.c_float), ("adam", AdamConfig), ("form", C.c_uint32)]
+    _fields_ = [("w_l1", C.c_float), ("w_ssim", C.c_float), ("adam", AdamConfig), ("form", C.c_uint32),
+                ("loss", C.c_uint32)]
 
 
 class Anneal(C.Structure):
@@ -95,6 +96,7 @@ def lib():
         "gs_rasterizer_destroy": [vp],
         "gs_rasterizer_upload_scene": [vp, C.POINTER(SceneInputC), vp],
         "gs_rasterizer_set_lambda_dist": [vp, f32],
+        "gs_rasterizer_set_wait_limits": [vp, u64, u64],
         "gs_rasterizer_forward": [vp, C.POINTER(Camera), u32, u32, vp],
         "gs_rasterizer_backward": [vp, u32, vp],
         "gs_rasterizer_buffer": [vp, i32, C.POINTER(vp), C.POINTER(C.c_size_t)],
@@ -115,6 +117,7 @@ def lib():
         "gs_densify_prune": [vp, C.POINTER(DensifyConfig), u32, C.POINTER(u32), vp],
         "gs_autotune": [vp, C.POINTER(Camera), u32, u32, vp, C.POINTER(u32)],
         "gs_set_launch_shapes": [vp, C.POINTER(u32)],
+        "gs_raster_work": [vp, C.POINTER(u64), vp],
         "gs_autotune_tiles": [vp, C.POINTER(Camera), u32, u32, vp, C.POINTER(u32), C.POINTER(f32)],
         "gs_set_tile_size": [vp, u32],
         "gs_tile_size": [vp],
@@ -170,10 +173,10 @@ def exported_symbols() -> list[str]:
     lib()
     return ["gs_version"] + [
         "gs_rasterizer_create", "gs_rasterizer_destroy", "gs_rasterizer_upload_scene", "gs_rasterizer_set_lambda_dist",
-        "gs_rasterizer_forward", "gs_rasterizer_backward", "gs_rasterizer_buffer", "gs_rasterizer_view_offset",
+        "gs_rasterizer_set_wait_limits", "gs_rasterizer_forward", "gs_rasterizer_backward", "gs_rasterizer_buffer", "gs_rasterizer_view_offset",
         "gs_rasterizer_read", "gs_rasterizer_write", "gs_rasterizer_read_async", "gs_rasterizer_write_async",
         "gs_rasterizer_check", "gs_last_error", "gs_loss_l1_ssim", "gs_optimizer_init", "gs_optimizer_step",
-        "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_autotune_tiles", "gs_set_tile_size", "gs_tile_size", "gs_set_launch_shapes", "gs_binner_create",
+        "gs_adam_flat", "gs_train_step", "gs_train_step_profiled", "gs_densify_prune", "gs_autotune", "gs_autotune_tiles", "gs_set_tile_size", "gs_tile_size", "gs_set_launch_shapes", "gs_raster_work", "gs_binner_create",
         "gs_binner_destroy", "gs_binner_encode", "gs_binner_buffer", "gs_radix_sort_pairs", "gs_radix_sort_pairs_noalloc",
         "gs_exclusive_scan_u32",
         "gs_camera_rotation", "gs_shutdown", "gs_loss_normal", "gs_camera_step_grad", "gs_camera_adam6",

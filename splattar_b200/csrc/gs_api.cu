@@ -148,6 +148,9 @@ struct gs_rasterizer {
   float* grad_opacity = nullptr;
   float* grad_sh = nullptr;
   float* grad_cam = nullptr;
+  // deterministic mode: per (unit, view) camera partials of the projection
+  // backward, summed in unit order
+  float* cam_part = nullptr;
 
   // optimizer
   float* raw[5] = {};
@@ -155,6 +158,9 @@ struct gs_rasterizer {
   float* mom2[5] = {};
   uint32_t t = 0;
   bool optim_ready = false;
+  // limits (SM cycles) of the fused projection backward + Adam kernel's two
+  // bounded waits on its optimizer-row copies (gs_rasterizer_set_wait_limits)
+  long long wait_cycles[2] = {2000000000ll, 2000000000ll};
   float* accum_norm = nullptr;
   uint32_t accum_steps = 0;
   float* dyn_dev = nullptr;
@@ -179,6 +185,8 @@ struct gs_rasterizer {
   const ViewInfo* last_views_dev = nullptr;
   const ViewInfo* last_views_host = nullptr;
   bool have_forward = false;
+  int last_prec = 0;  // storage precision of the last forward's records
+  unsigned long long* work_counts = nullptr;  // gs_raster_work's device counters
 
   void* scan_scratch = nullptr;
   void* sort_scratch = nullptr;
@@ -296,6 +304,8 @@ gs_status set_views(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32
     const gs_camera& c = cams[v];
     if (c.width == 0 || c.height == 0 || !(c.focal > 0.f) || c.sh_degree > 3)
       return fail(r, GS_ERR_INVALID_ARG, "bad camera (size, focal or sh_degree)");
+    if (r->cfg.precision != GS_PREC_F32 && (c.width > (uint32_t)REC_MAX_SIDE_H || c.height > (uint32_t)REC_MAX_SIDE_H))
+      return fail(r, GS_ERR_INVALID_ARG, "16-bit storage supports images up to 32766 pixels per side");
     ViewInfo vi = make_view(c, r->tile);
     vi.pix_base = pix;
     vi.tile_base = tiles;
@@ -477,6 +487,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
     mark(prof, 5, st);
   }
   r->last_nv = nv; r->last_n = n; r->last_tiles = tiles; r->last_views_dev = vdev; r->last_views_host = vhost;
+  r->last_prec = prec;
   r->have_forward = true;
   return GS_OK;
 }
@@ -532,6 +543,7 @@ ProjectBwdArgs pbwd_args(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, ui
   b.counts = r->counts;
   b.grad_pos = r->grad_pos; b.grad_scales = r->grad_scales; b.grad_quat = r->grad_quat;
   b.grad_opacity = r->grad_opacity; b.grad_sh = r->grad_sh; b.grad_cam = r->grad_cam;
+  b.cam_partials = r->det ? r->cam_part : nullptr;
   return b;
 }
 
@@ -554,6 +566,8 @@ gs_status run_project_bwd(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, u
     b.view = (int)v;
     b.grad_cam = grad_cam_base;
     TRY_LAUNCH(r, launch_project_bwd(b, prec, aux, st));
+    if (b.cam_partials)  // deterministic mode: this view's camera gradient, summed in warp order
+      TRY_LAUNCH(r, launch_cam_reduce(b.cam_partials, cam_partial_units(n, 0), 1, grad_cam_base + 16 * v, st));
   }
   return GS_OK;
 }
@@ -681,8 +695,10 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
     TRY_LAUNCH(r, launch_tile_order(r->ranges, r->tile_walk, (uint32_t)tiles, r->tile_order, side));
   TRY_CUDA(r, cudaEventRecord(r->ev_side, side));
   TRY_CUDA(r, cudaMemsetAsync(r->loss_sums, 0, sizeof(double) * 2 * nv, st));
-  s = run_loss(r, vdev, r->views_batched.data(), nv, cfg->w_l1, cfg->w_ssim, r->loss_sums, st);
-  if (s) return s;
+  if (cfg->loss == GS_LOSS_L1_SSIM) {
+    s = run_loss(r, vdev, r->views_batched.data(), nv, cfg->w_l1, cfg->w_ssim, r->loss_sums, st);
+    if (s) return s;
+  }
   mark(prof, 6, st);
   TRY_CUDA(r, cudaStreamWaitEvent(st, r->ev_side, 0));
   s = run_backward_raster(r, vdev, nv, tiles, n, prec, false, true, st, true);
@@ -698,7 +714,11 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   o.sh_half_is_bf16 = prec == 2;
   o.accum_grad_norm = r->accum_norm;
   o.error_word = r->words + 1;
+  o.wait_cycles[0] = r->wait_cycles[0];
+  o.wait_cycles[1] = r->wait_cycles[1];
   TRY_LAUNCH(r, launch_project_bwd_adam(b, o, prec, false, st));
+  if (b.cam_partials)  // deterministic mode: camera gradients summed in block order
+    TRY_LAUNCH(r, launch_cam_reduce(b.cam_partials, cam_partial_units(n, (int)nv), (int)nv, r->grad_cam, st));
   mark(prof, 8, st);
   return GS_OK;
 }
@@ -715,8 +735,10 @@ gs_status plain_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_co
     const int tiles = vi.tiles_x * vi.tiles_y;
     s = run_forward(r, vd, &r->views_single[v], 1, tiles, n, 0, false, false, st, prof);
     if (s) return s;
-    s = run_loss(r, vd, &r->views_single[v], 1, cfg->w_l1, cfg->w_ssim, r->loss_sums + 2 * v, st);
-    if (s) return s;
+    if (cfg->loss == GS_LOSS_L1_SSIM) {
+      s = run_loss(r, vd, &r->views_single[v], 1, cfg->w_l1, cfg->w_ssim, r->loss_sums + 2 * v, st);
+      if (s) return s;
+    }
     mark(prof, 6, st);
     s = run_backward_raster(r, vd, 1, tiles, n, 0, false, false, st);
     if (s) return s;
@@ -834,6 +856,9 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
     ALLOC(r->exp_item, E);
     ALLOC(r->partials, E * GG_STRIDE);
     ALLOC(r->entry_offset, I);
+    uint64_t units = cam_partial_units(c.capacity, 0);
+    for (uint32_t v = 1; v <= c.max_views; ++v) units = std::max<uint64_t>(units, cam_partial_units(c.capacity, (int)v) * v);
+    ALLOC(r->cam_part, units * 16);
   }
   ALLOC(r->ranges, r->max_tiles);
   ALLOC(r->tile_order, r->max_tiles);
@@ -861,6 +886,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   }
   ALLOC(r->entry_total, 1);
   ALLOC(r->words, 8);
+  ALLOC(r->work_counts, 4);
   ALLOC(r->out_color, P); ALLOC(r->out_aux, P); ALLOC(r->out_normal, P); ALLOC(r->dl_dcolor, P);
   ALLOC(r->dl_dnormal, P); ALLOC(r->target, P); ALLOC(r->out_nc, P);
   ALLOC(r->coef, P * 9);
@@ -910,13 +936,13 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->entry_offset, r->ent_pairs[0], r->ent_pairs[1], r->exp_item,
                   r->partials, r->ranges, r->entry_total, r->words, r->out_color, r->out_aux, r->out_normal,
                   r->dl_dcolor, r->dl_dnormal, r->target, r->out_nc, r->coef, r->loss_sums, r->grad_geom,
-                  r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam,
+                  r->grad_pos, r->grad_scales, r->grad_quat, r->grad_opacity, r->grad_sh, r->grad_cam, r->cam_part,
                   r->accum_norm, r->dyn_dev, r->dens_flags, r->dens_slots, r->dens_tmp, r->views_dev,
                   r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask, r->tile_order, r->tile_walk,
                   r->normal_loss_sums,
                   r->mask_words,
                   r->tile_cut, r->inc_list, r->inc_skip, r->inc_src, r->inc_flag, r->item_key, r->counts2, r->cutw, r->entry_total2,
-                  r->scan_scratch, r->sort_scratch};
+                  r->scan_scratch, r->sort_scratch, r->work_counts};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 5; ++k) {
@@ -959,6 +985,17 @@ gs_status gs_rasterizer_upload_scene(gs_rasterizer* r, const gs_scene_input* s, 
 gs_status gs_rasterizer_set_lambda_dist(gs_rasterizer* r, float lambda_dist) {
   if (!r) return GS_ERR_INVALID_ARG;
   r->lambda_dist = lambda_dist;
+  return GS_OK;
+}
+
+gs_status gs_rasterizer_set_wait_limits(gs_rasterizer* r, uint64_t copy_wait_cycles, uint64_t drain_wait_cycles) {
+  if (!r) return GS_ERR_INVALID_ARG;
+  // The drain wait keeps an expired block from exiting while its copies are
+  // in flight; it must stay long enough for them to land.
+  if (drain_wait_cycles < 100000000ull || drain_wait_cycles > (1ull << 62) || copy_wait_cycles > (1ull << 62))
+    return fail(r, GS_ERR_INVALID_ARG, "drain wait below 1e8 cycles, or a limit beyond 2^62");
+  r->wait_cycles[0] = (long long)copy_wait_cycles;
+  r->wait_cycles[1] = (long long)drain_wait_cycles;
   return GS_OK;
 }
 
@@ -1281,7 +1318,7 @@ gs_status gs_adam_flat(float* raw, const float* grad, float* m, float* v, float*
 
 gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32_t n, const gs_step_config* cfg,
                         void* stream) {
-  if (!r || !cfg) return GS_ERR_INVALID_ARG;
+  if (!r || !cfg || cfg->loss > GS_LOSS_GIVEN) return GS_ERR_INVALID_ARG;
   if (!r->optim_ready) return fail(r, GS_ERR_STATE, "gs_optimizer_init first");
   gs_status s = set_views(r, cams, nv, n);
   if (s) return s;
@@ -1308,6 +1345,9 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, ui
   std::memcpy(&wb[0], &cfg->w_l1, 4);
   std::memcpy(&wb[1], &cfg->w_ssim, 4);
   key.push_back(wb[0]); key.push_back(wb[1]);
+  key.push_back(cfg->loss);
+  key.push_back((uint64_t)r->wait_cycles[0]);
+  key.push_back((uint64_t)r->wait_cycles[1]);
   for (const ViewInfo& v : r->views_batched) key.push_back(((uint64_t)v.width << 32) | (uint64_t)v.height);
   if (!r->graph || key != r->graph_key) {
     if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
@@ -1333,7 +1373,7 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, ui
 
 gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, uint32_t n,
                                  const gs_step_config* cfg, void* stream, float* stage_ms, uint32_t* n_stages) {
-  if (!r || !cfg || !stage_ms || !n_stages) return GS_ERR_INVALID_ARG;
+  if (!r || !cfg || !stage_ms || !n_stages || cfg->loss > GS_LOSS_GIVEN) return GS_ERR_INVALID_ARG;
   if (!r->optim_ready) return fail(r, GS_ERR_STATE, "gs_optimizer_init first");
   gs_status s = set_views(r, cams, nv, n);
   if (s) return s;
@@ -1365,6 +1405,28 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
     if (stg >= 0 && stg < N_STAGES) stage_ms[stg] += ms;
   }
   *n_stages = N_STAGES;
+  return GS_OK;
+}
+
+gs_status gs_raster_work(gs_rasterizer* r, uint64_t out[4], void* stream) {
+  if (!r || !out) return GS_ERR_INVALID_ARG;
+  if (!r->have_forward) return fail(r, GS_ERR_STATE, "gs_raster_work needs a forward");
+  cudaStream_t st = S(stream);
+  RasterArgs ra{};
+  ra.views = r->last_views_dev; ra.n_views = (int)r->last_nv; ra.total_tiles = r->last_tiles;
+  ra.ranges = r->ranges; ra.sorted_pairs = r->ent_pairs[r->ent_in1];
+  ra.exp_item = r->det ? r->exp_item : nullptr;
+  ra.records = r->records;
+  ra.out_nc = r->out_nc; ra.out_aux = r->out_aux;
+  ra.gmask = r->gmask_valid ? r->gmask : nullptr;
+  TRY_CUDA(r, cudaMemsetAsync(r->work_counts, 0, 4 * sizeof(unsigned long long), st));
+  TRY_LAUNCH(r, launch_raster_work(ra, r->tile, r->last_prec, r->work_counts, st));
+  unsigned long long h[4] = {0, 0, 0, 0};
+  TRY_CUDA(r, cudaMemcpyAsync(h, r->work_counts, sizeof(h), cudaMemcpyDeviceToHost, st));
+  TRY_CUDA(r, cudaStreamSynchronize(st));
+  for (int k = 0; k < 4; ++k) out[k] = h[k];
+  // The stored-state backward evaluates only the recorded contributors.
+  if (r->mask_valid) out[2] = out[1];
   return GS_OK;
 }
 

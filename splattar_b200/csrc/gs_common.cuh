@@ -50,11 +50,19 @@ struct ViewInfo {
 //   r0 = (M, tn)  r1 = (Bu, px)  r2 = (Bv, py)
 //   r3 = (colour rgb, opacity)  r4 = (normal xyz, centre depth)
 //   bb = pixel box (x0, x1, y0, y1) outside which α < 1/255 for certain
-// FP32 record: 6 float4 = 96 B. Mixed-precision record: geometry and box stay
-// FP32 (the geometry feeds a ratio of nearly cancelling dot products),
-// colour/opacity/normal/depth are 16-bit: 5 float4 = 80 B.
+// FP32 record: 6 float4 = 96 B. Mixed-precision record (80 B, 5 float4):
+// geometry r0..r2 and colour/opacity r3 stay FP32 (the geometry feeds a ratio
+// of nearly cancelling dot products; colour and opacity rounded to 16 bits
+// dominate the gradient error, about 6e-4 and 2e-4 relative at 200k surfels
+// x 720p), normal and depth are 16-bit, and the α-box is stored as int16
+// pixel bounds: the smallest and largest pixel index whose centre lies inside
+// the float box, per axis. Pixel x's centre x + 0.5 lies in [b.x, b.y] exactly
+// when lo <= x <= hi, so the loader returns (lo + 0.5, hi + 0.5, ...) and every
+// box test selects the same pixels as with the float box. Images up to 32766
+// pixels per side.
 constexpr int REC_F4_F32 = 6;
 constexpr int REC_F4_H = 5;
+constexpr int REC_MAX_SIDE_H = 32766;
 
 template <typename H> __device__ __forceinline__ float h2f(H x);
 template <> __device__ __forceinline__ float h2f<__half>(__half x) { return __half2float(x); }
@@ -62,6 +70,25 @@ template <> __device__ __forceinline__ float h2f<__nv_bfloat16>(__nv_bfloat16 x)
 template <typename H> __device__ __forceinline__ H f2h(float x);
 template <> __device__ __forceinline__ __half f2h<__half>(float x) { return __float2half_rn(x); }
 template <> __device__ __forceinline__ __nv_bfloat16 f2h<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+
+// Smallest integer k with k + 0.5 >= z, and largest k with k + 0.5 <= z,
+// clamped to [-5, 32767] (beyond every pixel of an image of at most 32766
+// pixels per side). The float estimate is corrected with the exact
+// comparisons the raster's per-pixel test makes.
+__device__ __forceinline__ int pix_lo(float z) {
+  const float zc = fminf(fmaxf(z, -4.0f), 32767.0f);
+  int k = (int)ceilf(zc - 0.5f);
+  if ((float)k + 0.5f < zc) ++k;
+  if ((float)(k - 1) + 0.5f >= zc) --k;
+  return k;
+}
+__device__ __forceinline__ int pix_hi(float z) {
+  const float zc = fminf(fmaxf(z, -4.0f), 32767.0f);
+  int k = (int)floorf(zc - 0.5f);
+  if ((float)k + 0.5f > zc) --k;
+  if ((float)(k + 1) + 0.5f <= zc) ++k;
+  return k;
+}
 
 template <int PREC>
 __device__ __forceinline__ const float4* record_ptr(const void* recs, uint32_t idx) {
@@ -71,7 +98,15 @@ __device__ __forceinline__ const float4* record_ptr(const void* recs, uint32_t i
 // The α box of record `idx` (read first, so culled entries cost one load).
 template <int PREC>
 __device__ __forceinline__ float4 load_record_box(const void* recs, uint32_t idx) {
-  return __ldg(record_ptr<PREC>(recs, idx) + (PREC == 0 ? 5 : 4));
+  if constexpr (PREC == 0) {
+    return __ldg(record_ptr<PREC>(recs, idx) + 5);
+  } else {
+    const int4 raw = __ldg(reinterpret_cast<const int4*>(record_ptr<PREC>(recs, idx) + 4));
+    // int16 pairs (lo, hi) of x in raw.z, of y in raw.w (little endian)
+    const int x0 = (int)(short)(raw.z & 0xffff), x1 = raw.z >> 16;
+    const int y0 = (int)(short)(raw.w & 0xffff), y1 = raw.w >> 16;
+    return make_float4((float)x0 + 0.5f, (float)x1 + 0.5f, (float)y0 + 0.5f, (float)y1 + 0.5f);
+  }
 }
 
 // Loads the geometry and appearance of record `idx` as five float4
@@ -80,33 +115,41 @@ template <int PREC>
 __device__ __forceinline__ void load_record(const void* recs, uint32_t idx, float4& r0, float4& r1, float4& r2,
                                             float4& r3, float4& r4) {
   const float4* p = record_ptr<PREC>(recs, idx);
+  r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2); r3 = __ldg(p + 3);
   if constexpr (PREC == 0) {
-    r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2); r3 = __ldg(p + 3); r4 = __ldg(p + 4);
+    r4 = __ldg(p + 4);
   } else {
     using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
-    r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2);
-    float4 raw = __ldg(p + 3);
+    const float4 raw = __ldg(p + 4);
     const H* h = reinterpret_cast<const H*>(&raw);
-    r3 = make_float4(h2f<H>(h[0]), h2f<H>(h[1]), h2f<H>(h[2]), h2f<H>(h[3]));
-    r4 = make_float4(h2f<H>(h[4]), h2f<H>(h[5]), h2f<H>(h[6]), h2f<H>(h[7]));
+    r4 = make_float4(h2f<H>(h[0]), h2f<H>(h[1]), h2f<H>(h[2]), h2f<H>(h[3]));
   }
+}
+
+// The geometry and colour/opacity alone (r0..r3): what the colour-only
+// kernels read.
+template <int PREC>
+__device__ __forceinline__ void load_record4(const void* recs, uint32_t idx, float4& r0, float4& r1, float4& r2,
+                                             float4& r3) {
+  const float4* p = record_ptr<PREC>(recs, idx);
+  r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2); r3 = __ldg(p + 3);
 }
 
 template <int PREC>
 __device__ __forceinline__ void store_record(void* recs, uint32_t idx, float4 r0, float4 r1, float4 r2, float4 r3,
                                              float4 r4, float4 box) {
   float4* p = reinterpret_cast<float4*>(recs) + (size_t)idx * (PREC == 0 ? REC_F4_F32 : REC_F4_H);
+  p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3;
   if constexpr (PREC == 0) {
-    p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = box;
+    p[4] = r4; p[5] = box;
   } else {
     using H = typename std::conditional<PREC == 1, __half, __nv_bfloat16>::type;
-    p[0] = r0; p[1] = r1; p[2] = r2;
-    float4 raw;
+    int4 raw;
     H* h = reinterpret_cast<H*>(&raw);
-    h[0] = f2h<H>(r3.x); h[1] = f2h<H>(r3.y); h[2] = f2h<H>(r3.z); h[3] = f2h<H>(r3.w);
-    h[4] = f2h<H>(r4.x); h[5] = f2h<H>(r4.y); h[6] = f2h<H>(r4.z); h[7] = f2h<H>(r4.w);
-    p[3] = raw;
-    p[4] = box;
+    h[0] = f2h<H>(r4.x); h[1] = f2h<H>(r4.y); h[2] = f2h<H>(r4.z); h[3] = f2h<H>(r4.w);
+    raw.z = (int)(((uint32_t)pix_hi(box.y) << 16) | ((uint32_t)pix_lo(box.x) & 0xffffu));
+    raw.w = (int)(((uint32_t)pix_hi(box.w) << 16) | ((uint32_t)pix_lo(box.z) & 0xffffu));
+    reinterpret_cast<int4*>(p)[4] = raw;
   }
 }
 

@@ -55,6 +55,10 @@ struct ProjectBwdArgs {
   float* grad_opacity;
   float* grad_sh;
   float* grad_cam;        // 16 per view, or null
+  // Deterministic mode: per (unit, view) camera partial sums, 16 floats each
+  // (units: warps of the plain kernel, blocks of the fused one), summed in
+  // unit order by launch_cam_reduce; null: added into grad_cam by atomics.
+  float* cam_partials;
 };
 
 struct AdamClass {
@@ -74,6 +78,11 @@ struct AdamFusedArgs {
   int sh_half_is_bf16;
   float* accum_grad_norm; // per-surfel running sum of |dL/dpos| (densify), or null
   uint32_t* error_word;   // sticky device error word (bounded-wait expiry)
+  // Limits in SM cycles of the two bounded waits on the optimizer-row copies:
+  // [0] before the Adam update (expiry sets ERR_TIMEOUT and skips the block's
+  // update; 0 gives up at once), [1] the drain wait that lets the copies land
+  // before an expired block exits.
+  long long wait_cycles[2];
 };
 
 struct RasterArgs {
@@ -147,8 +156,19 @@ int launch_project(const ProjectArgs& a, int prec, uint32_t n_views, cudaStream_
 int launch_project_bwd(const ProjectBwdArgs& a, int prec, bool aux, cudaStream_t st);
 int prepare_project_kernels();
 int launch_project_bwd_adam(const ProjectBwdArgs& a, const AdamFusedArgs& opt, int prec, bool aux, cudaStream_t st);
+// Units of camera partials a projection-backward launch writes per view
+// (deterministic mode): warps of the plain kernel (n_views 0) or blocks of the
+// fused kernel over n_views views.
+uint64_t cam_partial_units(uint32_t n, int n_views);
+// grad_cam[16 v + c] = sum over units u, in unit order, of
+// partials[(u * n_views + v) * 16 + c], c < 13 (one block per view).
+int launch_cam_reduce(const float* partials, uint64_t units, int n_views, float* grad_cam, cudaStream_t st);
 int launch_raster_fwd(const RasterArgs& a, int tile, int prec, int batch, int ppt, bool det, bool persistent,
                       bool color, int grid, cudaStream_t st);
+// Counts the raster kernels' work on the last forward (k_raster_work): adds
+// {forward hit evaluations, contributing pairs, backward hit evaluations,
+// pixels} into out4 (zeroed by the caller).
+int launch_raster_work(const RasterArgs& a, int tile, int prec, unsigned long long* out4, cudaStream_t st);
 int launch_raster_bwd(const RasterArgs& a, int tile, int prec, bool aux, int ppt, int batch, bool det,
                       bool persistent, int grid, cudaStream_t st);
 

@@ -213,6 +213,19 @@ __device__ __forceinline__ void flush_cam(float* grad_cam_view, const float cam[
   }
 }
 
+// Deterministic mode: the warp's camera gradient summed in a fixed order
+// (the transpose reduction) and stored, 16 floats (13 used), at dst. All 32
+// lanes must call.
+__device__ __forceinline__ void store_cam_warp(float* dst, const float cam[13]) {
+  float v[16];
+#pragma unroll
+  for (int k = 0; k < 13; ++k) v[k] = cam[k];
+  v[13] = v[14] = v[15] = 0.0f;
+  const float r = warp_reduce16(v);
+  const int lane = threadIdx.x & 31;
+  if (!(lane & 1)) dst[reduce16_component(lane)] = r;
+}
+
 // Plain form: one view per launch, gradients ADDED into the grad buffers.
 template <int PREC, bool AUX>
 __global__ void __launch_bounds__(256) k_project_bwd(ProjectBwdArgs a) {
@@ -231,7 +244,11 @@ __global__ void __launch_bounds__(256) k_project_bwd(ProjectBwdArgs a) {
       any = true;
     }
   }
-  if (a.grad_cam && __any_sync(0xffffffffu, any)) flush_cam(a.grad_cam + 16 * v, o.cam);
+  if (a.cam_partials) {
+    store_cam_warp(a.cam_partials + ((size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 16, o.cam);
+  } else if (a.grad_cam && __any_sync(0xffffffffu, any)) {
+    flush_cam(a.grad_cam + 16 * v, o.cam);
+  }
   if (!any) return;
   float4* gp = a.grad_pos + i;
   float4 t = *gp;
@@ -344,8 +361,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Waits for phase 0 of the barrier for at most ~max_cycles SM cycles.
+// Waits for phase 0 of the barrier for at most ~max_cycles SM cycles (a limit
+// of 0 or less gives up at once, without looking).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, long long max_cycles) {
+  if (max_cycles <= 0) return false;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, 0)) {
     if (clock64() - t0 > max_cycles) return false;
@@ -373,6 +392,28 @@ __device__ __forceinline__ void flush_cam_group(float* grad_cam_view, const floa
     red_add_v4(grad_cam_view + 4, v[4], v[5], v[6], v[7]);
     red_add_v4(grad_cam_view + 8, v[8], v[9], v[10], v[11]);
     atomicAdd(grad_cam_view + 12, v[12]);
+  }
+}
+
+// Deterministic mode: the camera gradient of one view summed over groups of
+// `group` lanes in a fixed order and stored (16 floats, 13 used) at dst by
+// the group's first lane when `write`. All 32 lanes must call.
+__device__ __forceinline__ void store_cam_group(float* dst, const float cam[13], int group, bool write) {
+  if (group >= 32) {
+    if (__any_sync(0xffffffffu, write)) store_cam_warp(dst, cam);
+    return;
+  }
+  float v[13];
+#pragma unroll
+  for (int k = 0; k < 13; ++k) v[k] = cam[k];
+  for (int o = group >> 1; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < 13; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  }
+  if (write && (threadIdx.x & (group - 1)) == 0) {
+#pragma unroll
+    for (int k = 0; k < 13; ++k) dst[k] = v[k];
+    dst[13] = dst[14] = dst[15] = 0.0f;
   }
 }
 
@@ -491,14 +532,23 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
     }
     // Every lane of a group holds the same view (S is a power of two, V·S a
     // multiple of S); lanes past the last view hold zeros and write nothing.
-    if (a.grad_cam && __any_sync(0xffffffffu, any))
+    if (a.cam_partials)
+      store_cam_group(a.cam_partials + ((size_t)blockIdx.x * V + (v < V ? v : V - 1)) * 16, o.cam, S < 32 ? S : 32,
+                      v < V);
+    else if (a.grad_cam && __any_sync(0xffffffffu, any))
       flush_cam_group(a.grad_cam + 16 * (v < V ? v : V - 1), o.cam, S < 32 ? S : 32, v < V);
   }
   __syncthreads();
   // ---- phase 2
-  if (!mbar_wait_bounded(&s_bar, 2000000000ll)) {
+  if (!mbar_wait_bounded(&s_bar, opt.wait_cycles[0])) {
+    // The block's optimizer rows are not (known to be) in shared memory: flag
+    // the expiry, skip this block's update, and give the copies in flight the
+    // drain limit to land before the block exits. Should the drain wait expire
+    // too, the block exits with copies in flight, which may then land in
+    // shared memory a later block of the SM uses: the error word reports the
+    // launch as failed and its results must be discarded.
     if (tid == 0 && opt.error_word) atomicOr(opt.error_word, ERR_TIMEOUT);
-    mbar_wait_bounded(&s_bar, 2000000000ll);  // let copies in flight land before the block exits
+    mbar_wait_bounded(&s_bar, opt.wait_cycles[1]);
     return;
   }
   const float b1 = opt.beta1, b2 = opt.beta2, eps = opt.eps;
@@ -587,6 +637,39 @@ int launch_project_bwd(const ProjectBwdArgs& a, int prec, bool aux, cudaStream_t
   else if (prec == 1) { if (aux) GS_PB(1, true); else GS_PB(1, false); }
   else { if (aux) GS_PB(2, true); else GS_PB(2, false); }
 #undef GS_PB
+  return (int)cudaGetLastError();
+}
+
+namespace {
+
+// One block per view: 16 unit-lanes × 16 components, each unit-lane summing
+// a fixed stride of units in order, then the 16 lanes in order.
+__global__ void __launch_bounds__(256) k_cam_reduce(const float* part, uint64_t units, int V, float* grad_cam) {
+  __shared__ float s_sum[16][17];
+  const int v = blockIdx.x, c = threadIdx.x & 15, ul = threadIdx.x >> 4;
+  float acc = 0.0f;
+  for (uint64_t u = (uint64_t)ul; u < units; u += 16) acc += __ldg(part + (u * (uint64_t)V + (uint64_t)v) * 16 + c);
+  s_sum[ul][c] = acc;
+  __syncthreads();
+  if (threadIdx.x < 13) {
+    float t = 0.0f;
+#pragma unroll
+    for (int l = 0; l < 16; ++l) t += s_sum[l][threadIdx.x];
+    grad_cam[16 * v + threadIdx.x] = t;
+  }
+}
+
+}  // namespace
+
+uint64_t cam_partial_units(uint32_t n, int n_views) {
+  if (n_views <= 0) return (uint64_t)((n + 255) / 256) * 8;  // plain kernel: 8 warps per 256-thread block
+  const uint32_t S = (uint32_t)pba_surfels(n_views);
+  return (uint64_t)((n + S - 1) / S);
+}
+
+int launch_cam_reduce(const float* partials, uint64_t units, int n_views, float* grad_cam, cudaStream_t st) {
+  if (n_views <= 0) return 0;
+  k_cam_reduce<<<n_views, 256, 0, st>>>(partials, units, n_views, grad_cam);
   return (int)cudaGetLastError();
 }
 

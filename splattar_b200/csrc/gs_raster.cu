@@ -64,6 +64,21 @@ int launch_raster_fwd(const RasterArgs& a, int tile, int prec, int batch, int pp
   return (int)cudaErrorInvalidValue;
 }
 
+int launch_raster_work(const RasterArgs& a, int tile, int prec, unsigned long long* out4, cudaStream_t st) {
+  if (a.total_tiles == 0) return 0;
+  auto go = [&](auto kernel, int threads) { kernel<<<a.total_tiles, threads, 0, st>>>(a, out4); };
+  if (tile == 8) {
+    if (prec == 0) go(k_raster_work<8, 0>, 64); else if (prec == 1) go(k_raster_work<8, 1>, 64); else go(k_raster_work<8, 2>, 64);
+  } else if (tile == 16) {
+    if (prec == 0) go(k_raster_work<16, 0>, 256); else if (prec == 1) go(k_raster_work<16, 1>, 256); else go(k_raster_work<16, 2>, 256);
+  } else if (tile == 32) {
+    if (prec == 0) go(k_raster_work<32, 0>, 256); else if (prec == 1) go(k_raster_work<32, 1>, 256); else go(k_raster_work<32, 2>, 256);
+  } else {
+    return (int)cudaErrorInvalidValue;
+  }
+  return (int)cudaGetLastError();
+}
+
 int launch_raster_bwd(const RasterArgs& a, int tile, int prec, bool aux, int ppt, int batch, bool det,
                       bool persistent, int grid, cudaStream_t st) {
   if (tile == 8) return launch_raster_bwd_t<8>(a, prec, aux, ppt, batch, det, persistent, grid, st);

@@ -366,7 +366,8 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
         const int slot = kept + compact_slot<NW>(keep, s_wcount[rd & 1], kr);
         if (keep) {
           float4 r0, r1, r2, r3, r4;
-          load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
+          if (COLOR) load_record4<PREC>(a.records, item, r0, r1, r2, r3);
+          else load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (!COLOR) s_r4[slot] = r4;
           s_bb[slot] = bb;
@@ -722,7 +723,8 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
         const int slot = kept + compact_slot<NW>(keep, s_wcount[rd & 1], kr);
         if (keep) {
           float4 r0, r1, r2, r3, r4;
-          load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
+          if (AUX) load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
+          else load_record4<PREC>(a.records, item, r0, r1, r2, r3);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (AUX) s_r4[slot] = r4;
           s_msk[slot] = box_masks<TS, PPT>(bb, g);
@@ -918,6 +920,67 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
     if (!PERSIST) return;
     __syncthreads();
   }
+}
+
+// Work of the raster kernels on the last forward, counted by replaying each
+// pixel's walk (outside any timed region): one thread per pixel, TS·TS/NPT
+// threads per tile. Per pixel, the forward evaluates the hit of every list
+// entry whose α-box holds the pixel until the pixel terminates (its last
+// contributor when T < 1e-4 at the end, else the whole list); a pair
+// contributes when α ≥ 1/255 (the same eval_hit, so the same decisions as
+// the forward); the backward evaluates the entries before the pixel's last
+// contributor whose box holds it and, with the row-group summary, whose
+// summary byte has the pixel's group. out: {forward evaluations,
+// contributing pairs, backward evaluations, pixels}.
+template <int TS, int PREC>
+__global__ void __launch_bounds__(256) k_raster_work(RasterArgs a, unsigned long long* out) {
+  constexpr int NP = TS * TS, NT = NP < 256 ? NP : 256;
+  __shared__ unsigned long long s_cnt[4];
+  if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0ull;
+  __syncthreads();
+  const int tile = blockIdx.x;
+  int v = 0;
+  while (v + 1 < a.n_views && tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
+  const ViewInfo* V = a.views + v;
+  const int tiles_x = __ldg(&V->tiles_x), W = __ldg(&V->width), H = __ldg(&V->height);
+  const int lt = tile - __ldg(&V->tile_base);
+  const int x0 = (lt % tiles_x) * TS, y0 = (lt / tiles_x) * TS;
+  const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
+  const uint2 range = __ldg(&a.ranges[tile]);
+  const uint32_t len = range.y > range.x ? range.y - range.x : 0u;
+  unsigned long long fe = 0, co = 0, be = 0, px = 0;
+  for (int q = threadIdx.x; q < NP; q += NT) {
+    const int x = x0 + q % TS, y = y0 + q / TS;
+    if (x >= W || y >= H) continue;
+    ++px;
+    const long long pix = __ldg(&V->pix_base) + (long long)y * W + x;
+    const uint32_t nc = a.out_nc[pix];
+    const float Tf = a.out_aux[pix].x;
+    const uint32_t stop = Tf < T_TERMINATE ? min(nc, len) : len;
+    const float pxc = (float)x + 0.5f, pyc = (float)y + 0.5f;
+    const float sx = -((pxc - cx) / f), sy = (pyc - cy) / f;
+    const uint32_t gbit = 1u << ((q / TS) >> 2);
+    for (uint32_t j = 0; j < stop; ++j) {
+      uint32_t item = __ldg(&a.sorted_pairs[range.x + j].y);
+      if (a.exp_item != nullptr) item = __ldg(&a.exp_item[item]);
+      const float4 bb = load_record_box<PREC>(a.records, item);
+      if (!(pxc >= bb.x && pxc <= bb.y && pyc >= bb.z && pyc <= bb.w)) continue;
+      ++fe;
+      float4 r0, r1, r2, r3;
+      load_record4<PREC>(a.records, item, r0, r1, r2, r3);
+      const ColPart cp = col_part(r0, r1, r2, sx, pxc);
+      const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, sy, pyc);
+      const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
+      if (!(alpha < ALPHA_SKIP)) ++co;
+      if (j < nc && (TS != 16 || a.gmask == nullptr || (__ldg(a.gmask + range.x + j) & gbit))) ++be;
+    }
+  }
+  atomicAdd(&s_cnt[0], fe);
+  atomicAdd(&s_cnt[1], co);
+  atomicAdd(&s_cnt[2], be);
+  atomicAdd(&s_cnt[3], px);
+  __syncthreads();
+  if (threadIdx.x < 4) atomicAdd(out + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
 }  // namespace

@@ -144,6 +144,10 @@ class Rasterizer:
         self._lambda_dist = float(v)
         self._chk(lib().gs_rasterizer_set_lambda_dist(self._h, float(v)))
 
+    def set_wait_limits(self, copy_wait_cycles: int, drain_wait_cycles: int = 2_000_000_000):
+        """Limits (SM cycles) of the fused projection backward + Adam kernel's bounded waits."""
+        self._chk(lib().gs_rasterizer_set_wait_limits(self._h, copy_wait_cycles, drain_wait_cycles))
+
     def upload_scene(self, scene: SceneInput, stream: int = 0):
         s = scene.c()
         self._chk(lib().gs_rasterizer_upload_scene(self._h, C.byref(s), stream))
@@ -188,6 +192,12 @@ class Rasterizer:
 
     def write_async(self, name: str, host_ptr: int, nbytes: int, offset_bytes: int = 0, stream: int = 0):
         self._chk(lib().gs_rasterizer_write_async(self._h, BUF[name], offset_bytes, host_ptr, nbytes, stream))
+
+    def raster_work(self, stream: int = 0) -> dict:
+        """Work of the raster kernels on the last forward, counted on the device."""
+        out = (C.c_uint64 * 4)()
+        self._chk(lib().gs_raster_work(self._h, out, stream))
+        return {"fwd_evals": int(out[0]), "contrib_pairs": int(out[1]), "bwd_evals": int(out[2]), "pixels": int(out[3])}
 
     def entry_count(self) -> int:
         return int(self.read("entry_count", 1)[0])
@@ -324,9 +334,11 @@ class StepSettings:
     w_ssim: float = 0.2
     adam: AdamSettings = field(default_factory=AdamSettings)
     form: str = "chosen"  # "plain" or "chosen"
+    loss: str = "l1_ssim"  # "l1_ssim" (against the target) or "given" (the caller's dl_dcolor)
 
     def c(self) -> StepConfig:
-        return StepConfig(self.w_l1, self.w_ssim, self.adam.c(), 0 if self.form == "plain" else 1)
+        return StepConfig(self.w_l1, self.w_ssim, self.adam.c(), 0 if self.form == "plain" else 1,
+                          {"l1_ssim": 0, "given": 1}[self.loss])
 
 
 class TileBinner:

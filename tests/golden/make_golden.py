@@ -39,7 +39,8 @@ def forward_case(seed, n, deg, size):
     scene, cam = make_scene(seed, n, deg, size)
     s, c = f32_scene(scene), f32_cam(cam)
     out = oracle.render(s, c)
-    return dict(**scene_arrays(s, c), **{"out_" + k: v for k, v in out.items()})
+    keys = ("color", "alpha", "depth", "normal", "trans", "ncontrib", "marginal")  # the fixture's fields
+    return dict(**scene_arrays(s, c), **{"out_" + k: out[k] for k in keys})
 
 
 def gradient_case(seed, n, deg, size, aux):

@@ -1,16 +1,24 @@
 """Precision report: the CUDA forward and backward with FP32, FP16 and BF16
-storage of SH and projected record fields (geometry, compositing and
-accumulation stay FP32), each against the FP64 oracle (tile-binned walk) on
-the same f32-rounded scene: image PSNR and, for the linear loss Σ w·colour,
-the relative L2 error of each parameter class's gradient. Pixels the oracle
-flags as marginal carry no loss weight and are left out of the PSNR; besides
-the fixed bands around the α, clamp, transmittance and branch thresholds, the
-oracle flags a pixel where a float32 evaluation of a hit's exponent is
-ill-conditioned (surfels seen nearly edge-on, where the ray–splat solve divides
-by det ≈ 0) or a decision lies within that error bound.
+storage of SH and projected record fields (geometry, colour, opacity,
+compositing and accumulation stay FP32; normal and depth are 16-bit), each
+against the FP64 oracle (tile-binned walk) on the same f32-rounded scene:
+image PSNR and, for the linear loss sum w.colour, the relative L2 error of
+each parameter class's gradient. Pixels the oracle flags as marginal carry no
+loss weight and are left out of the PSNR; besides the fixed bands around the
+alpha, clamp, transmittance and branch thresholds, the oracle flags a pixel
+where a float32 evaluation of a hit's exponent is ill-conditioned (surfels
+seen nearly edge-on, where the ray-splat solve divides by det ~ 0) or a
+decision lies within that error bound.
 
-Default size: 200,000 clustered surfels (SH degree 3) and one 1280×720 view.
-With GS_PRECISION_FULL=1: 3,000,000 surfels and four 1920×1080 views."""
+Targets: PSNR >= 60 dB and gradient relative error <= 1e-3 for every storage
+precision. BF16 misses the gradient target by construction: its 8-bit
+significand rounds SH coefficients of N(0, 0.1) by up to 2e-4 absolute, which
+alone moves the colour gradients' chain by about 1.2e-3 relative (measured by
+rounding the oracle's own SH). That miss is reported as an expected failure;
+BF16 is held to 3e-3.
+
+Default size: 1,000,000 clustered surfels (SH degree 3) and one 1920x1080 view.
+With GS_PRECISION_FULL=1: 3,000,000 surfels and four 1920x1080 views."""
 import json
 import os
 
@@ -24,15 +32,17 @@ from splattar_b200.synthetic import make_surfels, ring_cameras
 pytestmark = pytest.mark.gpu
 
 CLASSES = (("pos", 4, 3), ("scales", 2, 2), ("quat", 4, 4), ("opacity", 1, 1), ("sh", 48, 48))
-MIN_PSNR = {"f32": 60.0, "f16": 50.0, "bf16": 40.0}
-MAX_GRAD_ERR = {"f32": 1e-3, "f16": 2e-3, "bf16": 1e-2}
+MIN_PSNR = {"f32": 60.0, "f16": 60.0, "bf16": 60.0}
+TARGET_GRAD_ERR = 1e-3
+MAX_GRAD_ERR = {"f32": 1e-3, "f16": 1e-3, "bf16": 3e-3}
+_REPORT = {}
 
 
 def _setup():
     if os.environ.get("GS_PRECISION_FULL") == "1":
         n, res = 3_000_000, [(1920, 1080)] * 4
     else:
-        n, res = 200_000, [(1280, 720)]
+        n, res = 1_000_000, [(1920, 1080)]
     s = make_surfels(n, 0, True, 3, 0.1)
     cams = ring_cameras(res)
     return s, cams
@@ -40,7 +50,7 @@ def _setup():
 
 def _gpu(s, cam, precision, w4):
     n, P = s.n, cam.width * cam.height
-    r = Rasterizer(n, cam.width, cam.height, 48 * n, precision=precision)
+    r = Rasterizer(n, cam.width, cam.height, 64 * n, precision=precision)
     r.upload_scene(s.scene_input())
     r.forward(cam, n)
     r.check()
@@ -58,7 +68,9 @@ def _gpu(s, cam, precision, w4):
     return img, g
 
 
-def test_precision_report():
+def _report():
+    if _REPORT:
+        return _REPORT
     s, cams = _setup()
     scene = oracle.Scene(s.positions.astype(np.float64), s.scales.astype(np.float64), s.quats.astype(np.float64),
                          s.opacities.astype(np.float64), s.sh48().astype(np.float64), 3)
@@ -93,7 +105,22 @@ def test_precision_report():
         report["precisions"][prec] = {"psnr_db": round(psnr, 2), "grad_rel_l2": {k: float(f"{e:.3e}") for k, e in
                                                                                  errs.items()}}
     print("PRECISION_REPORT " + json.dumps(report))
-    for prec, rep in report["precisions"].items():
-        assert rep["psnr_db"] >= MIN_PSNR[prec], (prec, rep)
-        for k, e in rep["grad_rel_l2"].items():
-            assert e <= MAX_GRAD_ERR[prec], (prec, k, e)
+    _REPORT.update(report)
+    return _REPORT
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16", "bf16"])
+def test_precision_report(prec):
+    rep = _report()["precisions"][prec]
+    assert rep["psnr_db"] >= MIN_PSNR[prec], (prec, rep)
+    for k, e in rep["grad_rel_l2"].items():
+        assert e <= MAX_GRAD_ERR[prec], (prec, k, e)
+
+
+def test_bf16_gradient_target():
+    """The 1e-3 gradient target with BF16 storage: expected to fail (see the module docstring)."""
+    rep = _report()["precisions"]["bf16"]
+    worst = max(rep["grad_rel_l2"].values())
+    if worst > TARGET_GRAD_ERR:
+        pytest.xfail(f"bf16 storage misses the 1e-3 gradient target: worst class {worst:.2e}")
+    assert worst <= TARGET_GRAD_ERR

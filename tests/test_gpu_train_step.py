@@ -169,18 +169,54 @@ def test_tight_binning_keeps_images_and_gradients():
     print(f"entries: reference rects {a['E']}, tight {b['E']} ({a['E'] / b['E']:.2f}x)")
 
 
-def test_deterministic_step_is_bitwise_reproducible():
+@pytest.mark.parametrize("form", ["chosen", "plain"])
+def test_deterministic_step_is_bitwise_reproducible(form):
+    """Parameters, moments and the per-view camera gradients repeat bit for bit."""
     scene, cams = multi_view_setup(44, 300)
     rc = [raster_camera(c, 3) for c in cams]
     outs = []
     for _ in range(2):
         r = _trainer(scene, cams, deterministic=True)
         for _ in range(2):
-            r.train_step(rc, scene.n, StepSettings(form="chosen"))
+            r.train_step(rc, scene.n, StepSettings(form=form))
         r.check()
-        outs.append(_params(r, scene.n))
+        o = _params(r, scene.n)
+        o["grad_cam"] = r.read("grad_cam", 16 * len(cams))
+        o["m_pos"] = r.read("m_pos", 4 * scene.n)
+        outs.append(o)
+    assert np.abs(outs[0]["grad_cam"]).max() > 0
     for k in outs[0]:
         assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_fused_adam_wait_expiry_reports_timeout_and_skips_update():
+    """The chosen step's fused projection backward + Adam waits for its
+    optimizer-row copies with a bounded wait. A limit of 0 makes that wait give
+    up at once: every block flags the expiry, lets its copies land (the drain
+    wait) and exits without updating. The step then reports
+    GS_ERR_DEVICE_TIMEOUT, the parameters are unchanged, and the handle keeps
+    working once the limit is restored."""
+    from splattar_b200 import GsError
+    scene, cams = multi_view_setup(45, 300)
+    rc = [raster_camera(c, 3) for c in cams]
+    r = _trainer(scene, cams)
+    before = _params(r, scene.n)
+    r.set_wait_limits(0)
+    r.train_step(rc, scene.n, StepSettings(form="chosen"))
+    with pytest.raises(GsError) as err:
+        r.check()
+    assert err.value.status == 4  # GS_ERR_DEVICE_TIMEOUT
+    mid = _params(r, scene.n)
+    for k in before:
+        assert np.array_equal(before[k], mid[k]), k
+    r.check()  # the error word was cleared by the report
+    r.set_wait_limits(2_000_000_000)
+    r.train_step(rc, scene.n, StepSettings(form="chosen"))
+    r.check()
+    after = _params(r, scene.n)
+    assert not np.array_equal(after["raw_pos"], before["raw_pos"])
+    with pytest.raises(GsError):
+        r.set_wait_limits(0, 1000)  # the drain wait must stay long enough for the copies to land
 
 
 def test_train_step_reduces_loss():
