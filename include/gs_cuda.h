@@ -454,10 +454,12 @@ gs_status gs_exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, u
  * scratch is a fixed array in the library's device image sized for at most
  * 1,048,576 pairs (about 8.6 MB, held by every GPU that loads the library
  * until exit); larger n returns GS_ERR_CAPACITY. The first call on a device
- * looks up that array's device address, so make it before any stream
- * capture. Calls share the array: calls that overlap on the GPU (different
- * streams, or different host threads) race and corrupt each other's
- * results. Stream-ordered, does not synchronise. */
+ * looks up that array's device address and keeps it for the process, so make
+ * it before any stream capture, and do not call this entry point after
+ * resetting the device (cudaDeviceReset), which invalidates that address.
+ * Calls share the array: calls that overlap on the GPU (different streams,
+ * or different host threads) race and corrupt each other's results.
+ * Stream-ordered, does not synchronise. */
 gs_status gs_radix_sort_pairs_noalloc(uint32_t* keys, uint32_t* vals, uint64_t n, uint32_t key_bits, void* stream);
 
 /* ---- Surfel PLY files (first_attempt/crates/gs-io/src/ply) ---------------

@@ -36,7 +36,10 @@ unsigned char* g_noalloc_ptr[MAX_DEVICES] = {};
 
 // Device address of the scratch array on the current device. In host code
 // the array's name is only a host-side stand-in, so its device address is
-// looked up once per device (with that device current) and cached.
+// looked up once per device (with that device current) and cached for the
+// life of the process: a caller that resets the device (cudaDeviceReset)
+// destroys the context that address belongs to and must not call this entry
+// point afterwards.
 gs_status noalloc_scratch(unsigned char** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

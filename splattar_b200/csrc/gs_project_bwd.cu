@@ -436,6 +436,24 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
   float* s_sh = s_stage + PBA_PARAMS * 3 * S;          // [SH_FLOATS][SHP]: the block's activated SH, transposed
   float* s_g = s_sh + SH_FLOATS * SHP;                 // [PBA_SLOTS][PITCH]
   const uint32_t i0 = blockIdx.x * (uint32_t)S;
+  // This thread's (view, surfel) item and its record gradient, loaded first
+  // so the loads are in flight while the block stages its SH rows.
+  const int v1 = tid / S, sl1 = tid % S;
+  const uint32_t i1 = i0 + (uint32_t)sl1;
+  const bool active1 = v1 < V && i1 < a.n;
+  float G[GG_STRIDE];
+  bool gnz = false;
+  if (active1) {
+    const uint32_t item = (uint32_t)v1 * a.n + i1;
+    if (a.touched == nullptr || a.partials != nullptr) {
+      gnz = load_G<AUX>(a, item, G);
+    } else if ((__ldg(a.touched + (item >> 5)) >> (item & 31u)) & 1u) {
+      gnz = load_G<AUX>(a, item, G);
+      float4* gp = reinterpret_cast<float4*>(const_cast<float*>(a.grad_geom) + (size_t)item * GG_STRIDE);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) gp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
   if (tid == 0) mbar_init(&s_bar);
   __syncthreads();
   if (tid == 0) {
@@ -481,9 +499,9 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
   __syncthreads();
   // ---- phase 1
   {
-    const int v = tid / S, sl = tid % S;
-    const uint32_t i = i0 + (uint32_t)sl;
-    const bool active = v < V && i < a.n;
+    const int v = v1, sl = sl1;
+    const uint32_t i = i1;
+    const bool active = active1;
     // ORD: this thread's column; atomic: the surfel's column, shared by its views.
     float* col = s_g + (ORD ? tid : sl);
     auto put = [&](int slot, float g) {
@@ -497,8 +515,7 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
     bool any = false;
     uint32_t written = 0;  // SH coefficients whose gradient slots the chain wrote
     if (active) {
-      float G[GG_STRIDE];
-      if (load_G<AUX>(a, (uint32_t)v * a.n + i, G)) {
+      if (gnz) {
         const Cam k = load_cam(a.views, v);
         const float* shc = s_sh + sl;
         chain_core<PREC, AUX>(k, __ldg(a.pos + i), __ldg(a.scales + i), __ldg(a.quats + i),

@@ -560,8 +560,14 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
   }
 }
 
+// Resident single-warp backward CTAs per SM that the register allocation must
+// allow (1: the compiler's choice).
+#ifndef GS_BWD_WARP_CTAS
+#define GS_BWD_WARP_CTAS 1
+#endif
 template <int TS, int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT, bool MASK = false>
-__global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
+__global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_WARP_CTAS : 1)
+    k_raster_bwd(RasterArgs a) {
   static_assert(!MASK || !AUX, "contributor masks cover the colour-only backward");
   using L = Layout<TS, PPT>;
   constexpr int NT = L::NT, NW = NT / 32, TP = TS * TS;
@@ -587,6 +593,11 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
   __shared__ float s_part[DIRECT ? 1 : NW][DIRECT ? 1 : BATCH][NG];
   __shared__ int s_wcount[2][NW];
   __shared__ int s_tile, s_maxnc;
+  // Colour-only: the tile's dL/dcolour per pixel (each thread reads back only
+  // its own pixels), read where a pair contributes instead of held in three
+  // registers per pixel.
+  constexpr bool DLC_SMEM = !AUX && TS <= 16;  // (tiles of 32: 16 KB more than the static limit allows)
+  __shared__ float4 s_dlc[DLC_SMEM ? TP : 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;
   uint32_t pbit[PPT], thread_gbits = 0u;
@@ -603,6 +614,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
       reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[q4] = make_float4(s0, s1, s2, s3);
     } else if (s0 != 0.f || s1 != 0.f || s2 != 0.f || s3 != 0.f) {
       red_add_v4(a.grad_geom + (size_t)s_item[k] * GG_STRIDE + 4 * q4, s0, s1, s2, s3);
+      if (!DIRECT && a.touched != nullptr) atomicOr(a.touched + (s_item[k] >> 5), 1u << (s_item[k] & 31u));
     }
   };
   auto emit_zero = [&](int k) {
@@ -652,6 +664,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
         const long long pix = g.row0 + (long long)p * g.W;
         const float4 gc = a.dl_dcolor[pix];
         dlc[p] = make_float3(gc.x, gc.y, gc.z);
+        if (DLC_SMEM) s_dlc[L::row(tid) * TS + L::col(tid) + p * TS] = gc;
         const float4 aux = a.out_aux[pix];
         T[p] = aux.x;
         nc[p] = a.out_nc[pix];
@@ -816,7 +829,12 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             const float inv_oma = rcp_approx(1.0f - alpha);
             const float t_before = T[p] * inv_oma;
             const float w = t_before * alpha;
-            const float dc = dlc[p].x * r3.x + dlc[p].y * r3.y + dlc[p].z * r3.z;
+            float3 gcol = dlc[p];
+            if (DLC_SMEM) {
+              const float4 g4 = s_dlc[L::row(tid) * TS + L::col(tid) + p * TS];
+              gcol = make_float3(g4.x, g4.y, g4.z);
+            }
+            const float dc = gcol.x * r3.x + gcol.y * r3.y + gcol.z * r3.z;
             float dl_dalpha = dc * t_before - suf_c[p] * inv_oma;
             float dl_dt = 0.f;
             if (AUX) {
@@ -841,9 +859,9 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             suf_c[p] += dc * w;
             T[p] = t_before;
             {  // packed pairs round per component as the scalar FFMAs (x·1 is exact)
-              const float2 c2 = __ffma2_rn(make_float2(dlc[p].x, dlc[p].y), make_float2(w, w), make_float2(gg[11], gg[12]));
+              const float2 c2 = __ffma2_rn(make_float2(gcol.x, gcol.y), make_float2(w, w), make_float2(gg[11], gg[12]));
               gg[11] = c2.x; gg[12] = c2.y;
-              gg[13] += dlc[p].z * w;
+              gg[13] += gcol.z * w;
             }
             if (raw_alpha <= ALPHA_CLAMP) {
               // dL/dĝ·ĝ = dL/dα·o·ĝ; ray branch: ĝ = exp(−(u²+v²)/2) with
@@ -887,6 +905,8 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_bwd(RasterArgs a) {
             const float r1 = __shfl_down_sync(FULL, r, 2), r2 = __shfl_down_sync(FULL, r, 4);
             const float r3 = __shfl_down_sync(FULL, r, 6);
             if ((lane & 7) == 0) emit4(k, lane >> 3, r, r1, r2, r3);
+            if (!DET && a.touched != nullptr && __ballot_sync(FULL, r != 0.f) && lane == 0)
+              atomicOr(a.touched + (s_item[k] >> 5), 1u << (s_item[k] & 31u));
           } else {
             if (!(lane & 1)) s_part[warp][k][lane >> 1] = r;
           }

@@ -23,7 +23,8 @@ def _images(seed, P, smooth=True):
     return img, ref
 
 
-@pytest.mark.parametrize("size,w_l1,w_ssim", [((64, 48), 0.8, 0.2), ((37, 53), 0.8, 0.1), ((128, 128), 0.0, 1.0)])
+@pytest.mark.parametrize("size,w_l1,w_ssim", [((64, 48), 0.8, 0.2), ((37, 53), 0.8, 0.1), ((128, 128), 0.0, 1.0),
+                                              ((45, 300), 0.8, 0.2), ((300, 261), 0.8, 0.2)])
 def test_l1_ssim_matches_oracle(size, w_l1, w_ssim):
     W, H = size
     scene, cam = make_scene(5, 10, 0, 32)

@@ -50,6 +50,10 @@ def test_noalloc_sort_matches_allocating_sort_twice():
         ((rng.integers(0, 8192, 1_000_003)).astype(np.uint32), 13),
         # full-range 32-bit keys (four passes), the maximum size
         (rng.integers(0, 2**32, MAX_PAIRS, dtype=np.uint64).astype(np.uint32), 32),
+        # odd pass counts (three passes, one pass): the sorted pairs end in the
+        # scratch array and are copied back into the caller's arrays
+        ((rng.integers(0, 2**24, 777_777)).astype(np.uint32), 24),
+        ((rng.integers(0, 32, 4099)).astype(np.uint32), 5),
     ]
     for keys, bits in cases:  # two calls in a row, the second reusing the scratch
         vals = np.arange(keys.size, dtype=np.uint32)
