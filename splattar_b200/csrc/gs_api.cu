@@ -584,13 +584,9 @@ gs_status run_loss(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vhost
                    float w_ssim, double* sums, cudaStream_t st) {
   SsimArgs a{};
   a.views = vdev; a.n_views = (int)nv;
-  int t16 = 0, strips = 0;
-  for (uint32_t v = 0; v < nv; ++v) {
-    t16 += ((vhost[v].width + 15) / 16) * ((vhost[v].height + 15) / 16);
-    strips += ssim_strips(vhost[v].width, vhost[v].height);
-  }
+  int t16 = 0;
+  for (uint32_t v = 0; v < nv; ++v) t16 += ((vhost[v].width + 15) / 16) * ((vhost[v].height + 15) / 16);
   a.total_tiles16 = t16;
-  a.total_strips = strips;
   a.img = r->out_color; a.target = r->target; a.coef = r->coef; a.coef_stride = r->max_pixels;
   a.dl_dcolor = r->dl_dcolor;
   a.loss_sums = sums;

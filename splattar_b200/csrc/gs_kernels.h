@@ -314,12 +314,8 @@ struct SsimArgs {
   double* loss_sums;          // 2 per view
   float w_l1, w_ssim;
   float w[6];                 // Gaussian window taps 0..5 (set by the launcher)
-  int total_strips;           // > 0: the fused streaming kernel over this many strip segments
-                              // (ssim_strips per view); 0: the two tiled kernels and the coef planes
 };
 int launch_ssim(const SsimArgs& a, cudaStream_t st);
-// Strip segments of the fused L1+SSIM kernel for one view.
-int ssim_strips(int width, int height);
 
 struct NormalArgs {
   const ViewInfo* views;

@@ -421,240 +421,6 @@ int launch_normal_loss(const NormalArgs& a, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
-// ---- fused streaming form -------------------------------------------------
-// One block per (view, strip of SW output columns, segment of up to SEG output
-// rows). The block walks its input rows downwards once; per input row y:
-//   A  the row's x and y (rgb, zero outside the image) over the strip plus a
-//      10-column halo are staged in shared memory (prefetched two rows ahead);
-//   B  thread (channel, moment column) blurs its channel horizontally into the
-//      five moments (x, y packed, x², y² packed, xy) and keeps them in an
-//      11-row register ring;
-//   C  with 11 rows in the ring it blurs them vertically: the moments of row
-//      y − 5, whose SSIM coefficient maps Cμ, Cx², Cxy it forms (zero outside
-//      the image) and places in a shared coefficient row;
-//   D  the output threads blur the coefficient row horizontally into an 11-row
-//      register ring;
-//   E  with 11 coefficient rows they blur vertically and combine with the L1
-//      term into dL/dx of row y − 10, written as float4 rows.
-// Each image pixel is read from HBM once and dL/dx written once (48 B per
-// pixel with float4 buffers); the halo columns and the 20 warm-up rows of a
-// segment come from L2. Blur, coefficient and gradient arithmetic are the
-// same operations in the same order as the two-kernel form above.
-namespace {
-
-constexpr int SW = 32;                // output columns per strip
-constexpr int SEG = 128;              // output rows per segment
-constexpr int MWC = SW + 2 * HALO;    // 42 moment columns (halo 5)
-constexpr int IWC = SW + 4 * HALO;    // 52 input columns (halo 10)
-constexpr int FT = 128;               // threads: 3 channels × 42 moment columns = 126 busy
-
-struct StripLoc {
-  int v, x0, y0, y1, W, H;
-  long long pix_base;
-};
-
-__device__ __forceinline__ StripLoc locate_strip(const SsimArgs& a, int b) {
-  StripLoc L;
-  int v = 0, base = 0;
-  for (;;) {
-    const ViewInfo* V = a.views + v;
-    const int W = __ldg(&V->width), H = __ldg(&V->height);
-    const int sx = (W + SW - 1) / SW, nb = sx * ((H + SEG - 1) / SEG);
-    if (b < base + nb || v + 1 == a.n_views) {
-      const int lb = b - base;
-      L.v = v; L.W = W; L.H = H;
-      L.x0 = (lb % sx) * SW;
-      L.y0 = (lb / sx) * SEG;
-      L.y1 = min(L.y0 + SEG, H);
-      L.pix_base = __ldg(&V->pix_base);
-      return L;
-    }
-    base += nb;
-    ++v;
-  }
-}
-
-// acc = w0·c[5] + Σ_d w[5−d]·(c[d] + c[10−d]), the order of slide11 / slide11x2.
-__device__ __forceinline__ float blur11(const float (&w)[6], const float (&c)[TAPS]) {
-  float acc = w[0] * c[HALO];
-#pragma unroll
-  for (int d = 0; d < HALO; ++d) acc += w[HALO - d] * (c[d] + c[TAPS - 1 - d]);
-  return acc;
-}
-__device__ __forceinline__ float2 blur11x2(const float (&w)[6], const float2 (&c)[TAPS]) {
-  float2 acc = __fmul2_rn(f2(w[0]), c[HALO]);
-#pragma unroll
-  for (int d = 0; d < HALO; ++d) acc = __ffma2_rn(f2(w[HALO - d]), __fadd2_rn(c[d], c[TAPS - 1 - d]), acc);
-  return acc;
-}
-
-__global__ void __launch_bounds__(FT) k_ssim_fused(SsimArgs a) {
-  __shared__ float2 s_in[2][3][IWC];   // (x, y) per channel of the staged input row
-  __shared__ float s_cf[2][3][3][MWC];  // coefficient row [buf][Cμ, Cx², Cxy][channel][moment column]
-  __shared__ float4 s_out[SW];
-  __shared__ double s_red[2][FT / 32];
-  const StripLoc L = locate_strip(a, blockIdx.x);
-  const int t = threadIdx.x;
-  const int ch = t / MWC, col = t - ch * MWC;
-  const bool mom = t < 3 * MWC;
-  const bool outp = mom && col >= HALO && col < HALO + SW;
-  const int ox = L.x0 + col - HALO;  // image column of this thread's moment column (and output column)
-  float w[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) w[k] = a.w[k];
-  const float C1 = 1e-4f, C2 = 9e-4f;
-  const float inv_n3 = 1.0f / (3.0f * (float)L.W * (float)L.H);
-  const float dw = -a.w_ssim * inv_n3;
-  const float k1 = a.w_l1 * inv_n3;
-  // Loader: thread t < IWC stages image column x0 − 10 + t of img, IWC ≤ t < 2·IWC of target.
-  const bool loader = t < 2 * IWC;
-  const int lc = t < IWC ? t : t - IWC;
-  const int lx = L.x0 - 2 * HALO + lc;
-  const float4* src = t < IWC ? a.img : a.target;
-  auto fetch = [&](int y) {
-    if (!loader || y < 0 || y >= L.H || lx < 0 || lx >= L.W) return make_float4(0.f, 0.f, 0.f, 0.f);
-    return __ldg(src + L.pix_base + (long long)y * L.W + lx);
-  };
-  const int ystart = L.y0 - 2 * HALO;
-  const int nsteps = (L.y1 - L.y0) + 4 * HALO;
-  float4 pf0 = fetch(ystart), pf1 = fetch(ystart + 1);
-  float2 mxy[TAPS], mqq[TAPS];  // per ring row: (μx, μy) and (E[x²], E[y²]) horizontal sums
-  float mp[TAPS];               // E[xy]
-  float2 cq[TAPS];              // (Cμ, Cx²) horizontal sums
-  float cc[TAPS];               // Cxy
-  float xr[TAPS], yr[TAPS];     // centre x, y of the thread's column
-#pragma unroll
-  for (int k = 0; k < TAPS; ++k) {
-    mxy[k] = mqq[k] = cq[k] = make_float2(0.f, 0.f);
-    mp[k] = cc[k] = xr[k] = yr[k] = 0.f;
-  }
-  float l1 = 0.f, ss = 0.f;
-  for (int base = 0; base < nsteps; base += TAPS) {
-#pragma unroll
-    for (int k = 0; k < TAPS; ++k) {
-      const int s = base + k;
-      if (s >= nsteps) break;
-      const int y = ystart + s, buf = s & 1;
-      // A: stage row y, prefetch row y + 2.
-      if (loader) {
-        const float4 v = pf0;
-        float2* row = &s_in[buf][0][0];
-        const int o = t < IWC ? 0 : 1;  // x goes to .x, y to .y
-        reinterpret_cast<float*>(row + 0 * IWC + lc)[o] = v.x;
-        reinterpret_cast<float*>(row + 1 * IWC + lc)[o] = v.y;
-        reinterpret_cast<float*>(row + 2 * IWC + lc)[o] = v.z;
-      }
-      pf0 = pf1;
-      pf1 = fetch(y + 2);
-      __syncthreads();
-      // B: horizontal moments of row y into ring slot k.
-      if (mom) {
-        const float2* R = &s_in[buf][ch][col];
-        float2 c[TAPS], q[TAPS];
-        float pr[TAPS];
-#pragma unroll
-        for (int i = 0; i < TAPS; ++i) {
-          c[i] = R[i];
-          q[i] = __fmul2_rn(c[i], c[i]);
-          pr[i] = c[i].x * c[i].y;
-        }
-        mxy[k] = blur11x2(w, c);
-        mqq[k] = blur11x2(w, q);
-        mp[k] = blur11(w, pr);
-        xr[k] = c[HALO].x;
-        yr[k] = c[HALO].y;
-      }
-      // C: vertical moments of row y − 5 and its coefficient maps.
-      if (s >= 2 * HALO) {
-        const int ym = y - HALO;
-        if (mom) {
-          float2 a2[TAPS], b2[TAPS];
-          float p1[TAPS];
-#pragma unroll
-          for (int d = 0; d < TAPS; ++d) {
-            a2[d] = mxy[(k + 1 + d) % TAPS];
-            b2[d] = mqq[(k + 1 + d) % TAPS];
-            p1[d] = mp[(k + 1 + d) % TAPS];
-          }
-          const float2 mu = blur11x2(w, a2), bb = blur11x2(w, b2);
-          const float bxy = blur11(w, p1);
-          float cmv = 0.f, cx2v = 0.f, cxyv = 0.f;
-          if (ym >= 0 && ym < L.H && ox >= 0 && ox < L.W) {
-            const float mu_x = mu.x, mu_y = mu.y;
-            const float sx2 = bb.x - mu_x * mu_x, sy2 = bb.y - mu_y * mu_y, sxy = bxy - mu_x * mu_y;
-            const float p = mu_x * mu_x + mu_y * mu_y + C1;
-            const float qd = sx2 + sy2 + C2;
-            const float ip = __fdividef(1.0f, p), iq = __fdividef(1.0f, qd);
-            const float l = (2.0f * mu_x * mu_y + C1) * ip;
-            const float cs = (2.0f * sxy + C2) * iq;
-            if (outp && ym >= L.y0 && ym < L.y1) ss += l * cs;
-            cmv = (cs * (2.0f * mu_y - 2.0f * mu_x * l) * ip + l * (-2.0f * mu_y + 2.0f * mu_x * cs) * iq) * dw;
-            cx2v = (-l * cs * iq) * dw;
-            cxyv = (2.0f * l * iq) * dw;
-          }
-          s_cf[buf][0][ch][col] = cmv;
-          s_cf[buf][1][ch][col] = cx2v;
-          s_cf[buf][2][ch][col] = cxyv;
-        }
-        __syncthreads();
-        // D: horizontal blur of the coefficient row into ring slot k.
-        if (outp) {
-          const float* P0 = &s_cf[buf][0][ch][col - HALO];
-          const float* P1 = &s_cf[buf][1][ch][col - HALO];
-          const float* P2 = &s_cf[buf][2][ch][col - HALO];
-          float2 c[TAPS];
-          float e[TAPS];
-#pragma unroll
-          for (int i = 0; i < TAPS; ++i) {
-            c[i] = make_float2(P0[i], P1[i]);
-            e[i] = P2[i];
-          }
-          cq[k] = blur11x2(w, c);
-          cc[k] = blur11(w, e);
-        }
-        // E: vertical blur of the coefficient rows, dL/dx of row y − 10.
-        if (s >= 4 * HALO) {
-          const int yo = y - 2 * HALO;
-          if (outp) {
-            float2 c[TAPS];
-            float e[TAPS];
-#pragma unroll
-            for (int d = 0; d < TAPS; ++d) {
-              c[d] = cq[(k + 1 + d) % TAPS];
-              e[d] = cc[(k + 1 + d) % TAPS];
-            }
-            const float2 v2 = blur11x2(w, c);
-            const float vxy = blur11(w, e);
-            const float xs = xr[(k + 1) % TAPS], ys = yr[(k + 1) % TAPS];
-            const float diff = xs - ys;
-            const float sg = diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f);
-            const float out = sg * k1 + v2.x + 2.0f * xs * v2.y + ys * vxy;
-            if (ox < L.W) l1 += fabsf(diff);
-            reinterpret_cast<float*>(&s_out[col - HALO])[ch] = out;
-          }
-          __syncthreads();
-          if (t < SW && L.x0 + t < L.W) {
-            const float4 o = s_out[t];
-            a.dl_dcolor[L.pix_base + (long long)yo * L.W + L.x0 + t] = make_float4(o.x, o.y, o.z, 0.f);
-          }
-        }
-      }
-    }
-  }
-  // Per-view loss sums: warp, then block, then one double atomic each.
-  double dl1 = warp_sum(l1), dss = warp_sum(ss);
-  if ((t & 31) == 0) { s_red[0][t >> 5] = dl1; s_red[1][t >> 5] = dss; }
-  __syncthreads();
-  if (t == 0) {
-    double t0 = 0, t1 = 0;
-    for (int k = 0; k < FT / 32; ++k) { t0 += s_red[0][k]; t1 += s_red[1][k]; }
-    atomicAdd(a.loss_sums + 2 * L.v, t0);
-    atomicAdd(a.loss_sums + 2 * L.v + 1, t1);
-  }
-}
-
-}  // namespace
-
 int launch_ssim(const SsimArgs& a_in, cudaStream_t st) {
   if (a_in.total_tiles16 == 0) return 0;
   SsimArgs a = a_in;
@@ -664,15 +430,9 @@ int launch_ssim(const SsimArgs& a_in, cudaStream_t st) {
   s = g[0];
   for (int k = 1; k <= 5; ++k) s += 2 * g[k];
   for (int k = 0; k <= 5; ++k) a.w[k] = (float)(g[k] / s);
-  if (a.total_strips > 0) {
-    k_ssim_fused<<<a.total_strips, FT, 0, st>>>(a);
-  } else {
-    k_ssim_moments<<<a.total_tiles16, 256, 0, st>>>(a);
-    k_ssim_grad<<<a.total_tiles16, 256, 0, st>>>(a);
-  }
+  k_ssim_moments<<<a.total_tiles16, 256, 0, st>>>(a);
+  k_ssim_grad<<<a.total_tiles16, 256, 0, st>>>(a);
   return (int)cudaGetLastError();
 }
-
-int ssim_strips(int width, int height) { return ((width + SW - 1) / SW) * ((height + SEG - 1) / SEG); }
 
 }  // namespace gs

@@ -596,7 +596,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
   // Colour-only: the tile's dL/dcolour per pixel (each thread reads back only
   // its own pixels), read where a pair contributes instead of held in three
   // registers per pixel.
-  constexpr bool DLC_SMEM = !AUX && TS <= 16;  // (tiles of 32: 16 KB more than the static limit allows)
+#ifndef GS_BWD_DLC_SMEM
+#define GS_BWD_DLC_SMEM 1
+#endif
+  constexpr bool DLC_SMEM = GS_BWD_DLC_SMEM && !AUX && TS <= 16;  // (tiles of 32: 16 KB more than the static limit allows)
   __shared__ float4 s_dlc[DLC_SMEM ? TP : 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;

@@ -255,19 +255,25 @@ def test_config0_full_frame_l1_ssim_matches_oracle():
         rel = float(np.linalg.norm(g_gpu[k] - gr) / np.linalg.norm(gr))
         assert rel <= 1e-3, (k, rel)
 
-    # One chosen training step on the same state: the gradient its fused Adam
-    # consumed (from the first moments of the first step, m = (1 - beta1) g)
-    # against the oracle's gradient of L1+SSIM of the step's own image.
+    # One chosen training step: the gradient its fused Adam consumed (from the
+    # first moments of the first step, m = (1 - beta1) g) against the oracle's
+    # gradient of L1+SSIM of the step's own image. optimizer_init re-derives
+    # the activated values through raw space (log/exp, logit/sigmoid), so the
+    # step's parameters are read after it.
     r.close()
     r = Rasterizer(n, c.width, c.height, precision="f32", color_only=True)
     r.upload_scene(wl.surfels.scene_input())
     r.write("target", target.ravel())
     r.optimizer_init(n)
+    scene = _scene_of(r, n, 0)
     a0 = {k: r.read(k, w * n).reshape(n, w).astype(np.float64) for k, w in (("scales", 2), ("opacities", 1))}
+    r.forward(c, n)
+    r.check()
+    img1 = r.read("out_color", 4 * P).reshape(P, 4)
     r.train_step([c], n, StepSettings(0.8, 0.2, AdamSettings(eps=1e-15), "chosen"))
     r.check()
     img2 = r.read("out_color", 4 * P).reshape(P, 4)
-    assert np.array_equal(img2[:, :3], img[:, :3])  # same parameters, same image (tight binning is exact)
+    assert np.array_equal(img2[:, :3], img1[:, :3])  # same parameters, same image (tight binning is exact)
     g_rec = {k: r.read("m_" + k, w * n).reshape(n, w).astype(np.float64) / float(np.float32(1.0) - np.float32(0.9))
              for k, w in (("pos", 4), ("scales", 2), ("quat", 4), ("opacity", 1), ("sh", 48))}
     r.close()

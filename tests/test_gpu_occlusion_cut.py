@@ -138,8 +138,12 @@ def test_training_with_the_cut_tracks_full_lists():
     handle as a second full-list handle does. Float atomics make any two
     runs differ slightly, and Adam's normalised step turns the sign of a
     near-zero gradient into a full learning-rate step, so the yardstick is
-    the spread between the two full-list runs (mean absolute difference)."""
+    the spread between the two full-list runs (mean absolute difference).
+    The cut changes which warps add an entry's gradient and in what order,
+    not only when; the second full-list run therefore uses another backward
+    launch shape, whose emission order differs in the same structural way."""
     a, b, c, cams, P, step = _pair(lr_zero=False, extra_full=True)
+    c.set_launch_shapes(64, 4, 128, 8)
     for _ in range(5):
         for r in (a, b, c):
             r.train_step(cams, N, step)
