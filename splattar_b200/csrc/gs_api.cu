@@ -142,11 +142,6 @@ struct gs_rasterizer {
 
   // gradients
   float* grad_geom = nullptr;
-  // Chosen step (atomic mode): one bit per item the backward raster added a
-  // record gradient to; the fused projection backward reads and zeroes
-  // exactly those, so grad_geom stays all zero between chosen steps.
-  uint32_t* touched = nullptr;
-  bool geom_clean = false;  // grad_geom known to be all zero over max_items
   float4* grad_pos = nullptr;
   float2* grad_scales = nullptr;
   float4* grad_quat = nullptr;
@@ -198,8 +193,8 @@ struct gs_rasterizer {
 
   // graph of the chosen-form step
   cudaStream_t cap_stream = nullptr;
-  // side stream of the chosen step: clears the touched-item bits and orders
-  // the backward's tiles while the forward and the loss run
+  // side stream of the chosen step: clears grad_geom and orders the
+  // backward's tiles while the forward and the loss run
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_fwd = nullptr, ev_side = nullptr;
   cudaGraphExec_t graph = nullptr;
@@ -515,12 +510,9 @@ RasterArgs bwd_args(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, int til
 // (the chosen step does both on its side stream).
 gs_status run_backward_raster(gs_rasterizer* r, const ViewInfo* vdev, uint32_t nv, int tiles, uint32_t n, int prec,
                               bool aux, bool persistent, cudaStream_t st, bool prepared = false) {
-  if (!r->det && !prepared) {
+  if (!r->det && !prepared)
     TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)nv * n, st));
-    r->geom_clean = false;  // this backward's record gradients stay in grad_geom
-  }
   RasterArgs ra = bwd_args(r, vdev, nv, tiles);
-  if (prepared && !r->det) ra.touched = r->touched;
   if (r->gmask_valid && !aux && r->tile == 16) ra.gmask = r->gmask;  // summary of the matching forward
   if (r->mask_valid && !aux) {  // masks of the matching colour-only forward
     ra.mask = r->mask;
@@ -666,17 +658,6 @@ gs_status cut_refresh(gs_rasterizer* r, uint32_t nv, uint32_t n, cudaStream_t st
   return GS_OK;
 }
 
-// The chosen step reads record gradients only for items its backward marked
-// and leaves grad_geom all zero; after any other backward (which keeps its
-// record gradients there) the buffer is cleared once before the next chosen
-// step, outside its graph.
-gs_status ensure_geom_clean(gs_rasterizer* r, cudaStream_t st) {
-  if (r->det || r->geom_clean) return GS_OK;
-  TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)r->max_items, st));
-  r->geom_clean = true;
-  return GS_OK;
-}
-
 gs_status ensure_graph_stream(gs_rasterizer* r) {
   if (!r->cap_stream) TRY_CUDA(r, cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking));
   return GS_OK;
@@ -698,12 +679,12 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   int tiles = 0;
   for (const ViewInfo& v : r->views_batched) tiles += v.tiles_x * v.tiles_y;
   // Side stream (forked from and joined into st, so it is part of a captured
-  // graph): the touched-item bits are cleared during the forward; the
-  // backward's tile order is computed during the loss.
+  // graph): grad_geom is cleared during the forward; the backward's tile
+  // order is computed during the loss.
   cudaStream_t side = r->side_stream;
   TRY_CUDA(r, cudaEventRecord(r->ev_fork, st));
   TRY_CUDA(r, cudaStreamWaitEvent(side, r->ev_fork, 0));
-  if (!r->det) TRY_CUDA(r, cudaMemsetAsync(r->touched, 0, sizeof(uint32_t) * (((size_t)nv * n + 31) / 32), side));
+  if (!r->det) TRY_CUDA(r, cudaMemsetAsync(r->grad_geom, 0, sizeof(float) * GG_STRIDE * (size_t)nv * n, side));
   // With GS_FLAG_COLOR_ONLY the step's forward leaves depth and normal unwritten (nothing reads them).
   gs_status s = run_forward(r, vdev, r->views_batched.data(), nv, tiles, n, prec, true, true, st, prof, r->color_only,
                             true);
@@ -725,7 +706,6 @@ gs_status chosen_body(gs_rasterizer* r, uint32_t nv, uint32_t n, const gs_step_c
   mark(prof, 7, st);
   TRY_CUDA(r, cudaMemsetAsync(r->grad_cam, 0, sizeof(float) * 16 * nv, st));
   ProjectBwdArgs b = pbwd_args(r, vdev, nv, n, prec);
-  if (!r->det) b.touched = r->touched;
   AdamFusedArgs o{};
   for (int k = 0; k < 5; ++k) o.cls[k] = AdamClass{r->raw[k], r->mom1[k], r->mom2[k], act_ptr(r, k), 0.f, 0.f};
   o.beta1 = cfg->adam.beta1; o.beta2 = cfg->adam.beta2; o.eps = cfg->adam.eps;
@@ -913,7 +893,6 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   ALLOC(r->loss_sums, 2 * (size_t)c.max_views);
   ALLOC(r->normal_loss_sums, (size_t)c.max_views);
   ALLOC(r->grad_geom, I * GG_STRIDE);
-  if (!r->det) ALLOC(r->touched, (I + 31) / 32);
   ALLOC(r->grad_pos, N); ALLOC(r->grad_scales, N); ALLOC(r->grad_quat, N); ALLOC(r->grad_opacity, N);
   ALLOC(r->grad_sh, N * SH_FLOATS);
   ALLOC(r->grad_cam, 16 * (size_t)c.max_views);
@@ -963,7 +942,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->normal_loss_sums,
                   r->mask_words,
                   r->tile_cut, r->inc_list, r->inc_skip, r->inc_src, r->inc_flag, r->item_key, r->counts2, r->cutw, r->entry_total2,
-                  r->scan_scratch, r->sort_scratch, r->work_counts, r->touched};
+                  r->scan_scratch, r->sort_scratch, r->work_counts};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 5; ++k) {
@@ -1350,7 +1329,6 @@ gs_status gs_train_step(gs_rasterizer* r, const gs_camera* cams, uint32_t nv, ui
   // Chosen form: batched step replayed from a CUDA graph; per-step values
   // (cameras, learning rates, bias corrections) are uploaded before replay.
   s = cut_refresh(r, nv, n, st);
-  if (!s) s = ensure_geom_clean(r, st);
   if (s) return s;
   r->t += 1;
   DynParams dp{};
@@ -1407,7 +1385,6 @@ gs_status gs_train_step_profiled(gs_rasterizer* r, const gs_camera* cams, uint32
     s = plain_body(r, nv, n, cfg, st, &prof);
   } else {
     s = cut_refresh(r, nv, n, st);
-    if (!s) s = ensure_geom_clean(r, st);
     if (s) return s;
     r->t += 1;
     DynParams dp{};

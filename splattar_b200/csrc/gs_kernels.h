@@ -59,11 +59,6 @@ struct ProjectBwdArgs {
   // (units: warps of the plain kernel, blocks of the fused one), summed in
   // unit order by launch_cam_reduce; null: added into grad_cam by atomics.
   float* cam_partials;
-  // Fused kernel, atomic mode (optional): only items marked in touched (one
-  // bit per item) have a record gradient to read; each one read is zeroed
-  // (its 16 colour-path components), so grad_geom is all zero again after
-  // the launch.
-  const uint32_t* touched;
 };
 
 struct AdamClass {
@@ -106,9 +101,6 @@ struct RasterArgs {
   const float4* dl_dnormal;
   float* grad_geom;
   float* partials;
-  // Optional (atomic mode): bit item of touched[item / 32] is set for every
-  // item the backward adds a record gradient to.
-  uint32_t* touched;
   float lambda_dist;
   uint32_t* tile_counter;       // persistent kernels: zeroed before each launch
   const uint32_t* tile_order;   // persistent kernels: the tile taken at each counter value (null: identity)

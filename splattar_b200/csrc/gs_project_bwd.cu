@@ -442,18 +442,7 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
   const uint32_t i1 = i0 + (uint32_t)sl1;
   const bool active1 = v1 < V && i1 < a.n;
   float G[GG_STRIDE];
-  bool gnz = false;
-  if (active1) {
-    const uint32_t item = (uint32_t)v1 * a.n + i1;
-    if (a.touched == nullptr || a.partials != nullptr) {
-      gnz = load_G<AUX>(a, item, G);
-    } else if ((__ldg(a.touched + (item >> 5)) >> (item & 31u)) & 1u) {
-      gnz = load_G<AUX>(a, item, G);
-      float4* gp = reinterpret_cast<float4*>(const_cast<float*>(a.grad_geom) + (size_t)item * GG_STRIDE);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) gp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  }
+  const bool gnz = active1 && load_G<AUX>(a, (uint32_t)v1 * a.n + i1, G);
   if (tid == 0) mbar_init(&s_bar);
   __syncthreads();
   if (tid == 0) {

@@ -256,6 +256,46 @@ __device__ __forceinline__ void flush_row_groups(uint32_t (&gcur)[GPL], uint32_t
   }
 }
 
+// Occlusion-cut bookkeeping of a tile at the end of a persistent colour-only
+// forward pass (one thread): `complete` when every pixel terminated, `walk`
+// the tile's largest contributor count. A truncated list that ran out first
+// is listed for the completion pass; otherwise the tile's next cut is
+// recorded.
+__device__ __forceinline__ void cut_tile_end(const RasterArgs& a, int tile, uint2 range, bool complete,
+                                             uint32_t walk) {
+  const uint32_t used = a.cut_pass == 1 ? a.tile_cut[tile] : 0xffffffffu;
+  const uint32_t len = range.y - range.x;
+  if (!complete && used != 0xffffffffu) {
+    // the truncated list ran out first: the completion pass continues the tile
+    a.inc_flag[tile] = 1u;
+    const uint32_t slot = atomicAdd(a.inc_count, 1u);
+    a.inc_list[slot] = (uint32_t)tile;
+    a.inc_skip[slot] = len;
+    a.inc_src[slot] = range.x;
+  } else {
+    // next cut: the depth key at list position walk + walk/4 + 32 (the last
+    // contributor plus a margin for the next step's changes). A truncated list
+    // shorter than that extends its cut past its last key by the key span from
+    // the last contributor to the list's end (at least 2^14 units in the last
+    // place, about 0.2 % of depth).
+    uint32_t next = 0xffffffffu;
+    if (complete) {
+      const uint32_t keep = walk + walk / 4u + 32u;
+      if (keep < len) {
+        next = __ldg(a.item_key + a.sorted_pairs[range.x + keep - 1u].y);
+      } else if (used == 0xffffffffu || walk == 0u || len == 0u) {
+        next = used;
+      } else {
+        const uint32_t kl = __ldg(a.item_key + a.sorted_pairs[range.y - 1u].y);
+        const uint32_t kw = __ldg(a.item_key + a.sorted_pairs[range.x + walk - 1u].y);
+        const uint32_t span = max(kl - kw, 1u << 14);
+        next = kl < 0x7f7fffffu - span ? kl + span : 0x7f7fffffu;
+      }
+    }
+    a.tile_cut[tile] = next;
+  }
+}
+
 // COLOR: colour, alpha and final transmittance only (the training step's
 // loss reads nothing else); depth and normal are neither accumulated nor
 // written.
@@ -521,39 +561,7 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
     }
     if (a.tile_cut != nullptr) {  // occlusion cut bookkeeping (set together with tile_walk)
       const bool complete = __syncthreads_count(tdone) == NT;  // every pixel terminated
-      if (tid == 0) {
-        const uint32_t used = a.cut_pass == 1 ? a.tile_cut[tile] : 0xffffffffu;
-        const uint32_t len = range.y - range.x;
-        if (!complete && used != 0xffffffffu) {
-          // the truncated list ran out first: the completion pass continues the tile
-          a.inc_flag[tile] = 1u;
-          const uint32_t slot = atomicAdd(a.inc_count, 1u);
-          a.inc_list[slot] = (uint32_t)tile;
-          a.inc_skip[slot] = len;
-          a.inc_src[slot] = range.x;
-        } else {
-          // next cut: the depth key at list position walk + walk/4 + 32 (the
-          // last contributor plus a margin for the next step's changes). A
-          // truncated list shorter than that extends its cut past its last
-          // key by the key span from the last contributor to the list's end
-          // (at least 2^14 units in the last place, about 0.2 % of depth).
-          uint32_t next = 0xffffffffu;
-          if (complete) {
-            const uint32_t walk = s_walk, keep = walk + walk / 4u + 32u;
-            if (keep < len) {
-              next = __ldg(a.item_key + a.sorted_pairs[range.x + keep - 1u].y);
-            } else if (used == 0xffffffffu || walk == 0u || len == 0u) {
-              next = used;
-            } else {
-              const uint32_t kl = __ldg(a.item_key + a.sorted_pairs[range.y - 1u].y);
-              const uint32_t kw = __ldg(a.item_key + a.sorted_pairs[range.x + walk - 1u].y);
-              const uint32_t span = max(kl - kw, 1u << 14);
-              next = kl < 0x7f7fffffu - span ? kl + span : 0x7f7fffffu;
-            }
-          }
-          a.tile_cut[tile] = next;
-        }
-      }
+      if (tid == 0) cut_tile_end(a, tile, range, complete, s_walk);
     }
     if (!PERSIST) return;
     __syncthreads();
@@ -617,7 +625,6 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
       reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[q4] = make_float4(s0, s1, s2, s3);
     } else if (s0 != 0.f || s1 != 0.f || s2 != 0.f || s3 != 0.f) {
       red_add_v4(a.grad_geom + (size_t)s_item[k] * GG_STRIDE + 4 * q4, s0, s1, s2, s3);
-      if (!DIRECT && a.touched != nullptr) atomicOr(a.touched + (s_item[k] >> 5), 1u << (s_item[k] & 31u));
     }
   };
   auto emit_zero = [&](int k) {
@@ -908,8 +915,6 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
             const float r1 = __shfl_down_sync(FULL, r, 2), r2 = __shfl_down_sync(FULL, r, 4);
             const float r3 = __shfl_down_sync(FULL, r, 6);
             if ((lane & 7) == 0) emit4(k, lane >> 3, r, r1, r2, r3);
-            if (!DET && a.touched != nullptr && __ballot_sync(FULL, r != 0.f) && lane == 0)
-              atomicOr(a.touched + (s_item[k] >> 5), 1u << (s_item[k] & 31u));
           } else {
             if (!(lane & 1)) s_part[warp][k][lane >> 1] = r;
           }
@@ -1006,6 +1011,361 @@ __global__ void __launch_bounds__(256) k_raster_work(RasterArgs a, unsigned long
   if (threadIdx.x < 4) atomicAdd(out + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
+// ---------------------------------------------------------------------------
+// Pixel-compacted raster kernels: 16-pixel tiles, colour-only, persistent (the
+// chosen training step). One warp owns a tile and keeps its per-pixel state in
+// shared memory; for each staged entry it spreads the pixels of the entry's
+// α-box ∩ tile (the only pixels whose α can reach 1/255) over its 32 lanes,
+// so lanes do not idle on pixels the entry cannot touch. Entries are
+// processed one after another, so each pixel still composites (or is walked
+// back) in list order. The hit test and compositing are the same operations
+// as in k_raster_fwd / k_raster_bwd: images, final T and contributor indices
+// are bit-identical, and gradients equal up to the order of float sums.
+constexpr int PX_TP = 256;  // pixels per tile
+constexpr int PX_NB = 32;   // staged entries per round: one per lane
+
+// Tile-local pixel rectangle of an α-box ∩ the tile's in-image pixels
+// (columns < tw, rows < th), packed x0 | x1 << 8 | y0 << 16 | y1 << 24;
+// 0xffffffff when empty. Same pixel decisions as the per-pixel box test.
+__device__ __forceinline__ uint32_t px_rect(const float4& b, float bx0, float by0, int tw, int th) {
+  const uint32_t cm = span_bits<16>(bx0, b.x, b.y) & ((1u << tw) - 1u);
+  const uint32_t rm = span_bits<16>(by0, b.z, b.w) & ((1u << th) - 1u);
+  if (!cm || !rm) return 0xffffffffu;
+  const uint32_t x0 = (uint32_t)(__ffs(cm) - 1), x1 = 31u - (uint32_t)__clz(cm);
+  const uint32_t y0 = (uint32_t)(__ffs(rm) - 1), y1 = 31u - (uint32_t)__clz(rm);
+  return x0 | (x1 << 8) | (y0 << 16) | (y1 << 24);
+}
+
+struct PxTile {
+  int tile;
+  uint32_t slot;
+  int W, tw, th;
+  float bx0, by0;
+  long long pbase;  // pixel (x0, y0) of the tile in per-pixel buffers
+};
+
+// Takes the next tile from the persistent queue (all lanes); false when done.
+// Writes the tile's column and row ray components into s_sx / s_sy exactly
+// as tile_geo computes them.
+__device__ __forceinline__ bool px_next_tile(const RasterArgs& a, PxTile& t, float* s_sx, float* s_sy) {
+  const int lane = threadIdx.x;
+  uint32_t slot = 0;
+  int tile = 0;
+  if (lane == 0) {
+    slot = atomicAdd(a.tile_counter, 1u);
+    const uint32_t lim = a.tile_limit != nullptr ? *a.tile_limit : (uint32_t)a.total_tiles;
+    tile = slot >= lim ? a.total_tiles : (int)(a.tile_order != nullptr ? __ldg(a.tile_order + slot) : slot);
+  }
+  t.tile = __shfl_sync(FULL, tile, 0);
+  t.slot = __shfl_sync(FULL, slot, 0);
+  if (t.tile >= a.total_tiles) return false;
+  int v = 0;
+  while (v + 1 < a.n_views && t.tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
+  const ViewInfo* V = a.views + v;
+  const int tiles_x = __ldg(&V->tiles_x), H = __ldg(&V->height);
+  t.W = __ldg(&V->width);
+  const int lt = t.tile - __ldg(&V->tile_base);
+  const int x0 = (lt % tiles_x) * 16, y0 = (lt / tiles_x) * 16;
+  t.tw = min(16, t.W - x0);
+  t.th = min(16, H - y0);
+  const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
+  if (lane < 16) {
+    const float pxc = (float)(x0 + lane) + 0.5f;
+    s_sx[lane] = -((pxc - cx) / f);
+  } else {
+    const float pyc = (float)(y0 + lane - 16) + 0.5f;
+    s_sy[lane - 16] = (pyc - cy) / f;
+  }
+  t.bx0 = (float)x0 + 0.5f;
+  t.by0 = (float)y0 + 0.5f;
+  t.pbase = __ldg(&V->pix_base) + (long long)y0 * t.W + x0;
+  return true;
+}
+
+// Stages up to 32 entries of [j0, j1): each lane takes one, culls it by its
+// α-box (and by an empty row-group summary when gm_mask), and the kept ones are
+// compacted in list order into the shared arrays. Returns the number kept.
+// In the deterministic backward (s_q given) every entry not kept gets its
+// ordered zero partial here.
+template <int PREC, bool DET>
+__device__ __forceinline__ int px_stage(const RasterArgs& a, const PxTile& t, uint32_t j0, uint32_t j1,
+                                        uint32_t rstart, bool use_gm, float4* s_r0, float4* s_r1, float4* s_r2,
+                                        float4* s_r3, uint32_t* s_rect, uint32_t* s_j, uint32_t* s_item,
+                                        uint32_t* s_q, uint8_t* s_gm) {
+  const int lane = threadIdx.x;
+  const uint32_t j = j0 + (uint32_t)lane;
+  uint32_t item = 0, q = 0, rect = 0xffffffffu;
+  uint32_t gm = 0xffu;
+  if (j < j1) {
+    q = __ldg(&a.sorted_pairs[j].y);
+    item = DET ? __ldg(&a.exp_item[q]) : q;
+    if (use_gm) gm = __ldg(a.gmask + j);
+    if (gm) {
+      rect = px_rect(load_record_box<PREC>(a.records, item), t.bx0, t.by0, t.tw, t.th);
+      if (use_gm && rect != 0xffffffffu) {  // rows of the 4-row groups with a contributor
+        const uint32_t g0 = (uint32_t)(__ffs(gm) - 1), g1 = 31u - (uint32_t)__clz(gm);
+        const uint32_t y0 = max((rect >> 16) & 255u, 4u * g0), y1 = min(rect >> 24, 4u * g1 + 3u);
+        rect = y0 <= y1 ? (rect & 0xffffu) | (y0 << 16) | (y1 << 24) : 0xffffffffu;
+      }
+    }
+    if (DET && s_q != nullptr && rect == 0xffffffffu) {  // no contribution: an ordered zero partial
+      float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)q * GG_STRIDE);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  const bool keep = rect != 0xffffffffu;
+  const unsigned bal = __ballot_sync(FULL, keep);
+  if (keep) {
+    const int sl = __popc(bal & lanemask_lt());
+    float4 r0, r1, r2, r3;
+    load_record4<PREC>(a.records, item, r0, r1, r2, r3);
+    s_r0[sl] = r0; s_r1[sl] = r1; s_r2[sl] = r2; s_r3[sl] = r3;
+    s_rect[sl] = rect;
+    s_j[sl] = j - rstart;
+    if (s_item) s_item[sl] = item;
+    if (DET && s_q) s_q[sl] = q;
+    if (s_gm) s_gm[sl] = (uint8_t)gm;
+  }
+  __syncwarp();
+  return __popc(bal);
+}
+
+template <int PREC, bool DET>
+__global__ void __launch_bounds__(32) k_raster_fwd_px(RasterArgs a) {
+  __shared__ float s_T[PX_TP];
+  __shared__ float4 s_c[PX_TP];
+  __shared__ uint32_t s_nc[PX_TP];
+  __shared__ float s_sx[16], s_sy[16];
+  __shared__ float4 s_r0[PX_NB], s_r1[PX_NB], s_r2[PX_NB], s_r3[PX_NB];
+  __shared__ uint32_t s_rect[PX_NB], s_j[PX_NB];
+  const int lane = threadIdx.x;
+  const bool gm_on = a.gmask != nullptr;
+  PxTile t;
+  while (px_next_tile(a, t, s_sx, s_sy)) {
+    const uint2 range = __ldg(&a.ranges[t.tile]);
+    // Completion pass of the occlusion cut: continue after the entries pass 1
+    // composited, from the pixel state it wrote.
+    const bool resume = a.cut_pass == 2;
+    uint32_t skip = 0;
+    if (resume) {
+      skip = a.inc_skip[t.slot];
+      if (range.y - range.x < skip) skip = 0;  // list not rebuilt (entry capacity error already flagged)
+    }
+    int alive = 0;
+    uint32_t walk = 0;
+    for (int p = lane; p < PX_TP; p += 32) {
+      const int ly = p >> 4, lx = p & 15;
+      float T = 0.f;  // pixels outside the image count as terminated
+      float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+      uint32_t nc = 0;
+      if (lx < t.tw && ly < t.th) {
+        T = 1.f;
+        if (resume) {
+          const long long pix = t.pbase + (long long)ly * t.W + lx;
+          c = a.out_color[pix];
+          T = a.out_aux[pix].x;
+          nc = a.out_nc[pix];
+        }
+        if (!(T < T_TERMINATE)) ++alive;
+      }
+      s_T[p] = T;
+      s_c[p] = c;
+      s_nc[p] = nc;
+      walk = max(walk, nc);
+    }
+    alive = __reduce_add_sync(FULL, alive);
+    walk = __reduce_max_sync(FULL, walk);
+    __syncwarp();
+    for (uint32_t base = range.x + skip; base < range.y && alive > 0; base += PX_NB) {
+      const int kept = px_stage<PREC, DET>(a, t, base, min(base + (uint32_t)PX_NB, range.y), range.x, false, s_r0,
+                                           s_r1, s_r2, s_r3, s_rect, s_j, nullptr, nullptr, nullptr);
+      for (int k = 0; k < kept; ++k) {
+        const uint32_t rc = s_rect[k];
+        const int rx0 = (int)(rc & 255u), rx1 = (int)((rc >> 8) & 255u), ry0 = (int)((rc >> 16) & 255u);
+        const int w = rx1 - rx0 + 1, cnt = w * ((int)(rc >> 24) - ry0 + 1);
+        const int rw = (4096 + w - 1) / w;  // q / w = (q·rw) >> 12 exactly for q < 256, w <= 16
+        const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
+        const uint32_t idx1 = s_j[k] + 1u;
+        uint32_t gbits = 0;
+        int nd = 0;
+        for (int q = lane; q < cnt; q += 32) {
+          const int dy = (q * rw) >> 12, ly = ry0 + dy, lx = rx0 + q - dy * w;
+          const int p = ly * 16 + lx;
+          const float T = s_T[p];
+          if (T < T_TERMINATE) continue;
+          const float pxc = t.bx0 + (float)lx, pyc = t.by0 + (float)ly;
+          const ColPart cp = col_part(r0, r1, r2, s_sx[lx], pxc);
+          const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, s_sy[ly], pyc);
+          const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
+          if (alpha < ALPHA_SKIP) continue;
+          const float wt = T * alpha;
+          float4 c = s_c[p];
+          c.x += r3.x * wt; c.y += r3.y * wt; c.z += r3.z * wt;
+          c.w += wt;
+          const float Tn = __fmul_rn(T, 1.0f - alpha);
+          s_c[p] = c;
+          s_T[p] = Tn;
+          s_nc[p] = idx1;
+          gbits |= 1u << (ly >> 2);
+          if (Tn < T_TERMINATE) ++nd;
+        }
+        const uint32_t gm = __reduce_or_sync(FULL, gbits);
+        alive -= __reduce_add_sync(FULL, nd);
+        if (gm) walk = idx1;  // entries come in list order: the latest contributor is the deepest
+        if (gm_on && lane == 0) a.gmask[range.x + idx1 - 1u] = (uint8_t)gm;
+        __syncwarp();
+        if (alive <= 0) break;
+      }
+    }
+    for (int p = lane; p < PX_TP; p += 32) {
+      const int ly = p >> 4, lx = p & 15;
+      if (lx < t.tw && ly < t.th) {
+        const long long pix = t.pbase + (long long)ly * t.W + lx;
+        a.out_color[pix] = s_c[p];
+        a.out_aux[pix].x = s_T[p];
+        a.out_nc[pix] = s_nc[p];
+      }
+    }
+    if (lane == 0) {
+      if (a.tile_walk != nullptr) a.tile_walk[t.tile] = walk;
+      if (a.tile_cut != nullptr) cut_tile_end(a, t.tile, range, alive <= 0, walk);
+    }
+    __syncwarp();
+  }
+}
+
+template <int PREC, bool DET>
+__global__ void __launch_bounds__(32) k_raster_bwd_px(RasterArgs a) {
+  __shared__ float s_T[PX_TP], s_suf[PX_TP];
+  __shared__ uint32_t s_nc[PX_TP];
+  __shared__ float4 s_dlc[PX_TP];
+  __shared__ float s_sx[16], s_sy[16];
+  __shared__ float4 s_r0[PX_NB], s_r1[PX_NB], s_r2[PX_NB], s_r3[PX_NB];
+  __shared__ uint32_t s_rect[PX_NB], s_j[PX_NB], s_item[PX_NB];
+  __shared__ uint32_t s_q[DET ? PX_NB : 1];
+  __shared__ uint8_t s_gm[PX_NB];
+  const int lane = threadIdx.x;
+  const bool use_gm = a.gmask != nullptr;
+  PxTile t;
+  while (px_next_tile(a, t, s_sx, s_sy)) {
+    const uint2 range = __ldg(&a.ranges[t.tile]);
+    if (range.y <= range.x) continue;
+    uint32_t mx = 0;
+    for (int p = lane; p < PX_TP; p += 32) {
+      const int ly = p >> 4, lx = p & 15;
+      float T = 1.f;
+      uint32_t nc = 0;
+      float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (lx < t.tw && ly < t.th) {
+        const long long pix = t.pbase + (long long)ly * t.W + lx;
+        g = a.dl_dcolor[pix];
+        T = a.out_aux[pix].x;
+        nc = a.out_nc[pix];
+        if (g.x == 0.f && g.y == 0.f && g.z == 0.f) nc = 0;  // no loss at the pixel: nothing to walk
+      }
+      s_T[p] = T;
+      s_suf[p] = 0.f;
+      s_nc[p] = nc;
+      s_dlc[p] = g;
+      mx = max(mx, nc);
+    }
+    const uint32_t maxnc = min(__reduce_max_sync(FULL, mx), range.y - range.x);
+    if (DET) {  // entries past the tile's last contributor get zero partials
+      for (uint32_t e = range.x + maxnc + (uint32_t)lane; e < range.y; e += 32) {
+        float4* pp = reinterpret_cast<float4*>(a.partials + (size_t)__ldg(&a.sorted_pairs[e].y) * GG_STRIDE);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) pp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+    __syncwarp();
+    uint32_t hi = range.x + maxnc;
+    while (hi > range.x) {
+      const uint32_t lo = hi - range.x > (uint32_t)PX_NB ? hi - PX_NB : range.x;
+      const int kept = px_stage<PREC, DET>(a, t, lo, hi, range.x, use_gm, s_r0, s_r1, s_r2, s_r3, s_rect, s_j, s_item,
+                                           DET ? s_q : nullptr, s_gm);
+      for (int k = kept - 1; k >= 0; --k) {
+        const uint32_t rc = s_rect[k];
+        const int rx0 = (int)(rc & 255u), rx1 = (int)((rc >> 8) & 255u), ry0 = (int)((rc >> 16) & 255u);
+        const int w = rx1 - rx0 + 1, cnt = w * ((int)(rc >> 24) - ry0 + 1);
+        const int rw = (4096 + w - 1) / w;
+        const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
+        const uint32_t cidx = s_j[k];
+        const uint32_t gm = s_gm[k];
+        float gg[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) gg[c] = 0.f;
+        bool contrib = false;
+        for (int q = lane; q < cnt; q += 32) {
+          const int dy = (q * rw) >> 12, ly = ry0 + dy, lx = rx0 + q - dy * w;
+          if (!((gm >> (ly >> 2)) & 1u)) continue;
+          const int p = ly * 16 + lx;
+          if (cidx >= s_nc[p]) continue;
+          const float sx = s_sx[lx], sy = s_sy[ly];
+          const float pxc = t.bx0 + (float)lx, pyc = t.by0 + (float)ly;
+          const ColPart cp = col_part(r0, r1, r2, sx, pxc);
+          const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, sy, pyc);
+          const float raw_alpha = __fmul_rn(r3.w, h.ghat);
+          const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
+          if (alpha < ALPHA_SKIP) continue;
+          contrib = true;
+          const float inv_oma = rcp_approx(1.0f - alpha);
+          const float t_before = s_T[p] * inv_oma;
+          const float wt = t_before * alpha;
+          const float4 g4 = s_dlc[p];
+          const float dc = g4.x * r3.x + g4.y * r3.y + g4.z * r3.z;
+          const float suf = s_suf[p];
+          const float dl_dalpha = dc * t_before - suf * inv_oma;
+          s_suf[p] = suf + dc * wt;
+          s_T[p] = t_before;
+          gg[11] += g4.x * wt; gg[12] += g4.y * wt; gg[13] += g4.z * wt;
+          if (raw_alpha <= ALPHA_CLAMP) {
+            const float dg = dl_dalpha * h.ghat;
+            gg[14] += dg;
+            const float K = dg * r3.w;
+            if (h.ray) {
+              // record moments sum over the pixel ray s = (sx, sy, 1) of the
+              // ray-branch adjoints (see k_raster_bwd)
+              const float Ki = K * h.inv_det;
+              const float gu = -h.u * Ki, gv = -h.v * Ki, gdet = h.q2 * Ki;
+              const float2 s2 = make_float2(sx, sy);
+              const float2 m0 = __ffma2_rn(make_float2(gdet, gdet), s2, make_float2(gg[0], gg[1]));
+              const float2 m1 = __ffma2_rn(make_float2(gu, gu), s2, make_float2(gg[3], gg[4]));
+              const float2 m2 = __ffma2_rn(make_float2(gv, gv), s2, make_float2(gg[6], gg[7]));
+              gg[0] = m0.x; gg[1] = m0.y; gg[3] = m1.x; gg[4] = m1.y; gg[6] = m2.x; gg[7] = m2.y;
+              gg[2] += gdet; gg[5] += gu; gg[8] += gv;
+            } else {
+              const float kk = K * (1.0f / LOWPASS_SIGMA2);
+              const float2 sd = __ffma2_rn(make_float2(cp.dx, h.dy), make_float2(kk, kk), make_float2(gg[9], gg[10]));
+              gg[9] = sd.x;
+              gg[10] = sd.y;
+            }
+          }
+        }
+        __syncwarp();
+        if (__any_sync(FULL, contrib)) {
+          const float r = warp_reduce16(gg);
+          // component c sits in lanes 2c and 2c+1: lane 8q gathers 4q..4q+3
+          const float u1 = __shfl_down_sync(FULL, r, 2), u2 = __shfl_down_sync(FULL, r, 4);
+          const float u3 = __shfl_down_sync(FULL, r, 6);
+          if ((lane & 7) == 0) {
+            const int q4 = lane >> 3;
+            if (DET) {
+              reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[q4] = make_float4(r, u1, u2, u3);
+            } else if (r != 0.f || u1 != 0.f || u2 != 0.f || u3 != 0.f) {
+              red_add_v4(a.grad_geom + (size_t)s_item[k] * GG_STRIDE + 4 * q4, r, u1, u2, u3);
+            }
+          }
+        } else if (DET && lane < 4) {
+          reinterpret_cast<float4*>(a.partials + (size_t)s_q[k] * GG_STRIDE)[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      hi = lo;
+    }
+    __syncwarp();
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- dispatch
@@ -1070,8 +1430,25 @@ bool by_prec(int prec, G&& g) {
 // Calls f(kernel, threads) with the forward kernel of these options, or
 // returns false when the combination is not built. Contributor masks exist
 // for TS 16 only; the colour-only variant is persistent.
+// Launch shape (32, 0) on 16-pixel tiles selects the pixel-compacted kernels,
+// which exist for the colour-only persistent passes without contributor
+// masks; elsewhere that shape stands for (64, 4) forward and (64, 8) backward.
 template <int TS, typename F>
 bool fwd_kernel(int prec, int batch, int ppt, bool det, bool persistent, bool color, bool mask, F&& f) {
+  if constexpr (TS == 16) {
+    if (ppt == 0 && batch == PX_NB) {
+      if (color && persistent && !mask) {
+        return by_prec(prec, [&](auto pc) -> bool {
+          constexpr int P = decltype(pc)::value;
+          if (det) f(k_raster_fwd_px<P, true>, 32);
+          else f(k_raster_fwd_px<P, false>, 32);
+          return true;
+        });
+      }
+      batch = 64;
+      ppt = 4;
+    }
+  }
   return by_prec(prec, [&](auto pc) -> bool {
     constexpr int P = decltype(pc)::value;
     if (color) {
@@ -1096,6 +1473,20 @@ bool fwd_kernel(int prec, int batch, int ppt, bool det, bool persistent, bool co
 
 template <int TS, typename F>
 bool bwd_kernel(int prec, bool aux, int batch, int ppt, bool det, bool persistent, bool mask, F&& f) {
+  if constexpr (TS == 16) {
+    if (ppt == 0 && batch == PX_NB) {
+      if (!aux && persistent && !mask) {
+        return by_prec(prec, [&](auto pc) -> bool {
+          constexpr int P = decltype(pc)::value;
+          if (det) f(k_raster_bwd_px<P, true>, 32);
+          else f(k_raster_bwd_px<P, false>, 32);
+          return true;
+        });
+      }
+      batch = 64;
+      ppt = 8;
+    }
+  }
   if (aux) {  // one shape per tile size with aux losses
     batch = 32;
     ppt = TS == 32 ? 4 : 1;

@@ -165,9 +165,10 @@ def test_cut_is_off_where_documented():
 
 def test_chosen_forward_launch_shapes_agree():
     """The colour-only forward of the training step composites pixel pairs in
-    packed FP32 (2, 4 and 8 pixels per thread) and single pixels in scalar
-    code (1 pixel per thread): every shape gives bit-identical colour, final
-    T and contributor indices."""
+    packed FP32 (2, 4 and 8 pixels per thread), single pixels in scalar code
+    (1 pixel per thread), or spreads each entry's box over a warp (the
+    pixel-compacted kernel): every shape gives bit-identical colour, final T
+    and contributor indices."""
     s = make_surfels(20_000, 11, True, 3, 0.1)
     cams = ring_cameras(RES)
     P = sum(w * h for w, h in RES)
@@ -175,7 +176,7 @@ def test_chosen_forward_launch_shapes_agree():
     adam.lr = {k: 0.0 for k in adam.lr}
     step = StepSettings(0.8, 0.2, adam, "chosen")
     outs = []
-    for fb, fp in [(64, 1), (128, 2), (64, 4), (64, 8)]:
+    for fb, fp in [(64, 1), (128, 2), (64, 4), (64, 8), (32, 0)]:  # (32, 0): the pixel-compacted kernel
         r = Rasterizer(20_000, 0, 0, 20_000 * len(RES) * 64, max_views=len(RES), max_pixels=P, precision="f16",
                        color_only=True)
         r.upload_scene(s.scene_input())
