@@ -274,9 +274,21 @@ void rotation_of(const float q_in[4], float rot[9]) {
   rot[6] = xz + wy; rot[7] = yz - wx; rot[8] = 1.0f - (xx + yy);
 }
 
+// The same rotation in double (quaternion normalised in double, as the
+// oracle's quat_to_mat does): the projection's accurate surfel centres.
+void rotation64_of(const float q_in[4], double rot[9]) {
+  const double q0 = q_in[0], q1 = q_in[1], q2 = q_in[2], q3 = q_in[3];
+  const double n = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
+  const double x = q0 / n, y = q1 / n, z = q2 / n, w = q3 / n;
+  rot[0] = 1 - 2 * (y * y + z * z); rot[1] = 2 * (x * y + w * z); rot[2] = 2 * (x * z - w * y);
+  rot[3] = 2 * (x * y - w * z); rot[4] = 1 - 2 * (x * x + z * z); rot[5] = 2 * (y * z + w * x);
+  rot[6] = 2 * (x * z + w * y); rot[7] = 2 * (y * z - w * x); rot[8] = 1 - 2 * (x * x + y * y);
+}
+
 ViewInfo make_view(const gs_camera& c, int tile) {
   ViewInfo v{};
   rotation_of(c.quat, v.rot);
+  rotation64_of(c.quat, v.rot64);
   for (int k = 0; k < 3; ++k) v.center[k] = c.center[k];
   v.focal = c.focal;
   v.width = (int)c.width;

@@ -39,17 +39,26 @@ struct ViewInfo {
   int tile_base;      // first global tile id of this view
   int sh_degree;
   long long pix_base; // first pixel of this view in per-pixel buffers
+  double rot64[9];    // R again in double (accurate projected centres, see the record below)
 };
 
 // Projected surfel record ("SurfelCam"), one per (view, surfel). The ray–splat
 // intersection of crates/gs-cpu-ref/src/forward.rs:136-169 solves
 // [τu τv −d](u,v,t)ᵀ = −c by Cramer's rule; with s = −d every triple product
 // is linear in s:  det = s·M,  u·det = s·Bu,  v·det = s·Bv,  t·det = tn, where
-// M = τu×τv, Bu = τv×c, Bv = c×τu, tn = −c·M. Storing M, Bu, Bv, tn makes the
-// per-pixel intersection three 3-term dot products.
-//   r0 = (M, tn)  r1 = (Bu, px)  r2 = (Bv, py)
+// M = τu×τv, Bu = τv×c, Bv = c×τu, tn = −c·M. The ray s_c through the
+// surfel's centre is parallel to c, so Bu·s_c = Bv·s_c = 0 and, for a pixel
+// ray s = s_c + Δs with Δs = (−dx/f, dy/f, 0) (dx, dy: the pixel centre minus
+// the projected centre, in pixels), u·det = Bu·Δs and v·det = Bv·Δs exactly.
+// Evaluating them from the screen offsets avoids the cancellation of s·Bu
+// (|Bu| ~ |c||τ| against u·det ~ |τ|² cosθ for a surfel seen at angle θ to
+// its normal), which in FP32 costs up to ~10 % of a nearly edge-on surfel's
+// gradient; the projected centre is computed in double and kept as hi + lo.
+//   r0 = (M, tn)  r1 = (−Bu.x/f, Bu.y/f, px_lo, px_hi)  r2 = (−Bv.x/f, Bv.y/f, py_lo, py_hi)
 //   r3 = (colour rgb, opacity)  r4 = (normal xyz, centre depth)
 //   bb = pixel box (x0, x1, y0, y1) outside which α < 1/255 for certain
+// Per pixel: det = M·s, u·det = r1.x·dx + r1.y·dy, v·det = r2.x·dx + r2.y·dy,
+// t·det = tn, with dx = (pxc − px_hi) − px_lo, dy = (pyc − py_hi) − py_lo.
 // FP32 record: 6 float4 = 96 B. Mixed-precision record (80 B, 5 float4):
 // geometry r0..r2 and colour/opacity r3 stay FP32 (the geometry feeds a ratio
 // of nearly cancelling dot products; colour and opacity rounded to 16 bits

@@ -189,8 +189,22 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float3 Bu = cross3(tv, c);
   const float3 Bv = cross3(c, tu);
   const float tn = -dot3(c, M);
-  store_record<PREC>(a.records, item, make_float4(M.x, M.y, M.z, tn), make_float4(Bu.x, Bu.y, Bu.z, px),
-                     make_float4(Bv.x, Bv.y, Bv.z, py), make_float4(color.x, color.y, color.z, o),
+  // The projected centre for the hit test, accurate to double: the camera
+  // transform and the perspective division in double (the float px, py above
+  // keep the reference's rect arithmetic), stored as hi + lo.
+  const ViewInfo* V = a.views + v;
+  const double xd = (double)p.x - (double)k.C.x, yd = (double)p.y - (double)k.C.y, zd = (double)p.z - (double)k.C.z;
+  const double cxd = __ldg(&V->rot64[0]) * xd + __ldg(&V->rot64[1]) * yd + __ldg(&V->rot64[2]) * zd;
+  const double cyd = __ldg(&V->rot64[3]) * xd + __ldg(&V->rot64[4]) * yd + __ldg(&V->rot64[5]) * zd;
+  const double czd = __ldg(&V->rot64[6]) * xd + __ldg(&V->rot64[7]) * yd + __ldg(&V->rot64[8]) * zd;
+  const double pxd = (double)k.cx + (double)k.f * cxd / -czd;
+  const double pyd = (double)k.cy - (double)k.f * cyd / -czd;
+  const float pxh = (float)pxd, pyh = (float)pyd;
+  const float pxl = (float)(pxd - (double)pxh), pyl = (float)(pyd - (double)pyh);
+  const float inv_f = 1.0f / k.f;
+  store_record<PREC>(a.records, item, make_float4(M.x, M.y, M.z, tn),
+                     make_float4(-Bu.x * inv_f, Bu.y * inv_f, pxl, pxh),
+                     make_float4(-Bv.x * inv_f, Bv.y * inv_f, pyl, pyh), make_float4(color.x, color.y, color.z, o),
                      make_float4(nrm.x, nrm.y, nrm.z, depth), box);
 }
 

@@ -54,8 +54,9 @@ __device__ __forceinline__ float rcp_approx(float x) {
 }
 
 // The part of the hit test that depends on the pixel column only: a thread's
-// pixels share sx, so det, u·det and v·det are one FMA per pixel from these
-// partial sums, and the screen-space distance needs dy alone.
+// pixels share sx and dx, so det, u·det and v·det are one FMA per pixel from
+// these partial sums, and the screen-space distance needs dy alone. dx is the
+// pixel centre minus the projected centre (hi + lo).
 struct ColPart {
   float det0, un0, vn0, dx, dx2;
 };
@@ -63,9 +64,9 @@ __device__ __forceinline__ ColPart col_part(const float4& r0, const float4& r1, 
                                             float pxc) {
   ColPart c;
   c.det0 = fmaf(r0.x, sx, r0.z);
-  c.un0 = fmaf(r1.x, sx, r1.z);
-  c.vn0 = fmaf(r2.x, sx, r2.z);
-  c.dx = __fsub_rn(pxc, r1.w);
+  c.dx = __fsub_rn(__fsub_rn(pxc, r1.w), r1.z);
+  c.un0 = __fmul_rn(r1.x, c.dx);
+  c.vn0 = __fmul_rn(r2.x, c.dx);
   c.dx2 = __fmul_rn(c.dx, c.dx);
   return c;
 }
@@ -80,15 +81,15 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
   Hit h;
   const float det = fmaf(r0.y, sy, c.det0);
   const float inv = rcp_approx(det);
+  h.dy = __fsub_rn(__fsub_rn(pyc, r2.w), r2.z);
   // (u·det, v·det) and (u, v) as packed pairs, rounding per component as fmaf / __fmul_rn.
-  const float2 uvn = __ffma2_rn(make_float2(r1.y, r2.y), make_float2(sy, sy), make_float2(c.un0, c.vn0));
+  const float2 uvn = __ffma2_rn(make_float2(r1.y, r2.y), make_float2(h.dy, h.dy), make_float2(c.un0, c.vn0));
   const float2 uv = __fmul2_rn(uvn, make_float2(inv, inv));
   const float u = uv.x, v = uv.y;
   const float t = __fmul_rn(r0.w, inv);
   const bool ray_ok = fabsf(det) > 1e-12f && t > NEAR_DEPTH;
   h.q2 = fmaf(u, u, __fmul_rn(v, v));
   const float qr = ray_ok ? __fmul_rn(0.5f, h.q2) : __int_as_float(0x7f800000);
-  h.dy = __fsub_rn(pyc, r2.w);
   const float qs = fmaf(h.dy, h.dy, c.dx2);  // (dx²+dy²)/(2σ²) with σ² = 0.5
   h.ray = qr <= qs;
   const float q = h.ray ? qr : qs;
@@ -107,13 +108,14 @@ __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, co
                                           float depth, float2 sy, float2 pyc, Hit& ha, Hit& hb) {
   const float2 det = __ffma2_rn(make_float2(r0.y, r0.y), sy, make_float2(c.det0, c.det0));
   const float2 inv = make_float2(rcp_approx(det.x), rcp_approx(det.y));
-  const float2 un = __ffma2_rn(make_float2(r1.y, r1.y), sy, make_float2(c.un0, c.un0));
-  const float2 vn = __ffma2_rn(make_float2(r2.y, r2.y), sy, make_float2(c.vn0, c.vn0));
+  // (pyc − py_hi) − py_lo, each step as the scalar __fsub_rn rounds it
+  const float2 dy = __fadd2_rn(__fadd2_rn(pyc, make_float2(-r2.w, -r2.w)), make_float2(-r2.z, -r2.z));
+  const float2 un = __ffma2_rn(make_float2(r1.y, r1.y), dy, make_float2(c.un0, c.un0));
+  const float2 vn = __ffma2_rn(make_float2(r2.y, r2.y), dy, make_float2(c.vn0, c.vn0));
   const float2 u = __fmul2_rn(un, inv), v = __fmul2_rn(vn, inv);
   const float2 t = __fmul2_rn(make_float2(r0.w, r0.w), inv);
   const float2 q2 = __ffma2_rn(u, u, __fmul2_rn(v, v));
   const float2 qr0 = __fmul2_rn(make_float2(0.5f, 0.5f), q2);
-  const float2 dy = __fadd2_rn(pyc, make_float2(-r2.w, -r2.w));  // pyc − r2.w, exactly
   const float2 qs = __ffma2_rn(dy, dy, make_float2(c.dx2, c.dx2));
   const float inf = __int_as_float(0x7f800000);
   const float qra = fabsf(det.x) > 1e-12f && t.x > NEAR_DEPTH ? qr0.x : inf;

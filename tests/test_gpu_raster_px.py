@@ -19,15 +19,15 @@ THREAD = (64, 4, 64, 8)
 CLASSES = (("pos", 4), ("scales", 2), ("quat", 4), ("opacity", 1), ("sh", 48))
 
 
-def _handle(shapes, **kw):
-    s = make_surfels(N, 5, True, 3, 0.1)
-    cams = ring_cameras(RES)
-    P = sum(w * h for w, h in RES)
-    r = Rasterizer(N, 0, 0, N * len(RES) * 64, max_views=len(RES), max_pixels=P, precision="f16", color_only=True,
+def _handle(shapes, n=N, res=RES, **kw):
+    s = make_surfels(n, 5, True, 3, 0.1)
+    cams = ring_cameras(res)
+    P = sum(w * h for w, h in res)
+    r = Rasterizer(n, 0, 0, n * len(res) * 64, max_views=len(res), max_pixels=P, precision="f16", color_only=True,
                    **kw)
     r.upload_scene(s.scene_input())
     r.write("target", np.random.default_rng(9).uniform(0, 1, 4 * P).astype(np.float32))
-    r.optimizer_init(N)
+    r.optimizer_init(n)
     r.set_launch_shapes(*shapes)
     return r, cams, P
 
@@ -79,15 +79,17 @@ def test_px_kernels_deterministic_mode_repeats():
 
 
 def test_px_kernels_with_planted_cuts_equal_full_lists():
-    a, cams, P = _handle(PX)
-    b, _, _ = _handle(PX, full_lists=True)
+    # dense enough for most tiles to terminate (and so record a cut)
+    n, res = 120_000, [(320, 240), (256, 256), (200, 160)]
+    a, cams, P = _handle(PX, n, res)
+    b, _, _ = _handle(PX, n, res, full_lists=True)
     adam = AdamSettings(eps=1e-15)
     adam.lr = {k: 0.0 for k in adam.lr}
     step = StepSettings(0.8, 0.2, adam, "chosen")
     for r in (a, b):
-        r.train_step(cams, N, step)
+        r.train_step(cams, n, step)
     a.check(); b.check()
-    n_tiles = sum(((w + 15) // 16) * ((h + 15) // 16) for w, h in RES)
+    n_tiles = sum(((w + 15) // 16) * ((h + 15) // 16) for w, h in res)
     cut = a.read("tile_cut", n_tiles)
     finite = np.flatnonzero(cut != 0xFFFFFFFF)
     assert finite.size > 20
@@ -97,7 +99,7 @@ def test_px_kernels_with_planted_cuts_equal_full_lists():
     planted[pick[: pick.size // 4]] = 0  # binned empty: rendered entirely by the completion pass
     a.write("tile_cut", planted)
     for r in (a, b):
-        r.train_step(cams, N, step)
+        r.train_step(cams, n, step)
     a.check(); b.check()
     assert int(a.read("incomplete_tiles", 1)[0]) >= pick.size // 4
     oa, ob = _out(a, P), _out(b, P)
