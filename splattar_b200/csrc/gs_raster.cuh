@@ -53,18 +53,28 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
+// A staged record's centre as offsets from the tile's first pixel centre
+// (bx0, by0): r1.w = (bx0 − px_hi) − px_lo, r2.w = (by0 − py_hi) − py_lo, done
+// once per staged entry. A pixel k columns and l rows into the tile then has
+// dx = r1.w + k and dy = r2.w + l: one add each, computed the same way by
+// every kernel, so forward and backward evaluate bit-identical hits.
+__device__ __forceinline__ void stage_offsets(float4& r1, float4& r2, float bx0, float by0) {
+  r1.w = __fsub_rn(__fsub_rn(bx0, r1.w), r1.z);
+  r2.w = __fsub_rn(__fsub_rn(by0, r2.w), r2.z);
+}
+
 // The part of the hit test that depends on the pixel column only: a thread's
 // pixels share sx and dx, so det, u·det and v·det are one FMA per pixel from
-// these partial sums, and the screen-space distance needs dy alone. dx is the
-// pixel centre minus the projected centre (hi + lo).
+// these partial sums, and the screen-space distance needs dy alone. kx is the
+// pixel's column within the tile (records staged with stage_offsets).
 struct ColPart {
   float det0, un0, vn0, dx, dx2;
 };
 __device__ __forceinline__ ColPart col_part(const float4& r0, const float4& r1, const float4& r2, float sx,
-                                            float pxc) {
+                                            float kx) {
   ColPart c;
   c.det0 = fmaf(r0.x, sx, r0.z);
-  c.dx = __fsub_rn(__fsub_rn(pxc, r1.w), r1.z);
+  c.dx = __fadd_rn(r1.w, kx);
   c.un0 = __fmul_rn(r1.x, c.dx);
   c.vn0 = __fmul_rn(r2.x, c.dx);
   c.dx2 = __fmul_rn(c.dx, c.dx);
@@ -77,11 +87,11 @@ __device__ __forceinline__ ColPart col_part(const float4& r0, const float4& r1, 
 // (|det| ≤ 1e-12 or t ≤ near) q_ray is +inf and u, v, t are unused.
 // q2 = u² + v² (= 2·q_ray) is kept for the backward.
 __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
-                                        float depth, float sy, float pyc) {
+                                        float depth, float sy, float ky) {
   Hit h;
   const float det = fmaf(r0.y, sy, c.det0);
   const float inv = rcp_approx(det);
-  h.dy = __fsub_rn(__fsub_rn(pyc, r2.w), r2.z);
+  h.dy = __fadd_rn(r2.w, ky);
   // (u·det, v·det) and (u, v) as packed pairs, rounding per component as fmaf / __fmul_rn.
   const float2 uvn = __ffma2_rn(make_float2(r1.y, r2.y), make_float2(h.dy, h.dy), make_float2(c.un0, c.vn0));
   const float2 uv = __fmul2_rn(uvn, make_float2(inv, inv));
@@ -105,11 +115,10 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
 // Each component rounds exactly as the scalar operation of eval_hit, so
 // either form gives bit-identical results for a pixel.
 __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
-                                          float depth, float2 sy, float2 pyc, Hit& ha, Hit& hb) {
+                                          float depth, float2 sy, float2 ky, Hit& ha, Hit& hb) {
   const float2 det = __ffma2_rn(make_float2(r0.y, r0.y), sy, make_float2(c.det0, c.det0));
   const float2 inv = make_float2(rcp_approx(det.x), rcp_approx(det.y));
-  // (pyc − py_hi) − py_lo, each step as the scalar __fsub_rn rounds it
-  const float2 dy = __fadd2_rn(__fadd2_rn(pyc, make_float2(-r2.w, -r2.w)), make_float2(-r2.z, -r2.z));
+  const float2 dy = __fadd2_rn(make_float2(r2.w, r2.w), ky);  // as eval_hit's __fadd_rn, per component
   const float2 un = __ffma2_rn(make_float2(r1.y, r1.y), dy, make_float2(c.un0, c.un0));
   const float2 vn = __ffma2_rn(make_float2(r2.y, r2.y), dy, make_float2(c.vn0, c.vn0));
   const float2 u = __fmul2_rn(un, inv), v = __fmul2_rn(vn, inv);
@@ -149,8 +158,8 @@ template <int PPT>
 struct TileGeo {
   int W, H;
   long long row0;               // pix_base + y(p=0)·W + x
-  float pxc, sx;
-  float pyc[PPT], sy[PPT];
+  float pxc, sx, kx;                 // kx: column within the tile
+  float pyc[PPT], sy[PPT], ky[PPT];   // ky: rows within the tile
   bool inside[PPT];
   float bx0, bx1, by0, by1;     // pixel-centre extent of the tile's in-image pixels
 };
@@ -170,10 +179,12 @@ __device__ __forceinline__ TileGeo<PPT> tile_geo(const RasterArgs& a, int tile) 
   const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
   g.pxc = (float)x + 0.5f;
   g.sx = -((g.pxc - cx) / f);  // s = −d
+  g.kx = (float)(x - x0);
 #pragma unroll
   for (int p = 0; p < PPT; ++p) {
     g.pyc[p] = (float)(yb + p) + 0.5f;
     g.sy[p] = (g.pyc[p] - cy) / f;
+    g.ky[p] = (float)(yb + p - y0);
     g.inside[p] = x < g.W && yb + p < g.H;
   }
   g.row0 = __ldg(&V->pix_base) + (long long)yb * g.W + x;
@@ -301,8 +312,14 @@ __device__ __forceinline__ void cut_tile_end(const RasterArgs& a, int tile, uint
 // COLOR: colour, alpha and final transmittance only (the training step's
 // loss reads nothing else); depth and normal are neither accumulated nor
 // written.
+// Resident two-warp forward CTAs per SM that the register allocation must
+// allow (1: the compiler's choice).
+#ifndef GS_FWD_2WARP_CTAS
+#define GS_FWD_2WARP_CTAS 1
+#endif
 template <int TS, int BATCH, int PREC, bool DET, bool PERSIST, int PPT, bool COLOR = false, bool MASK = false>
-__global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
+__global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_2WARP_CTAS : 1)
+    k_raster_fwd(RasterArgs a) {
   static_assert(!MASK || COLOR, "contributor masks belong to the colour-only variant");
   using L = Layout<TS, PPT>;
   constexpr int NT = L::NT, NW = NT / 32, TP = TS * TS;
@@ -410,9 +427,12 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
           float4 r0, r1, r2, r3, r4;
           if (COLOR) load_record4<PREC>(a.records, item, r0, r1, r2, r3);
           else load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
+          stage_offsets(r1, r2, g.bx0, g.by0);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (!COLOR) s_r4[slot] = r4;
-          s_bb[slot] = bb;
+          // the box in tile-local pixel coordinates (its 1-pixel margin covers
+          // the rounding of the shift)
+          s_bb[slot] = make_float4(bb.x - g.bx0, bb.y - g.bx0, bb.z - g.by0, bb.w - g.by0);
           s_j[slot] = j;
         }
         kept += kr;
@@ -428,12 +448,12 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
         for (; k < kept; ++k) {
           const uint32_t kbit = 1u << (k & 31);
           const float4 bbk = s_bb[k];
-          if (!tdone && g.pxc >= bbk.x && g.pxc <= bbk.y) {
+          if (!tdone && g.kx >= bbk.x && g.kx <= bbk.y) {
             const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
             const float4 r3 = s_r3[k];
             const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
             const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
-            const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
+            const ColPart cp = col_part(r0, r1, r2, g.sx, g.kx);
             constexpr int PS = PPT >= 2 ? 2 : 1;  // pixels per hit evaluation
 #pragma unroll
             for (int pp = 0; pp < PPT; pp += PS) {
@@ -441,14 +461,14 @@ __global__ void __launch_bounds__(TS * TS / PPT) k_raster_fwd(RasterArgs a) {
             Hit hh[PS];
 #pragma unroll
             for (int q = 0; q < PS; ++q)
-              need[q] = !(done[pp + q] || g.pyc[pp + q] < bbk.z || g.pyc[pp + q] > bbk.w);
+              need[q] = !(done[pp + q] || g.ky[pp + q] < bbk.z || g.ky[pp + q] > bbk.w);
             if constexpr (PS == 2) {
               if (!need[0] && !need[1]) continue;
               eval_hit2(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
-                        make_float2(g.pyc[pp], g.pyc[pp + 1]), hh[0], hh[PS - 1]);
+                        make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
             } else {
               if (!need[0]) continue;
-              hh[0] = eval_hit(cp, r0, r1, r2, r4.w, g.sy[pp], g.pyc[pp]);
+              hh[0] = eval_hit(cp, r0, r1, r2, r4.w, g.sy[pp], g.ky[pp]);
             }
             if constexpr (PS == 2 && COLOR && !MASK && PPT <= 4) {  // (8 pixels per thread would spill)
               // Both pixels of the pair composited at once in packed FP32: a
@@ -750,6 +770,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
           float4 r0, r1, r2, r3, r4;
           if (AUX) load_record<PREC>(a.records, item, r0, r1, r2, r3, r4);
           else load_record4<PREC>(a.records, item, r0, r1, r2, r3);
+          stage_offsets(r1, r2, g.bx0, g.by0);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (AUX) s_r4[slot] = r4;
           s_msk[slot] = box_masks<TS, PPT>(bb, g);
@@ -807,7 +828,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
           if (AUX) { r4 = s_r4[k]; depth = r4.w; }
-          const ColPart cp = col_part(r0, r1, r2, g.sx, g.pxc);
+          const ColPart cp = col_part(r0, r1, r2, g.sx, g.kx);
           // One pixel per hit evaluation: evaluating pairs (eval_hit2) keeps two
           // hits live through the gradient code and costs more registers than
           // it saves instructions here.
@@ -824,10 +845,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
           if constexpr (PS == 2) {
             if (!need[0] && !need[1]) continue;
             eval_hit2(cp, r0, r1, r2, depth, make_float2(g.sy[pp], g.sy[pp + 1]),
-                      make_float2(g.pyc[pp], g.pyc[pp + 1]), hh[0], hh[PS - 1]);
+                      make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
           } else {
             if (!need[0]) continue;
-            hh[0] = eval_hit(cp, r0, r1, r2, depth, g.sy[pp], g.pyc[pp]);
+            hh[0] = eval_hit(cp, r0, r1, r2, depth, g.sy[pp], g.ky[pp]);
           }
 #pragma unroll
           for (int q = 0; q < PS; ++q) {
@@ -998,8 +1019,9 @@ __global__ void __launch_bounds__(256) k_raster_work(RasterArgs a, unsigned long
       ++fe;
       float4 r0, r1, r2, r3;
       load_record4<PREC>(a.records, item, r0, r1, r2, r3);
-      const ColPart cp = col_part(r0, r1, r2, sx, pxc);
-      const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, sy, pyc);
+      stage_offsets(r1, r2, (float)x0 + 0.5f, (float)y0 + 0.5f);
+      const ColPart cp = col_part(r0, r1, r2, sx, (float)(x - x0));
+      const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, sy, (float)(y - y0));
       const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
       if (!(alpha < ALPHA_SKIP)) ++co;
       if (j < nc && (TS != 16 || a.gmask == nullptr || (__ldg(a.gmask + range.x + j) & gbit))) ++be;
@@ -1122,6 +1144,7 @@ __device__ __forceinline__ int px_stage(const RasterArgs& a, const PxTile& t, ui
     const int sl = __popc(bal & lanemask_lt());
     float4 r0, r1, r2, r3;
     load_record4<PREC>(a.records, item, r0, r1, r2, r3);
+    stage_offsets(r1, r2, t.bx0, t.by0);
     s_r0[sl] = r0; s_r1[sl] = r1; s_r2[sl] = r2; s_r3[sl] = r3;
     s_rect[sl] = rect;
     s_j[sl] = j - rstart;
@@ -1196,9 +1219,8 @@ __global__ void __launch_bounds__(32) k_raster_fwd_px(RasterArgs a) {
           const int p = ly * 16 + lx;
           const float T = s_T[p];
           if (T < T_TERMINATE) continue;
-          const float pxc = t.bx0 + (float)lx, pyc = t.by0 + (float)ly;
-          const ColPart cp = col_part(r0, r1, r2, s_sx[lx], pxc);
-          const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, s_sy[ly], pyc);
+          const ColPart cp = col_part(r0, r1, r2, s_sx[lx], (float)lx);
+          const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, s_sy[ly], (float)ly);
           const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
           if (alpha < ALPHA_SKIP) continue;
           const float wt = T * alpha;
@@ -1304,9 +1326,8 @@ __global__ void __launch_bounds__(32) k_raster_bwd_px(RasterArgs a) {
           const int p = ly * 16 + lx;
           if (cidx >= s_nc[p]) continue;
           const float sx = s_sx[lx], sy = s_sy[ly];
-          const float pxc = t.bx0 + (float)lx, pyc = t.by0 + (float)ly;
-          const ColPart cp = col_part(r0, r1, r2, sx, pxc);
-          const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, sy, pyc);
+          const ColPart cp = col_part(r0, r1, r2, sx, (float)lx);
+          const Hit h = eval_hit(cp, r0, r1, r2, 0.0f, sy, (float)ly);
           const float raw_alpha = __fmul_rn(r3.w, h.ghat);
           const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
           if (alpha < ALPHA_SKIP) continue;
