@@ -631,6 +631,13 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
 #endif
   constexpr bool DLC_SMEM = GS_BWD_DLC_SMEM && !AUX && TS <= 16;  // (tiles of 32: 16 KB more than the static limit allows)
   __shared__ float4 s_dlc[DLC_SMEM ? TP : 1];
+  // Optionally each pixel's walked-back transmittance and colour suffix too
+  // (again read and written only by the thread that owns the pixel).
+#ifndef GS_BWD_STATE_SMEM
+#define GS_BWD_STATE_SMEM 0
+#endif
+  constexpr bool ST_SMEM = GS_BWD_STATE_SMEM && DLC_SMEM && DIRECT;  // single-warp CTAs
+  __shared__ float2 s_ts[ST_SMEM ? TP : 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;
   uint32_t pbit[PPT], thread_gbits = 0u;
@@ -699,6 +706,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
         if (DLC_SMEM) s_dlc[L::row(tid) * TS + L::col(tid) + p * TS] = gc;
         const float4 aux = a.out_aux[pix];
         T[p] = aux.x;
+        if (ST_SMEM) s_ts[L::row(tid) * TS + L::col(tid) + p * TS] = make_float2(aux.x, 0.f);
         nc[p] = a.out_nc[pix];
         if (AUX) {
           dld[p] = gc.w;
@@ -860,7 +868,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
             if (alpha < ALPHA_SKIP) continue;
             contrib = true;
             const float inv_oma = rcp_approx(1.0f - alpha);
-            const float t_before = T[p] * inv_oma;
+            float2 ts = make_float2(T[p], suf_c[p]);
+            if (ST_SMEM) ts = s_ts[L::row(tid) * TS + L::col(tid) + p * TS];
+            const float t_before = ts.x * inv_oma;
             const float w = t_before * alpha;
             float3 gcol = dlc[p];
             if (DLC_SMEM) {
@@ -868,7 +878,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
               gcol = make_float3(g4.x, g4.y, g4.z);
             }
             const float dc = gcol.x * r3.x + gcol.y * r3.y + gcol.z * r3.z;
-            float dl_dalpha = dc * t_before - suf_c[p] * inv_oma;
+            float dl_dalpha = dc * t_before - ts.y * inv_oma;
             float dl_dt = 0.f;
             if (AUX) {
               const float t_hit = h.t;
@@ -889,8 +899,12 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
               suf_cw[p] += coef * w;
               gg[17] += dln[p].x * w; gg[18] += dln[p].y * w; gg[19] += dln[p].z * w;
             }
-            suf_c[p] += dc * w;
-            T[p] = t_before;
+            if (ST_SMEM) {
+              s_ts[L::row(tid) * TS + L::col(tid) + p * TS] = make_float2(t_before, ts.y + dc * w);
+            } else {
+              suf_c[p] += dc * w;
+              T[p] = t_before;
+            }
             {  // packed pairs round per component as the scalar FFMAs (x·1 is exact)
               const float2 c2 = __ffma2_rn(make_float2(gcol.x, gcol.y), make_float2(w, w), make_float2(gg[11], gg[12]));
               gg[11] = c2.x; gg[12] = c2.y;
