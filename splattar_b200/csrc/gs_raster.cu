@@ -23,7 +23,7 @@ const RasterShape FWD8[] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}, {256
 const RasterShape FWD16[] = {{64, 1}, {128, 1}, {256, 1}, {64, 2}, {128, 2}, {64, 4}, {64, 8}, {128, 8}, {32, 0}};
 const RasterShape FWD32[] = {{64, 2}, {128, 2}, {256, 2}, {64, 4}, {128, 4}, {256, 4}, {128, 8}};
 const RasterShape BWD8[] = {{64, 1}, {64, 2}, {128, 2}};
-const RasterShape BWD16[] = {{64, 1}, {64, 2}, {128, 2}, {64, 4}, {64, 8}, {128, 8}, {32, 0}};
+const RasterShape BWD16[] = {{64, 1}, {64, 2}, {128, 2}, {64, 4}, {32, 8}, {64, 8}, {128, 8}, {32, 0}};
 const RasterShape BWD32[] = {{64, 4}, {64, 8}};
 }  // namespace
 
@@ -39,7 +39,7 @@ int raster_fwd_shapes(int tile, const RasterShape** out) {
 int raster_bwd_shapes(int tile, const RasterShape** out) {
   switch (tile) {
     case 8: *out = BWD8; return 3;
-    case 16: *out = BWD16; return 7;
+    case 16: *out = BWD16; return 8;
     case 32: *out = BWD32; return 2;
     default: *out = nullptr; return 0;
   }

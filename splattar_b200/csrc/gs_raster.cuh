@@ -312,13 +312,15 @@ __device__ __forceinline__ void cut_tile_end(const RasterArgs& a, int tile, uint
 // COLOR: colour, alpha and final transmittance only (the training step's
 // loss reads nothing else); depth and normal are neither accumulated nor
 // written.
-// Resident two-warp forward CTAs per SM that the register allocation must
-// allow (1: the compiler's choice).
+// Resident two-warp colour-only forward CTAs per SM that the register
+// allocation must allow (1: the compiler's choice). 14 caps the registers at 72 (7 warps per
+// SM sub-partition): on 1M surfels × 8 × 1080p the colour-only (64, 4)
+// forward ran 3.32 ms at 72 registers against 4.21 ms at the compiler's 99.
 #ifndef GS_FWD_2WARP_CTAS
-#define GS_FWD_2WARP_CTAS 1
+#define GS_FWD_2WARP_CTAS 14
 #endif
 template <int TS, int BATCH, int PREC, bool DET, bool PERSIST, int PPT, bool COLOR = false, bool MASK = false>
-__global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_2WARP_CTAS : 1)
+__global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR && !MASK) ? GS_FWD_2WARP_CTAS : 1)
     k_raster_fwd(RasterArgs a) {
   static_assert(!MASK || COLOR, "contributor masks belong to the colour-only variant");
   using L = Layout<TS, PPT>;
@@ -334,7 +336,8 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
   constexpr bool GM = COLOR && !MASK && TS == 16;
   constexpr int GPL = PPT >= 8 ? 2 : 1;              // row groups per lane
   constexpr int GW = (BATCH + 31) / 32;              // 32-entry words per batch
-  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH], s_bb[BATCH];
+  __shared__ float4 s_r0[BATCH], s_r1[BATCH], s_r2[BATCH], s_r3[BATCH];
+  __shared__ uint2 s_msk[BATCH];  // box_masks of the staged entry
   __shared__ float4 s_r4[COLOR ? 1 : BATCH];
   __shared__ int s_j[BATCH];
   __shared__ uint32_t s_gw[GM ? 4 : 1][GM ? GW : 1];
@@ -345,6 +348,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
   const int tid = threadIdx.x, lane = tid & 31;
   const bool gm_on = GM && a.gmask != nullptr;
   const int g0 = L::row(tid) >> 2;  // first row group of this lane's pixels
+  constexpr uint32_t PMASK = (1u << PPT) - 1u;  // a lane's pixels p as bits
   uint32_t gcur[GPL];
   int tile = blockIdx.x;
   for (;;) {
@@ -374,8 +378,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
     }
     float T[PPT], cr[PPT], cg[PPT], cb[PPT], aa[PPT], ad[PPT], nx[PPT], ny[PPT], nz[PPT];
     uint32_t nc[PPT];
-    bool done[PPT];
-    bool tdone = true;
+    uint32_t dm = 0u;  // bit p: pixel p terminated (or lies outside the image)
     // Stored-state contributor masks (colour-only variant): the word being
     // filled and its index, per pixel.
     uint32_t mw[PPT];
@@ -387,7 +390,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
     for (int p = 0; p < PPT; ++p) {
       T[p] = 1.f; cr[p] = cg[p] = cb[p] = aa[p] = ad[p] = nx[p] = ny[p] = nz[p] = 0.f;
       nc[p] = 0;
-      done[p] = !g.inside[p];
+      if (!g.inside[p]) dm |= 1u << p;
       if (resume && g.inside[p]) {
         const long long pix = g.row0 + (long long)p * g.W;
         const float4 c = a.out_color[pix], x = a.out_aux[pix];
@@ -399,12 +402,12 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
           nx[p] = nn.x; ny[p] = nn.y; nz[p] = nn.z;
         }
         nc[p] = a.out_nc[pix];
-        done[p] = T[p] < T_TERMINATE;
+        if (T[p] < T_TERMINATE) dm |= 1u << p;
       }
-      tdone &= done[p];
       mw[p] = 0u;
       mi[p] = 0;
     }
+    bool tdone = dm == PMASK;
     for (uint32_t base = range.x + skip; base < range.y; base += BATCH) {
       if (__syncthreads_count(tdone) == NT) break;
       const int count = (int)min((uint32_t)BATCH, range.y - base);
@@ -430,9 +433,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
           stage_offsets(r1, r2, g.bx0, g.by0);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (!COLOR) s_r4[slot] = r4;
-          // the box in tile-local pixel coordinates (its 1-pixel margin covers
-          // the rounding of the shift)
-          s_bb[slot] = make_float4(bb.x - g.bx0, bb.y - g.bx0, bb.z - g.by0, bb.w - g.by0);
+          s_msk[slot] = box_masks<TS, PPT>(bb, g);
           s_j[slot] = j;
         }
         kept += kr;
@@ -447,8 +448,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
         int k = 0;
         for (; k < kept; ++k) {
           const uint32_t kbit = 1u << (k & 31);
-          const float4 bbk = s_bb[k];
-          if (!tdone && g.kx >= bbk.x && g.kx <= bbk.y) {
+          const uint2 mk = s_msk[k];
+          // need: bit p when pixel p is live and inside the entry's α-box
+          const uint32_t need = ((mk.y >> L::col(tid)) & 1u) ? (mk.x >> L::row(tid)) & ~dm & PMASK : 0u;
+          if (need) {
             const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k];
             const float4 r3 = s_r3[k];
             const float4 r4 = COLOR ? make_float4(0.f, 0.f, 0.f, 0.f) : s_r4[k];
@@ -457,17 +460,16 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
             constexpr int PS = PPT >= 2 ? 2 : 1;  // pixels per hit evaluation
 #pragma unroll
             for (int pp = 0; pp < PPT; pp += PS) {
-            bool need[PS];
+            bool need_q[PS];
             Hit hh[PS];
 #pragma unroll
-            for (int q = 0; q < PS; ++q)
-              need[q] = !(done[pp + q] || g.ky[pp + q] < bbk.z || g.ky[pp + q] > bbk.w);
+            for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
             if constexpr (PS == 2) {
-              if (!need[0] && !need[1]) continue;
+              if (!need_q[0] && !need_q[1]) continue;
               eval_hit2(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
                         make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
             } else {
-              if (!need[0]) continue;
+              if (!need_q[0]) continue;
               hh[0] = eval_hit(cp, r0, r1, r2, r4.w, g.sy[pp], g.ky[pp]);
             }
             if constexpr (PS == 2 && COLOR && !MASK && PPT <= 4) {  // (8 pixels per thread would spill)
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
               // rounds as the scalar code below would.
               const float a0 = fminf(__fmul_rn(r3.w, hh[0].ghat), ALPHA_CLAMP);
               const float a1 = fminf(__fmul_rn(r3.w, hh[PS - 1].ghat), ALPHA_CLAMP);
-              const bool c0 = need[0] && !(a0 < ALPHA_SKIP), c1 = need[PS - 1] && !(a1 < ALPHA_SKIP);
+              const bool c0 = need_q[0] && !(a0 < ALPHA_SKIP), c1 = need_q[PS - 1] && !(a1 < ALPHA_SKIP);
               if (c0 || c1) {
                 const float2 al = make_float2(c0 ? a0 : 0.f, c1 ? a1 : 0.f);
                 const float2 Tp = make_float2(T[pp], T[pp + 1]);
@@ -493,12 +495,12 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
                 if (c0) {
                   nc[pp] = idx1;
                   if (GM) gcur[(((L::row(tid) & 3) + pp) >> 2) & (GPL - 1)] |= kbit;
-                  if (Tn.x < T_TERMINATE) done[pp] = true;
+                  if (Tn.x < T_TERMINATE) dm |= 1u << pp;
                 }
                 if (c1) {
                   nc[pp + 1] = idx1;
                   if (GM) gcur[(((L::row(tid) & 3) + pp + 1) >> 2) & (GPL - 1)] |= kbit;
-                  if (Tn.y < T_TERMINATE) done[pp + 1] = true;
+                  if (Tn.y < T_TERMINATE) dm |= 2u << pp;
                 }
               }
               continue;
@@ -506,7 +508,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
 #pragma unroll
             for (int q = 0; q < PS; ++q) {
               const int p = pp + q;
-              if (!need[q]) continue;
+              if (!need_q[q]) continue;
               const Hit& h = hh[q];
               const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
               if (alpha < ALPHA_SKIP) continue;
@@ -532,13 +534,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 64 ? GS_FWD_
                 }
                 mw[p] |= 1u << (cidx & 31u);
               }
-              if (T[p] < T_TERMINATE) done[p] = true;
+              if (T[p] < T_TERMINATE) dm |= 1u << p;
             }
             }
-            bool all = true;
-#pragma unroll
-            for (int p = 0; p < PPT; ++p) all &= done[p];
-            if (all) tdone = true;
+            tdone = dm == PMASK;
           }
           if (GM && gm_on && (k & 31) == 31) flush_row_groups<PPT, GPL, GM ? GW : 1>(gcur, s_gw, g0, k >> 5);
           if (__all_sync(FULL, tdone)) break;
@@ -640,12 +639,13 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
   __shared__ float2 s_ts[ST_SMEM ? TP : 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;
-  uint32_t pbit[PPT], thread_gbits = 0u;
-#pragma unroll
-  for (int p = 0; p < PPT; ++p) {
-    pbit[p] = 1u << ((L::row(tid) + p) >> 2);
-    thread_gbits |= pbit[p];
-  }
+  // A lane's pixels p (rows row(tid) + p) as bits of a PPT-bit mask. Row
+  // group g covers rows 4g..4g+3; a lane's first row is a multiple of
+  // min(PPT, 4), so its pixels fall in GPT whole groups of GSZ pixels.
+  constexpr uint32_t PMASK = (1u << PPT) - 1u;
+  constexpr int GSZ = PPT < 4 ? PPT : 4, GPT = PPT / GSZ;
+  const int g0 = L::row(tid) >> 2;  // the lane's first row group
+  const uint32_t thread_gbits = ((1u << GPT) - 1u) << g0;
   const uint32_t warp_gbits = __reduce_or_sync(FULL, thread_gbits);
   // Results of staged entry k: group q4 of four reduced components, or zeros
   // for an entry this warp's pixels did not composite.
@@ -729,6 +729,12 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
     if (my_max) atomicMax(&s_maxnc, (int)my_max);
     __syncthreads();
     const uint32_t maxnc = min((uint32_t)s_maxnc, range.y - range.x);
+    // Pixels whose walk has reached the current entry (cidx < nc[p]) as a
+    // mask. cidx only decreases, so the mask is rebuilt only when cidx drops
+    // below `thr`, the largest nc among the pixels not yet walking.
+    uint32_t alive = 0u, thr = 0u;
+#pragma unroll
+    for (int p = 0; p < PPT; ++p) thr = max(thr, nc[p]);
     // Stored-state mode: contributor masks written by the forward; the word
     // cached per pixel and its index (list positions are walked downwards).
     constexpr bool masks = MASK;
@@ -796,42 +802,53 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
           emit_zero(k);
           continue;
         }
-        bool bit[PPT];
-        bool anybit = false;
+        // need: bit p when pixel p evaluates the entry
+        uint32_t need = 0u;
         if (masks) {
 #pragma unroll
           for (int p = 0; p < PPT; ++p) {
-            bit[p] = false;
             if (cidx < nc[p]) {
               const int w = (int)(cidx >> 5);
               if (w != cw[p]) {
                 cw[p] = w;
                 cm[p] = __ldg(a.mask + mbase + mpix + p * TS + (size_t)w * TP);
               }
-              bit[p] = (cm[p] >> (cidx & 31u)) & 1u;
-              anybit |= bit[p];
+              need |= ((cm[p] >> (cidx & 31u)) & 1u) << p;
             }
           }
-          if (!__any_sync(FULL, anybit)) {  // no pixel of this warp composited the entry
+          if (!__any_sync(FULL, need != 0u)) {  // no pixel of this warp composited the entry
             emit_zero(k);
             continue;
           }
-        }
-        uint32_t gm = 0xffu;
-        if (GM) {
-          gm = s_gm[k];
-          if (!(gm & warp_gbits)) {  // no pixel of this warp's row groups composited the entry
-            emit_zero(k);
-            continue;
+        } else {
+          uint32_t gmp = PMASK;  // pixels in row groups that composited the entry
+          if (GM) {
+            const uint32_t gm = s_gm[k];
+            if (!(gm & warp_gbits)) {  // no pixel of this warp's row groups composited the entry
+              emit_zero(k);
+              continue;
+            }
+            gmp = 0u;
+#pragma unroll
+            for (int i = 0; i < GPT; ++i) gmp |= ((gm >> (g0 + i)) & 1u) ? ((1u << GSZ) - 1u) << (GSZ * i) : 0u;
           }
+          if (cidx < thr) {  // a pixel's walk starts here
+            alive = 0u;
+            thr = 0u;
+#pragma unroll
+            for (int p = 0; p < PPT; ++p) {
+              if (cidx < nc[p]) alive |= 1u << p;
+              else thr = max(thr, nc[p]);
+            }
+          }
+          const uint2 mk = s_msk[k];  // bit p of mk.x >> row: pixel p's row is inside the box
+          need = ((mk.y >> L::col(tid)) & 1u) ? (mk.x >> L::row(tid)) & alive & gmp : 0u;
         }
-        const uint2 mk = s_msk[k];
-        const uint32_t rows = mk.x >> L::row(tid);  // bit p: pixel p's row is inside the box
         float gg[NG];
 #pragma unroll
         for (int c = 0; c < NG; ++c) gg[c] = 0.f;
         bool contrib = false;
-        if (masks ? anybit : ((gm & thread_gbits) && ((mk.y >> L::col(tid)) & 1u))) {
+        if (need) {
           const float4 r0 = s_r0[k], r1 = s_r1[k], r2 = s_r2[k], r3 = s_r3[k];
           float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
@@ -843,25 +860,22 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
           constexpr int PS = 1;
 #pragma unroll
           for (int pp = 0; pp < PPT; pp += PS) {
-          bool need[PS];
+          bool need_q[PS];
           Hit hh[PS];
 #pragma unroll
-          for (int q = 0; q < PS; ++q) {
-            const int p = pp + q;
-            need[q] = masks ? bit[p] : (cidx < nc[p] && (gm & pbit[p]) && ((rows >> p) & 1u));
-          }
+          for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
           if constexpr (PS == 2) {
-            if (!need[0] && !need[1]) continue;
+            if (!need_q[0] && !need_q[1]) continue;
             eval_hit2(cp, r0, r1, r2, depth, make_float2(g.sy[pp], g.sy[pp + 1]),
                       make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
           } else {
-            if (!need[0]) continue;
+            if (!need_q[0]) continue;
             hh[0] = eval_hit(cp, r0, r1, r2, depth, g.sy[pp], g.ky[pp]);
           }
 #pragma unroll
           for (int q = 0; q < PS; ++q) {
             const int p = pp + q;
-            if (!need[q]) continue;
+            if (!need_q[q]) continue;
             const Hit& h = hh[q];
             const float raw_alpha = __fmul_rn(r3.w, h.ghat);
             const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
@@ -1410,7 +1424,7 @@ __global__ void __launch_bounds__(32) k_raster_bwd_px(RasterArgs a) {
 // Forward: TS 8 → ppt 1/2 × batch 64/128/256; TS 16 → (64,1) (128,1) (256,1)
 // (64,2) (128,2) (64,4) (64,8) (128,8); TS 32 → ppt 2/4 × batch 64/128/256
 // and (128,8). Backward without aux losses: TS 8 → (64,1) (64,2) (128,2);
-// TS 16 → (64,1) (64,2) (128,2) (64,4) (64,8) (128,8); TS 32 → (64,4) (64,8). With aux losses: batch 32 at ppt 1 (TS 8,
+// TS 16 → (64,1) (64,2) (128,2) (64,4) (32,8) (64,8) (128,8); TS 32 → (64,4) (64,8). With aux losses: batch 32 at ppt 1 (TS 8,
 // 16) or 4 (TS 32). The backward's per-warp partial buffer NW·BATCH·NG floats
 // is static shared memory, which bounds the backward shapes.
 template <int TS, int PREC, bool DET, bool PERSIST, bool COLOR, bool MASK, typename F>
@@ -1448,7 +1462,7 @@ bool bwd_shape(int batch, int ppt, F&& f) {
   } else if constexpr (TS == 8) {
     GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2)
   } else if constexpr (TS == 16) {
-    GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2) GS_BWD(64, 4) GS_BWD(64, 8) GS_BWD(128, 8)
+    GS_BWD(64, 1) GS_BWD(64, 2) GS_BWD(128, 2) GS_BWD(64, 4) GS_BWD(32, 8) GS_BWD(64, 8) GS_BWD(128, 8)
   } else {
     GS_BWD(64, 4) GS_BWD(64, 8)
   }

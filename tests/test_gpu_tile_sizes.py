@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 FWD_SHAPES = {8: [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2), (256, 2)],
               16: [(64, 1), (128, 1), (256, 1), (64, 2), (128, 2), (64, 4), (64, 8), (128, 8)],
               32: [(64, 2), (128, 2), (256, 2), (64, 4), (128, 4), (256, 4), (128, 8)]}
-BWD_SHAPES = {8: [(64, 1), (64, 2), (128, 2)], 16: [(64, 1), (64, 2), (128, 2), (64, 4), (64, 8), (128, 8)],
+BWD_SHAPES = {8: [(64, 1), (64, 2), (128, 2)], 16: [(64, 1), (64, 2), (128, 2), (64, 4), (32, 8), (64, 8), (128, 8)],
               32: [(64, 4), (64, 8)]}
 
 
