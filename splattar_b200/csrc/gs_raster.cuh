@@ -139,33 +139,44 @@ __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, co
   hb.ghat = __expf(-(hb.ray ? qrb : qs.y));
 }
 
-// Thread → pixel layout of a TS×TS tile with PPT vertically adjacent pixels
-// per thread: each warp owns a compact block of WC columns × WR·PPT rows
-// (16 × 2·PPT for tiles of 16 and 32, 8 × 4·PPT for tiles of 8), blocks laid
-// row-major over the tile.
-template <int TS, int PPT>
+// Thread → pixel layout of a TS×TS tile with PPT pixels of one column per
+// thread. Threads form TS/PPT thread rows; warps own blocks of WC columns × WR
+// thread rows (16 × 2 for tiles of 16 and 32, 8 × 4 for tiles of 8), laid
+// row-major over the tile. Blocked (IL false): thread row t holds the PPT
+// adjacent pixel rows t·PPT .. t·PPT+PPT−1. Interleaved (IL true): thread row
+// t holds rows t, t+RS, t+2·RS, … with RS = TS/PPT, so a warp whose thread
+// rows span the tile covers a box of h rows with about h/RS + 1 distinct
+// pixel slots instead of min(h, PPT).
+template <int TS, int PPT, bool IL = false>
 struct Layout {
   static constexpr int NT = TS * TS / PPT;       // threads per CTA
   static constexpr int WC = TS < 16 ? TS : 16;   // pixel columns of a warp's block
   static constexpr int WR = 32 / WC;             // thread rows of a warp's block
   static constexpr int BPR = TS / WC;            // warp blocks across the tile
+  static constexpr int RS = IL ? TS / PPT : 1;   // row step between a thread's pixels
   static_assert(NT % 32 == 0 && NT <= 1024, "whole warps, at most 1024 threads");
   static __device__ __forceinline__ int col(int tid) { return ((tid >> 5) % BPR) * WC + (tid & 31) % WC; }
-  static __device__ __forceinline__ int row(int tid) { return (((tid >> 5) / BPR) * WR + (tid & 31) / WC) * PPT; }
+  static __device__ __forceinline__ int trow(int tid) { return ((tid >> 5) / BPR) * WR + (tid & 31) / WC; }
+  // row of the thread's pixel 0 (pixel p: row(tid) + p·RS)
+  static __device__ __forceinline__ int row(int tid) { return IL ? trow(tid) : trow(tid) * PPT; }
+  // the thread's PPT bits in a staged row mask (box_masks)
+  static __device__ __forceinline__ int mshift(int tid) { return trow(tid) * PPT; }
 };
 
 template <int PPT>
 struct TileGeo {
   int W, H;
   long long row0;               // pix_base + y(p=0)·W + x
+  long long pstride;            // buffer offset between a thread's pixels (RS·W)
   float pxc, sx, kx;                 // kx: column within the tile
   float pyc[PPT], sy[PPT], ky[PPT];   // ky: rows within the tile
   bool inside[PPT];
   float bx0, bx1, by0, by1;     // pixel-centre extent of the tile's in-image pixels
 };
 
-template <int TS, int PPT>
+template <int TS, int PPT, bool IL = false>
 __device__ __forceinline__ TileGeo<PPT> tile_geo(const RasterArgs& a, int tile) {
+  using L = Layout<TS, PPT, IL>;
   TileGeo<PPT> g;
   int v = 0;
   while (v + 1 < a.n_views && tile >= __ldg(&a.views[v + 1].tile_base)) ++v;
@@ -175,19 +186,21 @@ __device__ __forceinline__ TileGeo<PPT> tile_geo(const RasterArgs& a, int tile) 
   g.H = __ldg(&V->height);
   const int lt = tile - __ldg(&V->tile_base);
   const int x0 = (lt % tiles_x) * TS, y0 = (lt / tiles_x) * TS;
-  const int x = x0 + Layout<TS, PPT>::col(threadIdx.x), yb = y0 + Layout<TS, PPT>::row(threadIdx.x);
+  const int x = x0 + L::col(threadIdx.x), yb = y0 + L::row(threadIdx.x);
   const float f = __ldg(&V->focal), cx = __ldg(&V->cx), cy = __ldg(&V->cy);
   g.pxc = (float)x + 0.5f;
   g.sx = -((g.pxc - cx) / f);  // s = −d
   g.kx = (float)(x - x0);
 #pragma unroll
   for (int p = 0; p < PPT; ++p) {
-    g.pyc[p] = (float)(yb + p) + 0.5f;
+    const int y = yb + p * L::RS;
+    g.pyc[p] = (float)y + 0.5f;
     g.sy[p] = (g.pyc[p] - cy) / f;
-    g.ky[p] = (float)(yb + p - y0);
-    g.inside[p] = x < g.W && yb + p < g.H;
+    g.ky[p] = (float)(y - y0);
+    g.inside[p] = x < g.W && y < g.H;
   }
   g.row0 = __ldg(&V->pix_base) + (long long)yb * g.W + x;
+  g.pstride = (long long)L::RS * g.W;
   g.bx0 = (float)x0 + 0.5f;
   g.bx1 = (float)(min(x0 + TS, g.W) - 1) + 0.5f;
   g.by0 = (float)y0 + 0.5f;
@@ -205,27 +218,50 @@ __device__ __forceinline__ bool box_hits_tile(const float4& b, const TileGeo<PPT
 // for |z - c0| < 2^23; larger values are clamped) and are corrected with the
 // same comparisons the per-pixel test makes, so the result is exact.
 template <int TS>
-__device__ __forceinline__ uint32_t span_bits(float c0, float z0, float z1) {
-  int lo = (int)ceilf(fminf(fmaxf(z0 - c0, -1.0f), (float)TS));
+__device__ __forceinline__ void span_range(float c0, float z0, float z1, int& lo, int& hi) {
+  lo = (int)ceilf(fminf(fmaxf(z0 - c0, -1.0f), (float)TS));
   if (lo < TS && !(c0 + (float)lo >= z0)) ++lo;
   if (lo > 0 && c0 + (float)(lo - 1) >= z0) --lo;
-  int hi = (int)floorf(fminf(fmaxf(z1 - c0, -1.0f), (float)TS));
+  hi = (int)floorf(fminf(fmaxf(z1 - c0, -1.0f), (float)TS));
   if (hi >= 0 && !(c0 + (float)hi <= z1)) --hi;
   if (hi < TS - 1 && c0 + (float)(hi + 1) <= z1) ++hi;
   lo = max(lo, 0);
   hi = min(hi, TS - 1);
+}
+template <int TS>
+__device__ __forceinline__ uint32_t span_bits(float c0, float z0, float z1) {
+  int lo, hi;
+  span_range<TS>(c0, z0, z1, lo, hi);
   if (hi < lo) return 0u;
   return ((2u << hi) - 1u) & ~((1u << lo) - 1u);
 }
 
-// Pixel masks of an entry's α-box over the tile: bit r of .x when pixel row r
-// of the tile (centre by0 + r) lies in [b.z, b.w], bit c of .y when column c
-// (centre bx0 + c) lies in [b.x, b.y]: the per-pixel box test, decided once
-// per staged entry (backward); a lane then tests bits instead of comparing per
-// pixel.
-template <int TS, int PPT>
+// Pixel masks of an entry's α-box over the tile, the per-pixel box test
+// decided once per staged entry; a lane then tests bits instead of comparing
+// per pixel. .y: bit c when column c (centre bx0 + c) lies in [b.x, b.y].
+// .x: the rows (centres by0 + r) in [b.z, b.w] in the layout's order: PPT bits
+// per thread row t, bit t·PPT + p for the thread's pixel p (row t·PPT + p when
+// blocked, which is bit r for row r; row t + p·RS when interleaved).
+template <int TS, int PPT, bool IL = false>
 __device__ __forceinline__ uint2 box_masks(const float4& b, const TileGeo<PPT>& g) {
-  return make_uint2(span_bits<TS>(g.by0, b.z, b.w), span_bits<TS>(g.bx0, b.x, b.y));
+  if constexpr (!IL) {
+    return make_uint2(span_bits<TS>(g.by0, b.z, b.w), span_bits<TS>(g.bx0, b.x, b.y));
+  } else {
+    constexpr int RS = TS / PPT;
+    int lo, hi;
+    span_range<TS>(g.by0, b.z, b.w, lo, hi);
+    uint32_t m = 0u;
+    if (hi >= lo) {
+#pragma unroll
+      for (int t = 0; t < RS; ++t) {
+        // pixels p with lo <= t + p·RS <= hi
+        const int plo = lo <= t ? 0 : (lo - t + RS - 1) / RS;
+        const int phi = hi < t ? -1 : min((hi - t) / RS, PPT - 1);
+        if (phi >= plo) m |= (((2u << phi) - 1u) & ~((1u << plo) - 1u)) << (t * PPT);
+      }
+    }
+    return make_uint2(m, span_bits<TS>(g.bx0, b.x, b.y));
+  }
 }
 
 // Compaction of one staging round: returns this thread's slot among the kept
@@ -598,7 +634,14 @@ template <int TS, int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT
 __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_WARP_CTAS : 1)
     k_raster_bwd(RasterArgs a) {
   static_assert(!MASK || !AUX, "contributor masks cover the colour-only backward");
-  using L = Layout<TS, PPT>;
+  // Interleaved pixel rows (Layout) for two or more pixels per thread: on
+  // 16-pixel tiles with 8 pixels per thread, a box of h ≤ 8 rows takes about
+  // h/2 + 1 pixel slots of the warp instead of h.
+#ifndef GS_BWD_INTERLEAVE
+#define GS_BWD_INTERLEAVE 1
+#endif
+  constexpr bool IL = GS_BWD_INTERLEAVE && PPT >= 2;
+  using L = Layout<TS, PPT, IL>;
   constexpr int NT = L::NT, NW = NT / 32, TP = TS * TS;
   constexpr int ROUNDS = (BATCH + NT - 1) / NT;  // staging rounds per batch
   constexpr int NG = AUX ? 32 : 16;  // reduced components per entry (AUX: 20 used)
@@ -639,14 +682,18 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
   __shared__ float2 s_ts[ST_SMEM ? TP : 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;
-  // A lane's pixels p (rows row(tid) + p) as bits of a PPT-bit mask. Row
-  // group g covers rows 4g..4g+3; a lane's first row is a multiple of
+  // A lane's pixels p (rows row(tid) + p·RS) as bits of a PPT-bit mask. Row
+  // group g covers rows 4g..4g+3. Blocked, a lane's first row is a multiple of
   // min(PPT, 4), so its pixels fall in GPT whole groups of GSZ pixels.
   constexpr uint32_t PMASK = (1u << PPT) - 1u;
   constexpr int GSZ = PPT < 4 ? PPT : 4, GPT = PPT / GSZ;
   const int g0 = L::row(tid) >> 2;  // the lane's first row group
-  const uint32_t thread_gbits = ((1u << GPT) - 1u) << g0;
+  uint32_t thread_gbits = 0u;
+#pragma unroll
+  for (int p = 0; p < PPT; ++p) thread_gbits |= 1u << ((L::row(tid) + p * L::RS) >> 2);
   const uint32_t warp_gbits = __reduce_or_sync(FULL, thread_gbits);
+  const int lpix = L::row(tid) * TS + L::col(tid);  // tile-local index of pixel 0 (pixel p: + p·RS·TS)
+  constexpr int PSTEP = L::RS * TS;
   // Results of staged entry k: group q4 of four reduced components, or zeros
   // for an entry this warp's pixels did not composite.
   auto emit4 = [&](int k, int q4, float s0, float s1, float s2, float s3) {
@@ -683,7 +730,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
       __syncthreads();
       continue;
     }
-    const TileGeo<PPT> g = tile_geo<TS, PPT>(a, tile);
+    const TileGeo<PPT> g = tile_geo<TS, PPT, IL>(a, tile);
     // Suffix sums of what lies behind the current entry: colour and normal
     // enter only through their dot products with dL/dcolour and dL/dnormal,
     // so those scalars are carried instead of the vectors.
@@ -700,13 +747,13 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
       T[p] = 1.f;
       nc[p] = 0;
       if (g.inside[p]) {
-        const long long pix = g.row0 + (long long)p * g.W;
+        const long long pix = g.row0 + (long long)p * g.pstride;
         const float4 gc = a.dl_dcolor[pix];
         dlc[p] = make_float3(gc.x, gc.y, gc.z);
-        if (DLC_SMEM) s_dlc[L::row(tid) * TS + L::col(tid) + p * TS] = gc;
+        if (DLC_SMEM) s_dlc[lpix + p * PSTEP] = gc;
         const float4 aux = a.out_aux[pix];
         T[p] = aux.x;
-        if (ST_SMEM) s_ts[L::row(tid) * TS + L::col(tid) + p * TS] = make_float2(aux.x, 0.f);
+        if (ST_SMEM) s_ts[lpix + p * PSTEP] = make_float2(aux.x, 0.f);
         nc[p] = a.out_nc[pix];
         if (AUX) {
           dld[p] = gc.w;
@@ -739,7 +786,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
     // cached per pixel and its index (list positions are walked downwards).
     constexpr bool masks = MASK;
     const size_t mbase = masks ? (size_t)__ldg(&a.mask_off[tile]) * TP : 0;
-    const int mpix = L::row(tid) * TS + L::col(tid);
+    const int mpix = lpix;
     uint32_t cm[PPT];
     int cw[PPT];
 #pragma unroll
@@ -787,7 +834,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
           stage_offsets(r1, r2, g.bx0, g.by0);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (AUX) s_r4[slot] = r4;
-          s_msk[slot] = box_masks<TS, PPT>(bb, g);
+          s_msk[slot] = box_masks<TS, PPT, IL>(bb, g);
           s_item[slot] = item;
           if (DET) s_q[slot] = q;
           s_j[slot] = j;
@@ -811,7 +858,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
               const int w = (int)(cidx >> 5);
               if (w != cw[p]) {
                 cw[p] = w;
-                cm[p] = __ldg(a.mask + mbase + mpix + p * TS + (size_t)w * TP);
+                cm[p] = __ldg(a.mask + mbase + mpix + p * PSTEP + (size_t)w * TP);
               }
               need |= ((cm[p] >> (cidx & 31u)) & 1u) << p;
             }
@@ -828,9 +875,22 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
               emit_zero(k);
               continue;
             }
-            gmp = 0u;
+            if constexpr (!IL) {
+              gmp = 0u;
 #pragma unroll
-            for (int i = 0; i < GPT; ++i) gmp |= ((gm >> (g0 + i)) & 1u) ? ((1u << GSZ) - 1u) << (GSZ * i) : 0u;
+              for (int i = 0; i < GPT; ++i) gmp |= ((gm >> (g0 + i)) & 1u) ? ((1u << GSZ) - 1u) << (GSZ * i) : 0u;
+            } else if constexpr (L::RS == 2) {  // pixel p in group p / 2: each bit of gm doubled
+              uint32_t x = gm & 0xfu;
+              x = (x | (x << 2)) & 0x33u;
+              x = (x | (x << 1)) & 0x55u;
+              gmp = x | (x << 1);
+            } else if constexpr (L::RS == 4) {  // pixel p in group p
+              gmp = gm & PMASK;
+            } else {
+              gmp = 0u;
+#pragma unroll
+              for (int p = 0; p < PPT; ++p) gmp |= ((gm >> ((L::row(tid) + p * L::RS) >> 2)) & 1u) << p;
+            }
           }
           if (cidx < thr) {  // a pixel's walk starts here
             alive = 0u;
@@ -842,7 +902,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
             }
           }
           const uint2 mk = s_msk[k];  // bit p of mk.x >> row: pixel p's row is inside the box
-          need = ((mk.y >> L::col(tid)) & 1u) ? (mk.x >> L::row(tid)) & alive & gmp : 0u;
+          need = ((mk.y >> L::col(tid)) & 1u) ? (mk.x >> L::mshift(tid)) & alive & gmp : 0u;
         }
         float gg[NG];
 #pragma unroll
@@ -883,12 +943,12 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
             contrib = true;
             const float inv_oma = rcp_approx(1.0f - alpha);
             float2 ts = make_float2(T[p], suf_c[p]);
-            if (ST_SMEM) ts = s_ts[L::row(tid) * TS + L::col(tid) + p * TS];
+            if (ST_SMEM) ts = s_ts[lpix + p * PSTEP];
             const float t_before = ts.x * inv_oma;
             const float w = t_before * alpha;
             float3 gcol = dlc[p];
             if (DLC_SMEM) {
-              const float4 g4 = s_dlc[L::row(tid) * TS + L::col(tid) + p * TS];
+              const float4 g4 = s_dlc[lpix + p * PSTEP];
               gcol = make_float3(g4.x, g4.y, g4.z);
             }
             const float dc = gcol.x * r3.x + gcol.y * r3.y + gcol.z * r3.z;
@@ -914,7 +974,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
               gg[17] += dln[p].x * w; gg[18] += dln[p].y * w; gg[19] += dln[p].z * w;
             }
             if (ST_SMEM) {
-              s_ts[L::row(tid) * TS + L::col(tid) + p * TS] = make_float2(t_before, ts.y + dc * w);
+              s_ts[lpix + p * PSTEP] = make_float2(t_before, ts.y + dc * w);
             } else {
               suf_c[p] += dc * w;
               T[p] = t_before;
