@@ -35,9 +35,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd+Adam steps/s, 1M surfels 1080p: chosen vs plain form; HBM roofline frac"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel,
-# from one ncu capture of the same workload and launch shapes
-# (python profile_step.py --workload ring8_1m --shapes 64,4,128,8).
-TRAFFIC = {("ring8_1m", "raster_bwd"): 1_552_203_008}
+# from one ncu capture of the same workload
+# (python profile_step.py --workload ring8_1m --shapes 64,4,64,8; the staging
+# batch, 64 there and 32 as autotuned, does not change what is read).
+TRAFFIC = {("ring8_1m", "raster_bwd"): 1_545_378_304}
 # Launch shapes (fwd batch, fwd pixels/thread, bwd batch, bwd pixels/thread)
 # tried for the plain form at 16-pixel tiles before it is timed.
 PLAIN_SHAPES = [(128, 2, 128, 2), (128, 2, 64, 4), (128, 1, 128, 2), (64, 4, 64, 8)]
@@ -48,7 +49,7 @@ FALLBACK_HBM_GBS = 6650.0
 #   hit test eval_hit / eval_hit2: det 1 FMA, u.det and v.det 2 FMA, u and v
 #     2 MUL, t 1 MUL, u^2+v^2 1 MUL + 1 FMA, q_ray 1 MUL, dy 1 ADD, q_screen
 #     1 FMA, exp 1 MUL + 1 EX2, 1/det 1 RCP (17 flops, 2 MUFU), alpha 1 MUL,
-#     plus the column partial sums (3 FMA, 1 ADD, 1 MUL = 8 flops per entry
+#     plus the column partial sums (1 FMA, 1 ADD, 3 MUL = 6 flops per entry
 #     and thread, over 4 forward / 8 backward pixels per thread);
 #   forward composite: w 1 MUL, colour 3 FMA, alpha sum 1 ADD, T 1 ADD + 1 MUL;
 #   backward per contributor: 1 - alpha 1 ADD + 1 RCP, T_before 1 MUL, w 1 MUL,
@@ -60,7 +61,7 @@ RASTER_OPS = {"raster_fwd": (20, 10, 2, 0), "raster_bwd": (19, 38, 2, 1)}
 SM_COUNT, FP32_PER_SM_CLK, MUFU_PER_SM_CLK = 148, 256, 16
 # Issue-slot activity of the raster kernels measured by ncu on ring2_200k
 # (profiles/raster_fwd_bwd_ring2_200k.md).
-ISSUE_ACTIVE_NCU = {"raster_fwd": 0.800, "raster_bwd": 0.683}
+ISSUE_ACTIVE_NCU = {"raster_fwd": 0.854, "raster_bwd": 0.687}
 
 
 def parse(argv=None):
@@ -173,19 +174,26 @@ def measured_hbm_peak():
 
 
 # ------------------------------------------------------ CPU (oracle) timing
-def cpu_step_estimate(wl, seconds_target: float, threads: int = 0, view_ids=None):
+def cpu_step_estimate(wl, seconds_target: float, threads: int = 0, view_ids=None, stride: int = 0):
     """Seconds per full training step of the C++ restatement of the
     reference's CPU renderer (crates/gs-cpu-ref) on this workload, measured on
     a bounded sample: every view's projection, tile lists, L1+SSIM and
     parameter chain in full, the per-pixel forward and backward walks on every
-    `stride`-th tile only, scaled by `stride`; Adam over all parameters once."""
+    `stride`-th tile only, scaled by `stride`; Adam over all parameters once.
+    stride 0 chooses: every 64th tile, or every tile (no sampling, nothing
+    extrapolated) when the whole step is estimated at no more than half of
+    `seconds_target`."""
+    if stride == 0:
+        est, _, detail = cpu_step_estimate(wl, seconds_target, threads, view_ids, 64)
+        if seconds_target <= 0 or est > 0.5 * seconds_target:
+            return est, 64, detail
+        stride = 1
     import oracle
     s = wl.surfels
     scene = oracle.Scene(s.positions.astype(np.float64), s.scales.astype(np.float64), s.quats.astype(np.float64),
                          s.opacities.astype(np.float64), s.sh48().astype(np.float64), s.sh_degree)
     views = range(len(wl.cameras)) if view_ids is None else view_ids
     total, detail = 0.0, []
-    stride = 64
     adam = 0.0
     for v in views:
         c = wl.cameras[v]
@@ -490,6 +498,7 @@ def run_densify_cycle(args, ws, rank, local):
     rast.write("target", rast.read("out_color", 4 * P))
     rast.upload_scene(wl.surfels.scene_input())
     rast.optimizer_init(n)
+    tuned = rast.autotune(cams, n)  # raster launch shapes for this workload (tile 16)
     step = StepSettings(0.8, 0.2, AdamSettings(eps=1e-15), "chosen")
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
@@ -517,8 +526,9 @@ def run_densify_cycle(args, ws, rank, local):
     print(json.dumps({
         "metric": METRIC, "value": round(aggregate_steps_per_s(ms, ws), 4), "unit": "steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "views": nv, "pixels_per_step": P, "capacity": cap,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.precision == "f32" else f"f32 compute, {args.precision} storage", "data": "synthetic",
+        "config": {"workload": args.workload, "views": nv, "pixels_per_step": P, "capacity": cap, "autotuned": tuned,
                    "densify_every": args.densify_every, "mode": "deterministic" if args.deterministic else "atomic",
                    "surfels_after_each_densify": counts, "tile_entries_before_each_densify": entries,
                    "device_bytes_of_handle": int(free0 - free1), "device_bytes_total": int(total),
@@ -638,10 +648,11 @@ def main():
         step_s, stride, detail = cpu_step_estimate(r["wl"], args.cpu_seconds, threads=cores)
         spent = time.time() - t0
         line["cpu_baseline"] = {"value": round(1.0 / step_s, 6), "unit": "steps/s", "cores": cores, "kind": "port",
-                                "sample": f"all {nv} views; projection, tile lists, L1+SSIM, parameter chain and Adam "
-                                          f"in full; per-pixel forward/backward on every {stride}th tile, scaled by "
-                                          f"{stride}",
-                                "extrapolated": True, "sample_fraction_of_pixel_walks": round(1.0 / stride, 5),
+                                "sample": (f"all {nv} views; projection, tile lists, L1+SSIM, parameter chain and Adam "
+                                           f"in full; per-pixel forward/backward on every {stride}th tile, scaled by "
+                                           f"{stride}") if stride > 1 else
+                                          f"the whole step, all {nv} views, every tile (not sampled)",
+                                "extrapolated": stride > 1, "sample_fraction_of_pixel_walks": round(1.0 / stride, 5),
                                 "seconds_spent": round(spent, 2), "seconds_per_step": round(step_s, 3),
                                 "literal": literal_baselines()}
     print(json.dumps(line))
@@ -659,9 +670,12 @@ def main_reference(args, ws, rank):
     nv = len(wl.cameras)
     times = []
     t0 = time.time()
+    # every tile (no sampling) when a whole step takes at most 5 s, else every 64th tile
+    est, _, _ = cpu_step_estimate(wl, 0, threads=cores, view_ids=[0], stride=64)
+    stride = 1 if est <= 5.0 else 64
     for k in range(args.warmup + args.steps):
         v = k % nv
-        step_s, stride, _ = cpu_step_estimate(wl, 0, threads=cores, view_ids=[v])
+        step_s, stride, _ = cpu_step_estimate(wl, 0, threads=cores, view_ids=[v], stride=stride)
         if k >= args.warmup:
             times.append(step_s)
     spent = time.time() - t0
@@ -673,9 +687,12 @@ def main_reference(args, ws, rank):
             "config": {"workload": args.workload, "surfels": wl.surfels.n, "views": nv, "pixels_per_step": wl.pixels},
             "cpu_baseline": {"value": round(val, 6), "unit": "steps/s", "cores": cores, "kind": "port",
                              "sample": f"each step one view (rotating) of {nv}: projection, tile lists, L1+SSIM, "
-                                       f"parameter chain in full, per-pixel walks on every {stride}th tile scaled by "
-                                       f"{stride}, extrapolated to all {nv} views; Adam over all parameters",
-                             "extrapolated": True, "sample_fraction_of_pixel_walks": round(1.0 / (stride * nv), 6),
+                                       + (f"parameter chain in full, per-pixel walks on every {stride}th tile scaled by {stride}"
+                                          if stride > 1 else "parameter chain and per-pixel walks in full (every tile)")
+                                       + (f", extrapolated to all {nv} views" if nv > 1 else "")
+                                       + "; Adam over all parameters",
+                             "extrapolated": stride > 1 or nv > 1,
+                             "sample_fraction_of_pixel_walks": round(1.0 / (stride * nv), 6),
                              "seconds_spent": round(spent, 2)},
             "e2e": {"value": round(val, 6), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference (Rust + WGSL on wgpu/Vulkan) cannot be built or run here; this is its CPU "

@@ -67,6 +67,16 @@ __device__ __forceinline__ TileLoc locate(const SsimArgs& a, int t) {
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
+// Asynchronous copy of B bytes (4, 8 or 16; both addresses B-aligned) from
+// global to shared memory; when !valid nothing is read and the B bytes are
+// zero-filled. Completion: cp.async.wait_all, then a barrier for other threads.
+template <int B>
+__device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, bool valid) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(s), "l"(gmem), "n"(B), "r"(valid ? B : 0)
+               : "memory");
+}
+
 // Slides an 11-tap window along `N_OUT` outputs: out[o] = Σ_d w[|d−5|]·in(o+d)
 // (w[k] is the weight at offset ±k), for a scalar map.
 template <int N_OUT, class In, class Out>
@@ -141,9 +151,12 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
 #pragma unroll
   for (int k = 0; k < 6; ++k) w[k] = a.w[k];
   __syncthreads();
-  // Horizontal: item = (map, row).
-  for (int it = tid; it < (NM2 + 1) * EXT; it += 256) {
-    const int m = it / EXT, r = it - m * EXT;
+  // Horizontal: warp m blurs map m, lane r < EXT row r, so each warp runs one
+  // of the four code paths (an item order that put two maps in a warp ran
+  // both paths with half the lanes each).
+  static_assert(NM2 + 1 == 8 && EXT <= 32, "one warp per map, one lane per staged row");
+  if ((tid & 31) < EXT) {
+    const int m = tid >> 5, r = tid & 31;
     if (m < 6) {
       const float2* XY = &s_in[m >> 1][r][0];
       float2* O = &s_h2[m][r * H_ROW];
@@ -249,21 +262,26 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
   const TileLoc L = locate(a, blockIdx.x);
   const float2* P2 = reinterpret_cast<const float2*>(a.coef);
   const size_t st2 = a.coef_stride;
+  // Staged with asynchronous copies (global -> shared, no registers), so all
+  // of a thread's loads are in flight at once; pixels outside the view are
+  // zero-filled by the copy (source size 0).
   for (int k = tid; k < EXT * EXT; k += 256) {
     const int ly = k / EXT, lx = k % EXT;
     const int gx = L.x0 + lx - HALO, gy = L.y0 + ly - HALO;
     const bool in = gx >= 0 && gy >= 0 && gx < L.W && gy < L.H;
     const size_t p = in ? (size_t)(L.pix_base + (long long)gy * L.W + gx) : 0;
 #pragma unroll
-    for (int m = 0; m < 4; ++m) s_c2[m][ly][lx] = in ? __ldg(P2 + m * st2 + p) : make_float2(0.f, 0.f);
-    s_c1[ly][lx] = in ? __ldg(a.coef + 8 * a.coef_stride + p) : 0.f;
+    for (int m = 0; m < 4; ++m) cp_async_zfill<8>(&s_c2[m][ly][lx], P2 + m * st2 + p, in);
+    cp_async_zfill<4>(&s_c1[ly][lx], a.coef + 8 * a.coef_stride + p, in);
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   float w[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) w[k] = a.w[k];
   __syncthreads();
-  for (int it = tid; it < 5 * EXT; it += 256) {
-    const int m = it / EXT, r = it - m * EXT;
+  // Horizontal: warp m < 5 blurs plane m, lane r < EXT row r (one code path per warp).
+  if (tid < 5 * 32 && (tid & 31) < EXT) {
+    const int m = tid >> 5, r = tid & 31;
     if (m < 4) {
       const float2* X = &s_c2[m][r][0];
       float2* O = &s_h2[m][r * H_ROW];

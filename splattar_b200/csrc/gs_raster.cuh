@@ -634,13 +634,15 @@ template <int TS, int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT
 __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_WARP_CTAS : 1)
     k_raster_bwd(RasterArgs a) {
   static_assert(!MASK || !AUX, "contributor masks cover the colour-only backward");
-  // Interleaved pixel rows (Layout) for two or more pixels per thread: on
-  // 16-pixel tiles with 8 pixels per thread, a box of h ≤ 8 rows takes about
-  // h/2 + 1 pixel slots of the warp instead of h.
+  // Interleaved pixel rows (Layout) for single-warp CTAs with two or more
+  // pixels per thread: on 16-pixel tiles with 8 pixels per thread, a box of
+  // h ≤ 8 rows takes about h/2 + 1 pixel slots of the warp instead of h. With
+  // several warps, interleaving would spread every box over all of them (one
+  // more warp reduction per warp an entry reaches), so they stay blocked.
 #ifndef GS_BWD_INTERLEAVE
 #define GS_BWD_INTERLEAVE 1
 #endif
-  constexpr bool IL = GS_BWD_INTERLEAVE && PPT >= 2;
+  constexpr bool IL = GS_BWD_INTERLEAVE && PPT >= 2 && TS * TS / PPT == 32;
   using L = Layout<TS, PPT, IL>;
   constexpr int NT = L::NT, NW = NT / 32, TP = TS * TS;
   constexpr int ROUNDS = (BATCH + NT - 1) / NT;  // staging rounds per batch
