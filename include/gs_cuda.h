@@ -343,12 +343,15 @@ gs_status gs_raster_work(gs_rasterizer* r, uint64_t out[4], void* stream);
 
 /* Raster launch shapes (staging batch, pixels per thread) built per tile size:
  *   forward   tile 8:  ppt 1 or 2 with batch 64/128/256
- *             tile 16: (64,1) (128,1) (256,1) (64,2) (128,2) (64,4) (64,8) (128,8)
+ *             tile 16: (64,1) (128,1) (256,1) (64,2) (128,2) (64,4) (64,8) (128,8) (32,0)
  *             tile 32: ppt 2 or 4 with batch 64/128/256, and (128,8)
  *   backward  tile 8:  (64,1) (64,2) (128,2)
- *             tile 16: (64,1) (64,2) (128,2) (64,4) (64,8) (128,8)
+ *             tile 16: (64,1) (64,2) (128,2) (64,4) (32,8) (64,8) (128,8) (32,0)
  *             tile 32: (64,4) (64,8)
- * (the backward with aux losses uses its own fixed shape).
+ * (32,0) selects the pixel-compacted kernels (one warp per tile spreading each
+ * entry's box pixels over its lanes) for the colour-only persistent passes of
+ * the training step; other passes fall back to (64,4) forward and (64,8)
+ * backward. The backward with aux losses uses its own fixed shape.
  *
  * Autotuner (config-2 sweep of the batched form): at the handle's current
  * tile size, times the forward (projection + binning + raster) over every
