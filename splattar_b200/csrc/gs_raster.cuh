@@ -625,13 +625,17 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
   }
 }
 
-// Resident single-warp backward CTAs per SM that the register allocation must
-// allow (1: the compiler's choice).
+// Resident single-warp backward CTAs per SM (without stored-state masks, which
+// would spill) that the register allocation must allow (1: the compiler's
+// choice). 24 caps the registers at 80 (6 warps per
+// SM sub-partition instead of 4 at the compiler's 115): on 1M surfels × 8 ×
+// 1080p the (32, 8) backward ran 3.31 ms against 3.70 ms (24 B of spills;
+// at 72 registers the spills grew to 68 B and it ran 3.63 ms).
 #ifndef GS_BWD_WARP_CTAS
-#define GS_BWD_WARP_CTAS 1
+#define GS_BWD_WARP_CTAS 24
 #endif
 template <int TS, int BATCH, int PREC, bool AUX, bool DET, bool PERSIST, int PPT, bool MASK = false>
-__global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_WARP_CTAS : 1)
+__global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK) ? GS_BWD_WARP_CTAS : 1)
     k_raster_bwd(RasterArgs a) {
   static_assert(!MASK || !AUX, "contributor masks cover the colour-only backward");
   // Interleaved pixel rows (Layout) for single-warp CTAs with two or more
@@ -682,6 +686,18 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
 #endif
   constexpr bool ST_SMEM = GS_BWD_STATE_SMEM && DLC_SMEM && DIRECT;  // single-warp CTAs
   __shared__ float2 s_ts[ST_SMEM ? TP : 1];
+  // Single-warp interleaved colour-only CTAs keep the pixels' contributor
+  // counts in shared memory (read only when the walk mask is rebuilt), and
+  // optionally the rows' ray components (read once per evaluated pixel
+  // pair), instead of registers; a pixel's tile-local row offset is then
+  // formed from its first.
+#ifndef GS_BWD_SY_SMEM
+#define GS_BWD_SY_SMEM 0
+#endif
+  constexpr bool LEAN = DIRECT && IL && DLC_SMEM && !MASK;
+  constexpr bool SYS = LEAN && GS_BWD_SY_SMEM;
+  __shared__ uint32_t s_nc[LEAN ? TP : 1];
+  __shared__ float s_sy[SYS ? TS : 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;
   // A lane's pixels p (rows row(tid) + p·RS) as bits of a PPT-bit mask. Row
@@ -770,7 +786,15 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
                                           dln[p].z != 0.f || a.lambda_dist != 0.f);
       if (!has_loss) nc[p] = 0;  // nc = 0 disables the pixel's walk
       my_max = max(my_max, nc[p]);
+      if (LEAN) s_nc[lpix + p * PSTEP] = nc[p];
     }
+    if (SYS && (lane % L::WC) == 0) {  // one lane per thread row writes its rows' sy
+#pragma unroll
+      for (int p = 0; p < PPT; ++p) s_sy[L::row(tid) + p * L::RS] = g.sy[p];
+    }
+    // the ray component and tile-local row of pixel p (as tile_geo computes them)
+    auto sy_of = [&](int p) { return SYS ? s_sy[L::row(tid) + p * L::RS] : g.sy[p]; };
+    auto ky_of = [&](int p) { return LEAN ? __fadd_rn(g.ky[0], (float)(p * L::RS)) : g.ky[p]; };
     // Entries at or past this warp's last contributor are skipped warp-wide.
     const uint32_t warp_maxnc = __reduce_max_sync(FULL, my_max);
     if (tid == 0) s_maxnc = 0;
@@ -899,8 +923,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
             thr = 0u;
 #pragma unroll
             for (int p = 0; p < PPT; ++p) {
-              if (cidx < nc[p]) alive |= 1u << p;
-              else thr = max(thr, nc[p]);
+              const uint32_t ncp = LEAN ? s_nc[lpix + p * PSTEP] : nc[p];
+              if (cidx < ncp) alive |= 1u << p;
+              else thr = max(thr, ncp);
             }
           }
           const uint2 mk = s_msk[k];  // bit p of mk.x >> row: pixel p's row is inside the box
@@ -929,11 +954,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
           for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
           if constexpr (PS == 2) {
             if (!need_q[0] && !need_q[1]) continue;
-            eval_hit2(cp, r0, r1, r2, depth, make_float2(g.sy[pp], g.sy[pp + 1]),
-                      make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
+            eval_hit2(cp, r0, r1, r2, depth, make_float2(sy_of(pp), sy_of(pp + 1)),
+                      make_float2(ky_of(pp), ky_of(pp + 1)), hh[0], hh[PS - 1]);
           } else {
             if (!need_q[0]) continue;
-            hh[0] = eval_hit(cp, r0, r1, r2, depth, g.sy[pp], g.ky[pp]);
+            hh[0] = eval_hit(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
           }
 #pragma unroll
           for (int q = 0; q < PS; ++q) {
@@ -1000,7 +1025,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, (TS * TS / PPT) == 32 ? GS_BWD_
                 const float2 guv = __fmul2_rn(make_float2(-h.u, -h.v), make_float2(Ki, Ki));
                 float gdet = h.q2 * Ki;
                 if (AUX) gdet -= h.t * dl_dt * h.inv_det;
-                const float2 sy1 = make_float2(g.sy[p], 1.0f);
+                const float2 sy1 = make_float2(sy_of(p), 1.0f);
                 const float2 m0 = __ffma2_rn(make_float2(gdet, gdet), sy1, make_float2(gg[1], gg[2]));
                 const float2 m1 = __ffma2_rn(make_float2(guv.x, guv.x), sy1, make_float2(gg[4], gg[5]));
                 const float2 m2 = __ffma2_rn(make_float2(guv.y, guv.y), sy1, make_float2(gg[7], gg[8]));
