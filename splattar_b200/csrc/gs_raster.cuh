@@ -1019,7 +1019,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
               // through t = tn/det).
               const float dg = dl_dalpha * h.ghat;
               gg[14] += dg;
-              const float K = dg * r3.w;
+              const float K = dl_dalpha * raw_alpha;  // = dg·o, without waiting for dg
               if (h.ray) {
                 const float Ki = K * h.inv_det;
                 const float2 guv = __fmul2_rn(make_float2(-h.u, -h.v), make_float2(Ki, Ki));
@@ -1461,7 +1461,7 @@ __global__ void __launch_bounds__(32) k_raster_bwd_px(RasterArgs a) {
           if (raw_alpha <= ALPHA_CLAMP) {
             const float dg = dl_dalpha * h.ghat;
             gg[14] += dg;
-            const float K = dg * r3.w;
+            const float K = dl_dalpha * raw_alpha;  // = dg·o
             if (h.ray) {
               // record moments sum over the pixel ray s = (sx, sy, 1) of the
               // ray-branch adjoints (see k_raster_bwd)
