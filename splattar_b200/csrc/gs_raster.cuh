@@ -102,7 +102,7 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
   const float qr = ray_ok ? __fmul_rn(0.5f, h.q2) : __int_as_float(0x7f800000);
   const float qs = fmaf(h.dy, h.dy, c.dx2);  // (dx²+dy²)/(2σ²) with σ² = 0.5
   h.ray = qr <= qs;
-  const float q = h.ray ? qr : qs;
+  const float q = fminf(qr, qs);  // = ray ? qr : qs (neither is NaN; equal values are the same value)
   h.u = u; h.v = v; h.inv_det = inv;
   h.t = h.ray ? t : depth;
   h.ghat = __expf(-q);
@@ -135,8 +135,8 @@ __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, co
   hb.u = u.y; hb.v = v.y; hb.inv_det = inv.y; hb.q2 = q2.y; hb.dy = dy.y;
   ha.t = ha.ray ? t.x : depth;
   hb.t = hb.ray ? t.y : depth;
-  ha.ghat = __expf(-(ha.ray ? qra : qs.x));
-  hb.ghat = __expf(-(hb.ray ? qrb : qs.y));
+  ha.ghat = __expf(-fminf(qra, qs.x));  // = ray ? q_ray : q_screen, as in eval_hit
+  hb.ghat = __expf(-fminf(qrb, qs.y));
 }
 
 // Thread → pixel layout of a TS×TS tile with PPT pixels of one column per
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
 #pragma unroll
             for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
             if constexpr (PS == 2) {
-              if (!need_q[0] && !need_q[1]) continue;
+              if (!((need >> pp) & 3u)) continue;
               eval_hit2(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
                         make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
             } else {
@@ -528,14 +528,14 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
                 cr[pp] = vr.x; cr[pp + 1] = vr.y; cg[pp] = vg.x; cg[pp + 1] = vg.y;
                 cb[pp] = vb.x; cb[pp + 1] = vb.y; aa[pp] = va.x; aa[pp + 1] = va.y;
                 T[pp] = Tn.x; T[pp + 1] = Tn.y;
+                // both pixels of a pair lie in one 4-row group (a thread's first row is even)
+                if (GM) gcur[(((L::row(tid) & 3) + pp) >> 2) & (GPL - 1)] |= kbit;
                 if (c0) {
                   nc[pp] = idx1;
-                  if (GM) gcur[(((L::row(tid) & 3) + pp) >> 2) & (GPL - 1)] |= kbit;
                   if (Tn.x < T_TERMINATE) dm |= 1u << pp;
                 }
                 if (c1) {
                   nc[pp + 1] = idx1;
-                  if (GM) gcur[(((L::row(tid) & 3) + pp + 1) >> 2) & (GPL - 1)] |= kbit;
                   if (Tn.y < T_TERMINATE) dm |= 2u << pp;
                 }
               }
@@ -953,7 +953,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
 #pragma unroll
           for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
           if constexpr (PS == 2) {
-            if (!need_q[0] && !need_q[1]) continue;
+            if (!((need >> pp) & 3u)) continue;
             eval_hit2(cp, r0, r1, r2, depth, make_float2(sy_of(pp), sy_of(pp + 1)),
                       make_float2(ky_of(pp), ky_of(pp + 1)), hh[0], hh[PS - 1]);
           } else {
