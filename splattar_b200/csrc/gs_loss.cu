@@ -260,6 +260,17 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
   static_assert(4 * V_PLANE * 2 + V_PLANE <= 4 * EXT * IN_PITCH * 2, "vertical results fit in s_c2");
   const int tid = threadIdx.x;
   const TileLoc L = locate(a, blockIdx.x);
+  // This thread's pixel of the image and target, loaded now so the loads are
+  // in flight during the blurs.
+  const int ox = tid & 15, oy = tid >> 4;
+  const int gx = L.x0 + ox, gy = L.y0 + oy;
+  const bool inside = gx < L.W && gy < L.H;
+  const long long pix = inside ? L.pix_base + (long long)gy * L.W + gx : 0;
+  float4 x = make_float4(0.f, 0.f, 0.f, 0.f), y = x;
+  if (inside) {
+    x = a.img[pix];
+    y = a.target[pix];
+  }
   const float2* P2 = reinterpret_cast<const float2*>(a.coef);
   const size_t st2 = a.coef_stride;
   // Staged with asynchronous copies (global -> shared, no registers), so all
@@ -309,11 +320,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
     }
   }
   __syncthreads();
-  const int ox = tid & 15, oy = tid >> 4;
-  const int gx = L.x0 + ox, gy = L.y0 + oy;
-  if (gx >= L.W || gy >= L.H) return;
-  const long long pix = L.pix_base + (long long)gy * L.W + gx;
-  const float4 x = a.img[pix], y = a.target[pix];
+  if (!inside) return;
   const float k1 = a.w_l1 / (3.0f * (float)L.W * (float)L.H);
   const int q = oy * T16 + ox;
   const float2 vm = s_v2[0 * V_PLANE + q], vx2 = s_v2[1 * V_PLANE + q], vxy = s_v2[2 * V_PLANE + q];
