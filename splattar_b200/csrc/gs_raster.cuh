@@ -656,6 +656,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
   // (16-pixel tiles): entries no pixel of a group composited are skipped for
   // that group's pixels without evaluating them.
   constexpr bool GM = !AUX && !MASK && TS == 16;
+  // Interleaved single-warp tiles fold the summary into the staged row mask
+  // (a pixel's group depends on its slot alone there, not on its thread row).
+  constexpr bool GM_FOLD = GM && IL && L::RS == 2;
   // A single-warp CTA (8 pixels per thread on 16-pixel tiles) has nothing to
   // sum across warps: the lanes holding each group of four reduced components
   // gather them by shuffles and emit the vector reduction (or ordered store)
@@ -864,7 +867,20 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           s_item[slot] = item;
           if (DET) s_q[slot] = q;
           s_j[slot] = j;
-          if (GM) s_gm[slot] = gm_on ? __ldg(a.gmask + lo + j) : (uint8_t)0xffu;
+          if (GM) {
+            const uint8_t gm = gm_on ? __ldg(a.gmask + lo + j) : (uint8_t)0xffu;
+            if constexpr (GM_FOLD) {
+              // every thread row's pixel p lies in group p / 2: AND the doubled
+              // group bits into both thread rows' halves of the row mask
+              uint32_t x = gm & 0xfu;
+              x = (x | (x << 2)) & 0x33u;
+              x = (x | (x << 1)) & 0x55u;
+              x |= x << 1;
+              s_msk[slot].x &= x | (x << PPT);
+            } else {
+              s_gm[slot] = gm;
+            }
+          }
         }
         kept += kr;
       }
@@ -894,8 +910,14 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
             continue;
           }
         } else {
+          const uint2 mk = s_msk[k];  // bit p of mk.x >> mshift: pixel p's row is inside the box
           uint32_t gmp = PMASK;  // pixels in row groups that composited the entry
-          if (GM) {
+          if constexpr (GM_FOLD) {
+            if (!mk.x) {  // no row of the box holds a contributor
+              emit_zero(k);
+              continue;
+            }
+          } else if (GM) {
             const uint32_t gm = s_gm[k];
             if (!(gm & warp_gbits)) {  // no pixel of this warp's row groups composited the entry
               emit_zero(k);
@@ -928,7 +950,6 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
               else thr = max(thr, ncp);
             }
           }
-          const uint2 mk = s_msk[k];  // bit p of mk.x >> row: pixel p's row is inside the box
           need = ((mk.y >> L::col(tid)) & 1u) ? (mk.x >> L::mshift(tid)) & alive & gmp : 0u;
         }
         float gg[NG];
