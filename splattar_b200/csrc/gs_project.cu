@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   float3 nrm = M;
   float m2 = dot3(M, M);
   if (m2 > 0.0f) {
-    float ml = sqrtf(m2);
-    nrm = f3(M.x / ml, M.y / ml, M.z / ml);
+    const float il = rsqrtf(m2);  // the normal feeds only the aux outputs: no exact division needed
+    nrm = f3(M.x * il, M.y * il, M.z * il);
     if (dot3(nrm, c) > 0.0f) nrm = f3(-nrm.x, -nrm.y, -nrm.z);
   }
 
@@ -130,11 +130,14 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float lu = sqrtf(dot3(tu, tu)), lv = sqrtf(dot3(tv, tv));
   const float r = fminf(3.0f * k.f * (lu + lv) / depth + 3.0f, 64.0f);
   const float tf = (float)k.tile;
+  // The tile edge is a power of two (8, 16 or 32), so x·(1/tf) rounds exactly
+  // as x/tf: the rect stays bit-identical to the reference's division.
+  const float itf = 1.0f / tf;
   const float mx = (float)(k.tiles_x - 1), my = (float)(k.tiles_y - 1);
-  const uint32_t x0 = (uint32_t)fminf(fmaxf((px - r) / tf, 0.0f), mx);
-  const uint32_t y0 = (uint32_t)fminf(fmaxf((py - r) / tf, 0.0f), my);
-  const uint32_t x1 = (uint32_t)fminf(fmaxf((px + r) / tf, 0.0f), mx);
-  const uint32_t y1 = (uint32_t)fminf(fmaxf((py + r) / tf, 0.0f), my);
+  const uint32_t x0 = (uint32_t)fminf(fmaxf((px - r) * itf, 0.0f), mx);
+  const uint32_t y0 = (uint32_t)fminf(fmaxf((py - r) * itf, 0.0f), my);
+  const uint32_t x1 = (uint32_t)fminf(fmaxf((px + r) * itf, 0.0f), mx);
+  const uint32_t y1 = (uint32_t)fminf(fmaxf((py + r) * itf, 0.0f), my);
   uint32_t count = 0;
   if (px + r >= 0.0f && px - r < (float)k.W && py + r >= 0.0f && py - r < (float)k.H) {
     rect = make_uint4(x0, y0, x1, y1);
@@ -146,10 +149,10 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     // Tight binning: only the tiles of the reference rect that the α-box
     // overlaps. Tile t holds pixel centres [T·t + 0.5, T·t + T − 0.5].
     const float lim = 1e8f, hi = tf - 0.5f;
-    const float fx0 = ceilf((fminf(fmaxf(box.x, -lim), lim) - hi) / tf);
-    const float fx1 = floorf((fminf(fmaxf(box.y, -lim), lim) - 0.5f) / tf);
-    const float fy0 = ceilf((fminf(fmaxf(box.z, -lim), lim) - hi) / tf);
-    const float fy1 = floorf((fminf(fmaxf(box.w, -lim), lim) - 0.5f) / tf);
+    const float fx0 = ceilf((fminf(fmaxf(box.x, -lim), lim) - hi) * itf);
+    const float fx1 = floorf((fminf(fmaxf(box.y, -lim), lim) - 0.5f) * itf);
+    const float fy0 = ceilf((fminf(fmaxf(box.z, -lim), lim) - hi) * itf);
+    const float fy1 = floorf((fminf(fmaxf(box.w, -lim), lim) - 0.5f) * itf);
     const int tx0 = max((int)x0, (int)fmaxf(fx0, -1.f)), tx1 = min((int)x1, (int)fminf(fx1, 1e7f));
     const int ty0 = max((int)y0, (int)fmaxf(fy0, -1.f)), ty1 = min((int)y1, (int)fminf(fy1, 1e7f));
     if (tx0 <= tx1 && ty0 <= ty1) {
