@@ -975,8 +975,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
           if constexpr (PS == 2) {
             if (!((need >> pp) & 3u)) continue;
-            eval_hit2(cp, r0, r1, r2, depth, make_float2(sy_of(pp), sy_of(pp + 1)),
-                      make_float2(ky_of(pp), ky_of(pp + 1)), hh[0], hh[PS - 1]);
+            // both hits, evaluated one at a time: in this register-capped
+            // kernel the packed form's operand pairs cost more moves than
+            // its paired arithmetic saves
+            hh[0] = eval_hit(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
+            hh[PS - 1] = eval_hit(cp, r0, r1, r2, depth, sy_of(pp + 1), ky_of(pp + 1));
           } else {
             if (!need_q[0]) continue;
             hh[0] = eval_hit(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
