@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(PBA_MAX_THREADS, ORD ? 2 : 3) k_project_bwd_ad
     float* col = s_g + (ORD ? tid : sl);
     auto put = [&](int slot, float g) {
       if (ORD) col[slot * PITCH] = g;
-      else if (g != 0.0f) atomicAdd(col + slot * PITCH, g);
+      else atomicAdd(col + slot * PITCH, g);  // unconditional: a branch per slot cost more than adding zeros
     };
     GeoGrads o;
     o.pos = f3(0, 0, 0); o.scales = make_float2(0, 0); o.quat = make_float4(0, 0, 0, 0); o.opacity = 0;
