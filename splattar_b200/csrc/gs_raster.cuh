@@ -25,9 +25,10 @@
 // normal and depth distortion when aux losses are on). Per-entry gradients
 // are taken with respect to the record fields (M, Bu, Bv, tn, px, py, colour,
 // opacity, …) and reduced across the warp by a 16-lane transpose reduction,
-// then across the CTA's 8 warps in a fixed order, then either added to the
-// per-surfel accumulator with one vector reduction per 4 components (default)
-// or stored per entry for an ordered reduction (deterministic mode).
+// then (CTAs of several warps) across the warps in a fixed order, then either
+// added to the per-surfel accumulator with one vector reduction per 4
+// components (default) or stored per entry for an ordered reduction
+// (deterministic mode).
 #pragma once
 
 #include <type_traits>
@@ -962,10 +963,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           float depth = 0.f;  // feeds t in the screen branch, used by aux terms alone
           if (AUX) { r4 = s_r4[k]; depth = r4.w; }
           const ColPart cp = col_part(r0, r1, r2, g.sx, g.kx);
-          // Pixel pairs per hit evaluation (eval_hit2): with interleaved rows a
-          // box's pixel slots are consecutive, so pairs are mostly both needed
-          // (8 pixels per thread: 3.61 against 3.67 ms one at a time on 1M
-          // surfels × 8 × 1080p, at 123 registers).
+          // Pixel slots tested in pairs: with interleaved rows a box's slots
+          // are consecutive, so both pixels of a pair are mostly needed (one
+          // slot at a time ran 3.31 against 3.25 ms on 1M surfels × 8 × 1080p).
           constexpr int PS = PPT >= 2 ? 2 : 1;
 #pragma unroll
           for (int pp = 0; pp < PPT; pp += PS) {
