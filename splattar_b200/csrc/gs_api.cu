@@ -125,6 +125,7 @@ struct gs_rasterizer {
   uint8_t* inc_flag = nullptr;
   uint32_t* item_key = nullptr;
   uint32_t* counts2 = nullptr;
+  uint32_t* sorted_counts = nullptr;  // counts in depth order (written by the depth sort's final pass)
   uint32_t* cutw = nullptr;  // [0] unfinished tiles [1] completion items [2] completion entries (u32) [3] tile counter
   unsigned long long* entry_total2 = nullptr;
   std::vector<uint32_t> cut_sig;  // step shape and views the cuts were recorded for
@@ -391,15 +392,19 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   TRY_LAUNCH(r, launch_project(pa, prec, nv, st));
   mark(prof, 0, st);
   int in1 = 0;
+  // The final pass also lays the items' tile counts out in sorted order, so
+  // the entry scan and the expansion read them sequentially.
   TRY_LAUNCH(r, launch_radix_sort(r->item_keys[0], r->item_vals[0], r->item_keys[1], r->item_vals[1], items, nullptr,
-                                  32, r->sort_scratch, &in1, st));
+                                  32, r->sort_scratch, &in1, st, r->counts, r->sorted_counts));
   uint32_t* perm = r->item_vals[in1];
   uint32_t* n_entries = r->words;  // u32 saturated
-  TRY_LAUNCH(r, launch_scan(r->counts, perm, r->offsets, items, nullptr, n_entries, r->entry_total, r->scan_scratch, st));
+  TRY_LAUNCH(r, launch_scan(r->sorted_counts, nullptr, r->offsets, items, nullptr, n_entries, r->entry_total,
+                            r->scan_scratch, st));
   TRY_LAUNCH(r, launch_entry_guard(r->entry_total, n_entries, r->max_entries, r->words + 1, st));
   mark(prof, 1, st);
   ExpandArgs ea{};
-  ea.perm = perm; ea.counts = r->counts; ea.offsets = r->offsets; ea.rects = r->rects;
+  ea.perm = perm; ea.counts = r->counts; ea.sorted_counts = r->sorted_counts; ea.offsets = r->offsets;
+  ea.rects = r->rects;
   ea.views = vdev; ea.items_per_view = n; ea.tiles_x = 0;
   ea.n_items_dev = nullptr; ea.n_items_host = items;
   ea.total = r->entry_total; ea.capacity = r->max_entries;
@@ -409,7 +414,8 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
   ea.entry_offset = r->det ? r->entry_offset : nullptr;
   ea.error_word = r->words + 1;
   ExpandFilterArgs fa{};
-  fa.perm = perm; fa.counts = r->counts; fa.offsets = r->offsets; fa.rects = r->rects;
+  fa.perm = perm; fa.counts = r->counts; fa.sorted_counts = r->sorted_counts; fa.offsets = r->offsets;
+  fa.rects = r->rects;
   fa.views = vdev; fa.items_per_view = n; fa.n_items_host = items;
   fa.total = r->entry_total; fa.capacity = r->max_entries; fa.pairs = r->ent_pairs[0];
   fa.error_word = r->words + 1;
@@ -476,7 +482,7 @@ gs_status run_forward(gs_rasterizer* r, const ViewInfo* vdev, const ViewInfo* vh
     TRY_LAUNCH(r, launch_ranges_reset_list(r->inc_list, r->cutw, r->ranges, (uint32_t)tiles, st));
     mark(prof, 1, st);
     ExpandFilterArgs fb = fa;
-    fb.counts = r->counts2; fb.n_items_dev = r->cutw + 1;
+    fb.counts = r->counts2; fb.sorted_counts = nullptr; fb.n_items_dev = r->cutw + 1;
     fb.total = r->entry_total2; fb.base = r->entry_total;
     fb.cut = nullptr; fb.key_by_item = nullptr; fb.flag = r->inc_flag;
     TRY_LAUNCH(r, launch_expand_filtered(fb, st));
@@ -862,7 +868,7 @@ gs_status gs_rasterizer_create(const gs_raster_config* cfg_in, gs_rasterizer** o
   }
   ALLOC(r->rects, I);
   for (int k = 0; k < 2; ++k) { ALLOC(r->item_keys[k], I); ALLOC(r->item_vals[k], I); }
-  ALLOC(r->counts, I); ALLOC(r->offsets, I);
+  ALLOC(r->counts, I); ALLOC(r->offsets, I); ALLOC(r->sorted_counts, I);
   for (int k = 0; k < 2; ++k) ALLOC(r->ent_pairs[k], E);
   if (r->det) {
     ALLOC(r->exp_item, E);
@@ -953,7 +959,7 @@ gs_status gs_rasterizer_destroy(gs_rasterizer* r) {
                   r->mcmc_u32, r->mcmc_u64, r->mcmc_jump, r->mcmc_rng, r->mcmc_counters, r->mask, r->mask_off, r->gmask, r->tile_order, r->tile_walk,
                   r->normal_loss_sums,
                   r->mask_words,
-                  r->tile_cut, r->inc_list, r->inc_skip, r->inc_src, r->inc_flag, r->item_key, r->counts2, r->cutw, r->entry_total2,
+                  r->tile_cut, r->inc_list, r->inc_skip, r->inc_src, r->inc_flag, r->item_key, r->counts2, r->sorted_counts, r->cutw, r->entry_total2,
                   r->scan_scratch, r->sort_scratch, r->work_counts};
   for (void* p : ptrs)
     if (p) cudaFree(p);

@@ -187,8 +187,11 @@ int launch_scan(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_
                 uint32_t* total_u32, unsigned long long* total_u64, void* scratch, cudaStream_t st);
 // Stable LSD radix sort of (key, val) over bits [0, key_bits). Ping-pongs
 // between (k0,v0) and (k1,v1); returns in *result_in_1 where the output is.
+// With gather_dst, the final pass also writes gather_dst[i] = gather_src[val]
+// for every sorted position i.
 int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n_host, const uint32_t* n_dev,
-                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st);
+                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st,
+                      const uint32_t* gather_src = nullptr, uint32_t* gather_dst = nullptr);
 // The same sort on interleaved (key, val) pairs, ping-ponging between p0 and p1.
 int launch_radix_sort_pairs(uint2* p0, uint2* p1, uint64_t n_host, const uint32_t* n_dev, int key_bits, void* scratch,
                             int* result_in_1, cudaStream_t st, uint2* ranges = nullptr, uint32_t num_ranges = 0,
@@ -213,6 +216,7 @@ int launch_pair_values(const uint2* src, uint32_t* dst, const unsigned long long
 struct ExpandArgs {
   const uint32_t* perm;        // depth-sorted item order
   const uint32_t* counts;      // per item
+  const uint32_t* sorted_counts;  // counts in sorted order (counts[perm[k]]), or null
   const uint32_t* offsets;     // exclusive scan of counts in sorted order
   const uint4* rects;          // per item
   const ViewInfo* views;       // null for the standalone binner
@@ -241,6 +245,7 @@ int launch_expand(const ExpandArgs& a, cudaStream_t st);
 struct ExpandFilterArgs {
   const uint32_t* perm;
   const uint32_t* counts;
+  const uint32_t* sorted_counts;  // counts in sorted order, or null
   const uint32_t* offsets;
   const uint4* rects;
   const ViewInfo* views;

@@ -250,12 +250,25 @@ __global__ void __launch_bounds__(256) k_ssim_moments(SsimArgs a) {
 // Blur of the nine coefficient maps (the zero-padded symmetric window is
 // self-adjoint) combined with the L1 term into dL/dx: four float2 planes
 // blurred as packed pairs and one scalar plane.
-__global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
+#ifndef GS_SSIM_GRAD_INPLACE
+#define GS_SSIM_GRAD_INPLACE 1
+#endif
+__global__ void __launch_bounds__(256, GS_SSIM_GRAD_INPLACE ? 6 : 1) k_ssim_grad(SsimArgs a) {
   __shared__ float2 s_c2[4][EXT][IN_PITCH];
   __shared__ float s_c1[EXT][IN_PITCH];
-  __shared__ float2 s_h2[4][EXT * H_ROW];
-  __shared__ float s_h1[EXT * H_ROW];
-  float2* s_v2 = &s_c2[0][0][0];                                    // [4][16×16], reusing s_c2
+  // In place, the horizontal pass writes each row's 16 results over the row's
+  // first 16 staged values (a row belongs to one thread, and output o is
+  // written after input o + 10 has been read), so the vertical results get a
+  // buffer of their own and the block needs 34.5 KB of shared memory instead
+  // of 41.2 KB: 6 resident blocks per SM instead of 5.
+  constexpr bool INPL = GS_SSIM_GRAD_INPLACE;
+  constexpr int HP = INPL ? IN_PITCH : H_ROW;  // row pitch of the horizontal results
+  __shared__ float2 s_h2b[INPL ? 1 : 4][INPL ? 1 : EXT * H_ROW];
+  __shared__ float s_h1b[INPL ? 1 : EXT * H_ROW];
+  __shared__ float2 s_vb[INPL ? 4 * V_PLANE + V_PLANE / 2 : 1];
+  auto s_h2 = [&](int m) -> float2* { return INPL ? &s_c2[m][0][0] : &s_h2b[INPL ? 0 : m][0]; };
+  float* s_h1 = INPL ? &s_c1[0][0] : s_h1b;
+  float2* s_v2 = INPL ? s_vb : &s_c2[0][0][0];                      // [4][16×16]
   float* s_v1 = reinterpret_cast<float*>(s_v2 + 4 * V_PLANE);        // [16×16]
   static_assert(4 * V_PLANE * 2 + V_PLANE <= 4 * EXT * IN_PITCH * 2, "vertical results fit in s_c2");
   const int tid = threadIdx.x;
@@ -295,11 +308,11 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
     const int m = tid >> 5, r = tid & 31;
     if (m < 4) {
       const float2* X = &s_c2[m][r][0];
-      float2* O = &s_h2[m][r * H_ROW];
+      float2* O = s_h2(m) + r * HP;
       slide11x2<T16>(w, [&](int i) { return X[i]; }, [&](int o, float2 v) { O[o] = v; });
     } else {
       const float* X = &s_c1[r][0];
-      float* O = &s_h1[r * H_ROW];
+      float* O = s_h1 + r * HP;
       slide11<T16>(w, [&](int i) { return X[i]; }, [&](int o, float v) { O[o] = v; });
     }
   }
@@ -310,13 +323,13 @@ __global__ void __launch_bounds__(256) k_ssim_grad(SsimArgs a) {
     const int m = tid / (3 * T16), rem = tid - m * 3 * T16, sg = rem / T16, c = rem - sg * T16;
     const int r0 = 5 * sg;
     if (m < 4) {
-      const float2* I = &s_h2[m][c + r0 * H_ROW];
+      const float2* I = s_h2(m) + c + r0 * HP;
       float2* O = s_v2 + m * V_PLANE + c + r0 * T16;
-      slide11x2<6>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float2 v) { O[o * T16] = v; });
+      slide11x2<6>(w, [&](int i) { return I[i * HP]; }, [&](int o, float2 v) { O[o * T16] = v; });
     } else {
-      const float* I = &s_h1[c + r0 * H_ROW];
+      const float* I = s_h1 + c + r0 * HP;
       float* O = s_v1 + c + r0 * T16;
-      slide11<6>(w, [&](int i) { return I[i * H_ROW]; }, [&](int o, float v) { O[o * T16] = v; });
+      slide11<6>(w, [&](int i) { return I[i * HP]; }, [&](int o, float v) { O[o * T16] = v; });
     }
   }
   __syncthreads();

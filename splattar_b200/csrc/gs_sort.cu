@@ -135,15 +135,25 @@ __device__ __forceinline__ uint32_t match_digit(uint32_t d, int nbits, uint32_t 
 }
 
 // Element access: two arrays, or one interleaved uint2 array.
+// SplitIO's optional gather (final pass only): gdst[position] = gsrc[value],
+// e.g. each item's tile count in sorted order for the entry scan, which then
+// reads it sequentially instead of through the permutation.
 struct SplitIO {
   const uint32_t* kin; const uint32_t* vin; uint32_t* kout; uint32_t* vout;
+  const uint32_t* gsrc = nullptr; uint32_t* gdst = nullptr;
+  SplitIO plain() const { SplitIO y = *this; y.gdst = nullptr; return y; }
   __device__ __forceinline__ void skip(uint64_t b) { kin += b; vin += b; kout += b; vout += b; }
   __device__ __forceinline__ uint32_t key(uint64_t i) const { return __ldg(kin + i); }
   __device__ __forceinline__ uint2 load(uint64_t i) const { return make_uint2(__ldg(kin + i), __ldg(vin + i)); }
-  __device__ __forceinline__ void store(size_t g, uint2 e) const { kout[g] = e.x; vout[g] = e.y; }
+  __device__ __forceinline__ void store(size_t g, uint2 e) const {
+    kout[g] = e.x;
+    vout[g] = e.y;
+    if (gdst != nullptr) gdst[g] = __ldg(gsrc + e.y);
+  }
 };
 struct PairIO {
   const uint2* in; uint2* out;
+  PairIO plain() const { return *this; }
   __device__ __forceinline__ void skip(uint64_t b) { in += b; out += b; }
   __device__ __forceinline__ uint32_t key(uint64_t i) const {
     return __ldg(reinterpret_cast<const uint32_t*>(in + i));
@@ -303,7 +313,7 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
     uint32_t item = 0, cnt = 0, x0 = 0, y0 = 0, wd = 1, tb = 0, tx = a.tiles_x;
     if (valid) {
       item = a.perm[k];
-      cnt = a.counts[item];
+      cnt = a.sorted_counts != nullptr ? a.sorted_counts[k] : a.counts[item];
       if (cnt) {
         const uint4 r = a.rects[item];
         x0 = r.x; y0 = r.y; wd = r.z - r.x + 1u;
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(256) k_expand_filtered(ExpandFilterArgs a) {
     uint32_t item = 0, cnt = 0, full = 0, x0 = 0, y0 = 0, wd = 1, tb = 0, tx = 0, key = 0;
     if (k < n) {
       item = a.perm[k];
-      cnt = a.counts[item];
+      cnt = a.sorted_counts != nullptr ? a.sorted_counts[k] : a.counts[item];
       if (cnt) {
         const uint4 r = a.rects[item];
         x0 = r.x; y0 = r.y; wd = r.z - r.x + 1u;
@@ -608,7 +618,7 @@ int radix_passes(IO io, uint64_t n_host, const uint32_t* n_dev, int key_bits, vo
                               hist + RS_BINS * SORT_GRID, st);
     if (e) return e;
     const bool last = shift + 8 >= key_bits;
-    k_rs_downsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(io, n_host, n_dev, shift, nbits, hist,
+    k_rs_downsweep<IO><<<SORT_GRID, RS_THREADS, 0, st>>>(last ? io : io.plain(), n_host, n_dev, shift, nbits, hist,
                                                          last ? ranges : nullptr, num_ranges, base);
     swap(io);
     in1 ^= 1;
@@ -618,10 +628,11 @@ int radix_passes(IO io, uint64_t n_host, const uint32_t* n_dev, int key_bits, vo
 }
 
 int launch_radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n_host, const uint32_t* n_dev,
-                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st) {
-  SplitIO io{k0, v0, k1, v1};
+                      int key_bits, void* scratch, int* result_in_1, cudaStream_t st, const uint32_t* gather_src,
+                      uint32_t* gather_dst) {
+  SplitIO io{k0, v0, k1, v1, gather_src, gather_dst};
   return radix_passes(io, n_host, n_dev, key_bits, scratch, result_in_1, st, [](SplitIO& x) {
-    SplitIO y{x.kout, x.vout, const_cast<uint32_t*>(x.kin), const_cast<uint32_t*>(x.vin)};
+    SplitIO y{x.kout, x.vout, const_cast<uint32_t*>(x.kin), const_cast<uint32_t*>(x.vin), x.gsrc, x.gdst};
     x = y;
   });
 }
