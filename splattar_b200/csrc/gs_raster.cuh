@@ -87,6 +87,10 @@ __device__ __forceinline__ ColPart col_part(const float4& r0, const float4& r1, 
 // kernels compute bit-identical alphas. When the ray branch is unavailable
 // (|det| ≤ 1e-12 or t ≤ near) q_ray is +inf and u, v, t are unused.
 // q2 = u² + v² (= 2·q_ray) is kept for the backward.
+// RAY_OK: the staged entry's ray branch is known to be available at every
+// pixel of the tile (ray_available), so the per-pixel test is left out; the
+// result is the same as with the test.
+template <bool RAY_OK = false>
 __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
                                         float depth, float sy, float ky) {
   Hit h;
@@ -98,7 +102,7 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
   const float2 uv = __fmul2_rn(uvn, make_float2(inv, inv));
   const float u = uv.x, v = uv.y;
   const float t = __fmul_rn(r0.w, inv);
-  const bool ray_ok = fabsf(det) > 1e-12f && t > NEAR_DEPTH;
+  const bool ray_ok = RAY_OK || (fabsf(det) > 1e-12f && t > NEAR_DEPTH);
   h.q2 = fmaf(u, u, __fmul_rn(v, v));
   const float qr = ray_ok ? __fmul_rn(0.5f, h.q2) : __int_as_float(0x7f800000);
   const float qs = fmaf(h.dy, h.dy, c.dx2);  // (dx²+dy²)/(2σ²) with σ² = 0.5
@@ -115,6 +119,7 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
 // product and sum of the hit test takes one instruction for both pixels.
 // Each component rounds exactly as the scalar operation of eval_hit, so
 // either form gives bit-identical results for a pixel.
+template <bool RAY_OK = false>
 __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
                                           float depth, float2 sy, float2 ky, Hit& ha, Hit& hb) {
   const float2 det = __ffma2_rn(make_float2(r0.y, r0.y), sy, make_float2(c.det0, c.det0));
@@ -128,8 +133,8 @@ __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, co
   const float2 qr0 = __fmul2_rn(make_float2(0.5f, 0.5f), q2);
   const float2 qs = __ffma2_rn(dy, dy, make_float2(c.dx2, c.dx2));
   const float inf = __int_as_float(0x7f800000);
-  const float qra = fabsf(det.x) > 1e-12f && t.x > NEAR_DEPTH ? qr0.x : inf;
-  const float qrb = fabsf(det.y) > 1e-12f && t.y > NEAR_DEPTH ? qr0.y : inf;
+  const float qra = RAY_OK || (fabsf(det.x) > 1e-12f && t.x > NEAR_DEPTH) ? qr0.x : inf;
+  const float qrb = RAY_OK || (fabsf(det.y) > 1e-12f && t.y > NEAR_DEPTH) ? qr0.y : inf;
   ha.ray = qra <= qs.x;
   hb.ray = qrb <= qs.y;
   ha.u = u.x; ha.v = v.x; ha.inv_det = inv.x; ha.q2 = q2.x; ha.dy = dy.x;
@@ -173,6 +178,7 @@ struct TileGeo {
   float pyc[PPT], sy[PPT], ky[PPT];   // ky: rows within the tile
   bool inside[PPT];
   float bx0, bx1, by0, by1;     // pixel-centre extent of the tile's in-image pixels
+  float sxa, sxb, sya, syb;     // ray components of the tile's first and last pixel column and row
 };
 
 template <int TS, int PPT, bool IL = false>
@@ -206,7 +212,33 @@ __device__ __forceinline__ TileGeo<PPT> tile_geo(const RasterArgs& a, int tile) 
   g.bx1 = (float)(min(x0 + TS, g.W) - 1) + 0.5f;
   g.by0 = (float)y0 + 0.5f;
   g.by1 = (float)(min(y0 + TS, g.H) - 1) + 0.5f;
+  g.sxa = -(((float)x0 + 0.5f - cx) / f);
+  g.sxb = -(((float)(x0 + TS - 1) + 0.5f - cx) / f);
+  g.sya = ((float)y0 + 0.5f - cy) / f;
+  g.syb = ((float)(y0 + TS - 1) + 0.5f - cy) / f;
   return g;
+}
+
+// True when an entry's ray branch is available at every pixel of the tile:
+// |det| > 1e-12 and t = tn/det > NEAR_DEPTH. det = M·(sx, sy, 1) is affine
+// in the pixel's ray components, which are monotone in the pixel column and
+// row, so over the tile it lies between its values at the four corner
+// pixels; the margins (1e-5 of the terms' magnitude, 1e-5 of NEAR_DEPTH)
+// cover the rounding of the corner and per-pixel evaluations and of the
+// approximate reciprocal. A false answer only keeps the per-pixel test.
+template <int PPT>
+__device__ __forceinline__ bool ray_available(const float4& r0, const TileGeo<PPT>& g) {
+  const float e0 = fmaf(r0.x, g.sxa, r0.z), e1 = fmaf(r0.x, g.sxb, r0.z);
+  const float d00 = fmaf(r0.y, g.sya, e0), d01 = fmaf(r0.y, g.syb, e0);
+  const float d10 = fmaf(r0.y, g.sya, e1), d11 = fmaf(r0.y, g.syb, e1);
+  const float err = 1e-5f * (fabsf(r0.x) * fmaxf(fabsf(g.sxa), fabsf(g.sxb)) +
+                             fabsf(r0.y) * fmaxf(fabsf(g.sya), fabsf(g.syb)) + fabsf(r0.z));
+  const float lo = fminf(fminf(d00, d01), fminf(d10, d11)) - err;
+  const float hi = fmaxf(fmaxf(d00, d01), fmaxf(d10, d11)) + err;
+  const float near = NEAR_DEPTH * (1.0f + 1e-5f);
+  if (lo > 1e-12f) return r0.w > near * hi;     // det > 0 everywhere: t ≥ tn / hi
+  if (hi < -1e-12f) return -r0.w > near * -lo;  // det < 0 everywhere: t ≥ tn / lo
+  return false;
 }
 
 template <int PPT>
@@ -382,6 +414,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
   __shared__ int s_tile;
   __shared__ uint32_t s_walk;  // tile_walk: the tile's largest contributor count
   __shared__ uint32_t s_slot;  // counter value the tile was taken at
+  // Bit 31 of a staged column mask (free on tiles of up to 16 pixels): the
+  // entry's ray branch is available at every pixel of the tile, and its
+  // pixels are evaluated without the per-pixel test (ray_available).
+  constexpr bool RAYFLAG = TS <= 16;
+  constexpr uint32_t RAYBIT = 0x80000000u;
   const int tid = threadIdx.x, lane = tid & 31;
   const bool gm_on = GM && a.gmask != nullptr;
   const int g0 = L::row(tid) >> 2;  // first row group of this lane's pixels
@@ -470,7 +507,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
           stage_offsets(r1, r2, g.bx0, g.by0);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (!COLOR) s_r4[slot] = r4;
-          s_msk[slot] = box_masks<TS, PPT>(bb, g);
+          uint2 mk = box_masks<TS, PPT>(bb, g);
+          if (RAYFLAG && ray_available(r0, g)) mk.y |= RAYBIT;
+          s_msk[slot] = mk;
           s_j[slot] = j;
         }
         kept += kr;
@@ -495,6 +534,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
             const uint32_t idx1 = base - range.x + (uint32_t)s_j[k] + 1u;
             const ColPart cp = col_part(r0, r1, r2, g.sx, g.kx);
             constexpr int PS = PPT >= 2 ? 2 : 1;  // pixels per hit evaluation
+            // the pixel walk, with or without the per-pixel ray test
+            auto walk = [&](auto ray_tag) {
+            constexpr bool RAY_OK = decltype(ray_tag)::value;
 #pragma unroll
             for (int pp = 0; pp < PPT; pp += PS) {
             bool need_q[PS];
@@ -503,11 +545,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
             for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
             if constexpr (PS == 2) {
               if (!((need >> pp) & 3u)) continue;
-              eval_hit2(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
-                        make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
+              eval_hit2<RAY_OK>(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
+                                make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
             } else {
               if (!need_q[0]) continue;
-              hh[0] = eval_hit(cp, r0, r1, r2, r4.w, g.sy[pp], g.ky[pp]);
+              hh[0] = eval_hit<RAY_OK>(cp, r0, r1, r2, r4.w, g.sy[pp], g.ky[pp]);
             }
             if constexpr (PS == 2 && COLOR && !MASK && PPT <= 4) {  // (8 pixels per thread would spill)
               // Both pixels of the pair composited at once in packed FP32: a
@@ -574,6 +616,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
               if (T[p] < T_TERMINATE) dm |= 1u << p;
             }
             }
+            };
+            if (RAYFLAG && (mk.y & RAYBIT)) walk(std::true_type{});
+            else walk(std::false_type{});
             tdone = dm == PMASK;
           }
           if (GM && gm_on && (k & 31) == 31) flush_row_groups<PPT, GPL, GM ? GW : 1>(gcur, s_gw, g0, k >> 5);
@@ -702,6 +747,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
   constexpr bool SYS = LEAN && GS_BWD_SY_SMEM;
   __shared__ uint32_t s_nc[LEAN ? TP : 1];
   __shared__ float s_sy[SYS ? TS : 1];
+  // Bit 31 of a staged column mask (tiles of up to 16 pixels): the entry's
+  // ray branch is available at every pixel of the tile (ray_available).
+  constexpr bool RAYFLAG = TS <= 16;
+  constexpr uint32_t RAYBIT = 0x80000000u;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;
   // A lane's pixels p (rows row(tid) + p·RS) as bits of a PPT-bit mask. Row
@@ -864,7 +913,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           stage_offsets(r1, r2, g.bx0, g.by0);
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (AUX) s_r4[slot] = r4;
-          s_msk[slot] = box_masks<TS, PPT, IL>(bb, g);
+          {
+            uint2 mk = box_masks<TS, PPT, IL>(bb, g);
+            if (RAYFLAG && ray_available(r0, g)) mk.y |= RAYBIT;
+            s_msk[slot] = mk;
+          }
           s_item[slot] = item;
           if (DET) s_q[slot] = q;
           s_j[slot] = j;
@@ -967,6 +1020,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           // are consecutive, so both pixels of a pair are mostly needed (one
           // slot at a time ran 3.31 against 3.25 ms on 1M surfels × 8 × 1080p).
           constexpr int PS = PPT >= 2 ? 2 : 1;
+          // the pixel walk, with or without the per-pixel ray test
+          auto walk = [&](auto ray_tag) {
+          constexpr bool RAY_OK = decltype(ray_tag)::value;
 #pragma unroll
           for (int pp = 0; pp < PPT; pp += PS) {
           bool need_q[PS];
@@ -978,11 +1034,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
             // both hits, evaluated one at a time: in this register-capped
             // kernel the packed form's operand pairs cost more moves than
             // its paired arithmetic saves
-            hh[0] = eval_hit(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
-            hh[PS - 1] = eval_hit(cp, r0, r1, r2, depth, sy_of(pp + 1), ky_of(pp + 1));
+            hh[0] = eval_hit<RAY_OK>(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
+            hh[PS - 1] = eval_hit<RAY_OK>(cp, r0, r1, r2, depth, sy_of(pp + 1), ky_of(pp + 1));
           } else {
             if (!need_q[0]) continue;
-            hh[0] = eval_hit(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
+            hh[0] = eval_hit<RAY_OK>(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
           }
 #pragma unroll
           for (int q = 0; q < PS; ++q) {
@@ -1065,6 +1121,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
             }
           }
           }
+          };
+          if (RAYFLAG && (s_msk[k].y & RAYBIT)) walk(std::true_type{});
+          else walk(std::false_type{});
           // A thread's pixels share sx: the sx moments are sx times the plain sums.
           gg[0] = gg[2] * g.sx; gg[3] = gg[5] * g.sx; gg[6] = gg[8] * g.sx;
         }
