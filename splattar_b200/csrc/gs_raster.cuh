@@ -87,10 +87,15 @@ __device__ __forceinline__ ColPart col_part(const float4& r0, const float4& r1, 
 // kernels compute bit-identical alphas. When the ray branch is unavailable
 // (|det| ≤ 1e-12 or t ≤ near) q_ray is +inf and u, v, t are unused.
 // q2 = u² + v² (= 2·q_ray) is kept for the backward.
-// RAY_OK: the staged entry's ray branch is known to be available at every
-// pixel of the tile (ray_available), so the per-pixel test is left out; the
-// result is the same as with the test.
-template <bool RAY_OK = false>
+// Fast forms, decided per staged entry and tile, with the same α, skip
+// decision and branch for every pixel that takes the entry as the full test:
+//   RAY_OK (1): the entry's ray branch is available at every pixel of the
+//     tile (ray_available), so the per-pixel ray test is left out;
+//   RAY_FAR (2): besides, its screen-space low-pass disc stays away from the
+//     tile (screen_far), so q_screen is left out too: where q_screen < q_ray,
+//     q_screen > ln(255·o) + 0.05 already puts α below 1/255.
+constexpr int HIT_FULL = 0, HIT_RAY_OK = 1, HIT_RAY_FAR = 2;
+template <int FAST = HIT_FULL>
 __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
                                         float depth, float sy, float ky) {
   Hit h;
@@ -102,7 +107,15 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
   const float2 uv = __fmul2_rn(uvn, make_float2(inv, inv));
   const float u = uv.x, v = uv.y;
   const float t = __fmul_rn(r0.w, inv);
-  const bool ray_ok = RAY_OK || (fabsf(det) > 1e-12f && t > NEAR_DEPTH);
+  if constexpr (FAST == HIT_RAY_FAR) {
+    h.q2 = fmaf(u, u, __fmul_rn(v, v));
+    h.ray = true;
+    h.u = u; h.v = v; h.inv_det = inv;
+    h.t = t;
+    h.ghat = __expf(-__fmul_rn(0.5f, h.q2));
+    return h;
+  }
+  const bool ray_ok = FAST == HIT_RAY_OK || (fabsf(det) > 1e-12f && t > NEAR_DEPTH);
   h.q2 = fmaf(u, u, __fmul_rn(v, v));
   const float qr = ray_ok ? __fmul_rn(0.5f, h.q2) : __int_as_float(0x7f800000);
   const float qs = fmaf(h.dy, h.dy, c.dx2);  // (dx²+dy²)/(2σ²) with σ² = 0.5
@@ -119,7 +132,7 @@ __device__ __forceinline__ Hit eval_hit(const ColPart& c, const float4& r0, cons
 // product and sum of the hit test takes one instruction for both pixels.
 // Each component rounds exactly as the scalar operation of eval_hit, so
 // either form gives bit-identical results for a pixel.
-template <bool RAY_OK = false>
+template <int FAST = HIT_FULL>
 __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, const float4& r1, const float4& r2,
                                           float depth, float2 sy, float2 ky, Hit& ha, Hit& hb) {
   const float2 det = __ffma2_rn(make_float2(r0.y, r0.y), sy, make_float2(c.det0, c.det0));
@@ -131,10 +144,18 @@ __device__ __forceinline__ void eval_hit2(const ColPart& c, const float4& r0, co
   const float2 t = __fmul2_rn(make_float2(r0.w, r0.w), inv);
   const float2 q2 = __ffma2_rn(u, u, __fmul2_rn(v, v));
   const float2 qr0 = __fmul2_rn(make_float2(0.5f, 0.5f), q2);
+  if constexpr (FAST == HIT_RAY_FAR) {  // as eval_hit
+    ha.ray = hb.ray = true;
+    ha.u = u.x; ha.v = v.x; ha.inv_det = inv.x; ha.q2 = q2.x; ha.dy = dy.x; ha.t = t.x;
+    hb.u = u.y; hb.v = v.y; hb.inv_det = inv.y; hb.q2 = q2.y; hb.dy = dy.y; hb.t = t.y;
+    ha.ghat = __expf(-qr0.x);
+    hb.ghat = __expf(-qr0.y);
+    return;
+  }
   const float2 qs = __ffma2_rn(dy, dy, make_float2(c.dx2, c.dx2));
   const float inf = __int_as_float(0x7f800000);
-  const float qra = RAY_OK || (fabsf(det.x) > 1e-12f && t.x > NEAR_DEPTH) ? qr0.x : inf;
-  const float qrb = RAY_OK || (fabsf(det.y) > 1e-12f && t.y > NEAR_DEPTH) ? qr0.y : inf;
+  const float qra = FAST == HIT_RAY_OK || (fabsf(det.x) > 1e-12f && t.x > NEAR_DEPTH) ? qr0.x : inf;
+  const float qrb = FAST == HIT_RAY_OK || (fabsf(det.y) > 1e-12f && t.y > NEAR_DEPTH) ? qr0.y : inf;
   ha.ray = qra <= qs.x;
   hb.ray = qrb <= qs.y;
   ha.u = u.x; ha.v = v.x; ha.inv_det = inv.x; ha.q2 = q2.x; ha.dy = dy.x;
@@ -239,6 +260,18 @@ __device__ __forceinline__ bool ray_available(const float4& r0, const TileGeo<PP
   if (lo > 1e-12f) return r0.w > near * hi;     // det > 0 everywhere: t ≥ tn / hi
   if (hi < -1e-12f) return -r0.w > near * -lo;  // det < 0 everywhere: t ≥ tn / lo
   return false;
+}
+
+// True when q_screen = dx² + dy² exceeds ln(255·max(o, 1)) + 0.05 at every
+// pixel of the tile, for a record staged with stage_offsets (dx = r1.w +
+// column, dy = r2.w + row) and opacity o: there o·exp(−q_screen) < 1/255, so
+// the screen branch never decides a pixel that takes the entry.
+template <int TS>
+__device__ __forceinline__ bool screen_far(const float4& r1, const float4& r2, float o) {
+  const float ex = r1.w > 0.f ? r1.w : fmaxf(-(r1.w + (float)(TS - 1)), 0.f);
+  const float ey = r2.w > 0.f ? r2.w : fmaxf(-(r2.w + (float)(TS - 1)), 0.f);
+  const float lim = 5.5913f + fmaxf(__logf(o), 0.f) * 1.001f;  // ln 255 = 5.5413
+  return fmaf(ex, ex, ey * ey) > lim;
 }
 
 template <int PPT>
@@ -415,8 +448,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
   __shared__ uint32_t s_walk;  // tile_walk: the tile's largest contributor count
   __shared__ uint32_t s_slot;  // counter value the tile was taken at
   // Bit 31 of a staged column mask (free on tiles of up to 16 pixels): the
-  // entry's ray branch is available at every pixel of the tile, and its
-  // pixels are evaluated without the per-pixel test (ray_available).
+  // entry's ray branch is available at every pixel of the tile and its
+  // screen-space disc stays away from the tile, so its pixels are evaluated
+  // in the HIT_RAY_FAR form.
   constexpr bool RAYFLAG = TS <= 16;
   constexpr uint32_t RAYBIT = 0x80000000u;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -508,7 +542,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (!COLOR) s_r4[slot] = r4;
           uint2 mk = box_masks<TS, PPT>(bb, g);
-          if (RAYFLAG && ray_available(r0, g)) mk.y |= RAYBIT;
+          if (RAYFLAG && ray_available(r0, g) && screen_far<TS>(r1, r2, r3.w)) mk.y |= RAYBIT;
           s_msk[slot] = mk;
           s_j[slot] = j;
         }
@@ -536,7 +570,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
             constexpr int PS = PPT >= 2 ? 2 : 1;  // pixels per hit evaluation
             // the pixel walk, with or without the per-pixel ray test
             auto walk = [&](auto ray_tag) {
-            constexpr bool RAY_OK = decltype(ray_tag)::value;
+            constexpr int FAST = decltype(ray_tag)::value ? HIT_RAY_FAR : HIT_FULL;
 #pragma unroll
             for (int pp = 0; pp < PPT; pp += PS) {
             bool need_q[PS];
@@ -545,11 +579,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
             for (int q = 0; q < PS; ++q) need_q[q] = (need >> (pp + q)) & 1u;
             if constexpr (PS == 2) {
               if (!((need >> pp) & 3u)) continue;
-              eval_hit2<RAY_OK>(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
+              eval_hit2<FAST>(cp, r0, r1, r2, r4.w, make_float2(g.sy[pp], g.sy[pp + 1]),
                                 make_float2(g.ky[pp], g.ky[pp + 1]), hh[0], hh[PS - 1]);
             } else {
               if (!need_q[0]) continue;
-              hh[0] = eval_hit<RAY_OK>(cp, r0, r1, r2, r4.w, g.sy[pp], g.ky[pp]);
+              hh[0] = eval_hit<FAST>(cp, r0, r1, r2, r4.w, g.sy[pp], g.ky[pp]);
             }
             if constexpr (PS == 2 && COLOR && !MASK && PPT <= 4) {  // (8 pixels per thread would spill)
               // Both pixels of the pair composited at once in packed FP32: a
@@ -1022,7 +1056,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           constexpr int PS = PPT >= 2 ? 2 : 1;
           // the pixel walk, with or without the per-pixel ray test
           auto walk = [&](auto ray_tag) {
-          constexpr bool RAY_OK = decltype(ray_tag)::value;
+          constexpr int FAST = decltype(ray_tag)::value ? HIT_RAY_OK : HIT_FULL;
 #pragma unroll
           for (int pp = 0; pp < PPT; pp += PS) {
           bool need_q[PS];
@@ -1034,11 +1068,11 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
             // both hits, evaluated one at a time: in this register-capped
             // kernel the packed form's operand pairs cost more moves than
             // its paired arithmetic saves
-            hh[0] = eval_hit<RAY_OK>(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
-            hh[PS - 1] = eval_hit<RAY_OK>(cp, r0, r1, r2, depth, sy_of(pp + 1), ky_of(pp + 1));
+            hh[0] = eval_hit<FAST>(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
+            hh[PS - 1] = eval_hit<FAST>(cp, r0, r1, r2, depth, sy_of(pp + 1), ky_of(pp + 1));
           } else {
             if (!need_q[0]) continue;
-            hh[0] = eval_hit<RAY_OK>(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
+            hh[0] = eval_hit<FAST>(cp, r0, r1, r2, depth, sy_of(pp), ky_of(pp));
           }
 #pragma unroll
           for (int q = 0; q < PS; ++q) {
