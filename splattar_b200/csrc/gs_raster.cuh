@@ -448,9 +448,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
   __shared__ uint32_t s_walk;  // tile_walk: the tile's largest contributor count
   __shared__ uint32_t s_slot;  // counter value the tile was taken at
   // Bit 31 of a staged column mask (free on tiles of up to 16 pixels): the
-  // entry's ray branch is available at every pixel of the tile and its
-  // screen-space disc stays away from the tile, so its pixels are evaluated
-  // in the HIT_RAY_FAR form.
+  // entry's ray branch is available at every pixel of the tile, its
+  // screen-space disc stays away from the tile and its opacity is below the
+  // α clamp, so its pixels are evaluated in the HIT_RAY_FAR form and never
+  // clamped.
   constexpr bool RAYFLAG = TS <= 16;
   constexpr uint32_t RAYBIT = 0x80000000u;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -542,7 +543,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (!COLOR) s_r4[slot] = r4;
           uint2 mk = box_masks<TS, PPT>(bb, g);
-          if (RAYFLAG && ray_available(r0, g) && screen_far<TS>(r1, r2, r3.w)) mk.y |= RAYBIT;
+          if (RAYFLAG && r3.w < ALPHA_CLAMP && ray_available(r0, g) && screen_far<TS>(r1, r2, r3.w)) mk.y |= RAYBIT;
           s_msk[slot] = mk;
           s_j[slot] = j;
         }
@@ -590,8 +591,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
               // pixel that does not take the entry gets α = 0, so its weight is
               // 0 and its T is multiplied by 1 (both exact); each component
               // rounds as the scalar code below would.
-              const float a0 = fminf(__fmul_rn(r3.w, hh[0].ghat), ALPHA_CLAMP);
-              const float a1 = fminf(__fmul_rn(r3.w, hh[PS - 1].ghat), ALPHA_CLAMP);
+              // (fast form: opacity < ALPHA_CLAMP and ĝ ≤ 1, so the clamp never acts)
+              const float a0 = FAST ? __fmul_rn(r3.w, hh[0].ghat) : fminf(__fmul_rn(r3.w, hh[0].ghat), ALPHA_CLAMP);
+              const float a1 = FAST ? __fmul_rn(r3.w, hh[PS - 1].ghat)
+                                    : fminf(__fmul_rn(r3.w, hh[PS - 1].ghat), ALPHA_CLAMP);
               const bool c0 = need_q[0] && !(a0 < ALPHA_SKIP), c1 = need_q[PS - 1] && !(a1 < ALPHA_SKIP);
               if (c0 || c1) {
                 const float2 al = make_float2(c0 ? a0 : 0.f, c1 ? a1 : 0.f);
@@ -623,7 +626,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
               const int p = pp + q;
               if (!need_q[q]) continue;
               const Hit& h = hh[q];
-              const float alpha = fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
+              const float alpha = FAST ? __fmul_rn(r3.w, h.ghat) : fminf(__fmul_rn(r3.w, h.ghat), ALPHA_CLAMP);
               if (alpha < ALPHA_SKIP) continue;
               const float w = T[p] * alpha;
               cr[p] += r3.x * w; cg[p] += r3.y * w; cb[p] += r3.z * w;
@@ -782,7 +785,8 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
   __shared__ uint32_t s_nc[LEAN ? TP : 1];
   __shared__ float s_sy[SYS ? TS : 1];
   // Bit 31 of a staged column mask (tiles of up to 16 pixels): the entry's
-  // ray branch is available at every pixel of the tile (ray_available).
+  // ray branch is available at every pixel of the tile (ray_available) and
+  // its opacity is below the α clamp (α = o·ĝ with ĝ ≤ 1 is never clamped).
   constexpr bool RAYFLAG = TS <= 16;
   constexpr uint32_t RAYBIT = 0x80000000u;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -949,7 +953,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           if (AUX) s_r4[slot] = r4;
           {
             uint2 mk = box_masks<TS, PPT, IL>(bb, g);
-            if (RAYFLAG && ray_available(r0, g)) mk.y |= RAYBIT;
+            if (RAYFLAG && r3.w < ALPHA_CLAMP && ray_available(r0, g)) mk.y |= RAYBIT;
             s_msk[slot] = mk;
           }
           s_item[slot] = item;
@@ -1080,7 +1084,8 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
             if (!need_q[q]) continue;
             const Hit& h = hh[q];
             const float raw_alpha = __fmul_rn(r3.w, h.ghat);
-            const float alpha = fminf(raw_alpha, ALPHA_CLAMP);
+            // (fast form: opacity < ALPHA_CLAMP and ĝ ≤ 1, so the clamp never acts)
+            const float alpha = FAST ? raw_alpha : fminf(raw_alpha, ALPHA_CLAMP);
             if (alpha < ALPHA_SKIP) continue;
             contrib = true;
             const float inv_oma = rcp_approx(1.0f - alpha);
@@ -1126,7 +1131,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
               gg[11] = c2.x; gg[12] = c2.y;
               gg[13] += gcol.z * w;
             }
-            if (raw_alpha <= ALPHA_CLAMP) {
+            if (FAST || raw_alpha <= ALPHA_CLAMP) {
               // dL/dĝ·ĝ = dL/dα·o·ĝ; ray branch: ĝ = exp(−(u²+v²)/2) with
               // u = (s·Bu)/det, v = (s·Bv)/det, det = s·M, so dL/d(s·Bu) = −u·K/det,
               // dL/d(s·Bv) = −v·K/det and dL/ddet = (u²+v²)·K/det (− t·dL/dt/det
