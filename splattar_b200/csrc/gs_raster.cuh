@@ -789,6 +789,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
   // its opacity is below the α clamp (α = o·ĝ with ĝ ≤ 1 is never clamped).
   constexpr bool RAYFLAG = TS <= 16;
   constexpr uint32_t RAYBIT = 0x80000000u;
+  constexpr uint32_t FARBIT = 0x40000000u;  // with RAYBIT: the HIT_RAY_FAR form (screen_far)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool gm_on = GM && a.gmask != nullptr;
   // A lane's pixels p (rows row(tid) + p·RS) as bits of a PPT-bit mask. Row
@@ -953,7 +954,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           if (AUX) s_r4[slot] = r4;
           {
             uint2 mk = box_masks<TS, PPT, IL>(bb, g);
-            if (RAYFLAG && r3.w < ALPHA_CLAMP && ray_available(r0, g)) mk.y |= RAYBIT;
+            if (RAYFLAG && r3.w < ALPHA_CLAMP && ray_available(r0, g)) {
+              mk.y |= RAYBIT;
+              if (screen_far<TS>(r1, r2, r3.w)) mk.y |= FARBIT;
+            }
             s_msk[slot] = mk;
           }
           s_item[slot] = item;
@@ -1060,7 +1064,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           constexpr int PS = PPT >= 2 ? 2 : 1;
           // the pixel walk, with or without the per-pixel ray test
           auto walk = [&](auto ray_tag) {
-          constexpr int FAST = decltype(ray_tag)::value ? HIT_RAY_OK : HIT_FULL;
+          constexpr int FAST = decltype(ray_tag)::value;
 #pragma unroll
           for (int pp = 0; pp < PPT; pp += PS) {
           bool need_q[PS];
@@ -1161,8 +1165,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
           }
           }
           };
-          if (RAYFLAG && (s_msk[k].y & RAYBIT)) walk(std::true_type{});
-          else walk(std::false_type{});
+          const uint32_t fm = RAYFLAG ? s_msk[k].y : 0u;
+          if (fm & FARBIT) walk(std::integral_constant<int, HIT_RAY_FAR>{});
+          else if (fm & RAYBIT) walk(std::integral_constant<int, HIT_RAY_OK>{});
+          else walk(std::integral_constant<int, HIT_FULL>{});
           // A thread's pixels share sx: the sx moments are sx times the plain sums.
           gg[0] = gg[2] * g.sx; gg[3] = gg[5] * g.sx; gg[6] = gg[8] * g.sx;
         }
