@@ -447,13 +447,14 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
   __shared__ int s_tile;
   __shared__ uint32_t s_walk;  // tile_walk: the tile's largest contributor count
   __shared__ uint32_t s_slot;  // counter value the tile was taken at
-  // Bit 31 of a staged column mask (free on tiles of up to 16 pixels): the
-  // entry's ray branch is available at every pixel of the tile, its
-  // screen-space disc stays away from the tile and its opacity is below the
-  // α clamp, so its pixels are evaluated in the HIT_RAY_FAR form and never
-  // clamped.
+  // Bits 31 and 30 of a staged column mask (free on tiles of up to 16
+  // pixels): RAYBIT when the entry's ray branch is available at every pixel
+  // of the tile (ray_available) and its opacity is below the α clamp (α =
+  // o·ĝ with ĝ ≤ 1 is never clamped): the HIT_RAY_OK form; with FARBIT its
+  // screen-space disc also stays away from the tile (screen_far): the
+  // HIT_RAY_FAR form.
   constexpr bool RAYFLAG = TS <= 16;
-  constexpr uint32_t RAYBIT = 0x80000000u;
+  constexpr uint32_t RAYBIT = 0x80000000u, FARBIT = 0x40000000u;
   const int tid = threadIdx.x, lane = tid & 31;
   const bool gm_on = GM && a.gmask != nullptr;
   const int g0 = L::row(tid) >> 2;  // first row group of this lane's pixels
@@ -543,7 +544,10 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
           s_r0[slot] = r0; s_r1[slot] = r1; s_r2[slot] = r2; s_r3[slot] = r3;
           if (!COLOR) s_r4[slot] = r4;
           uint2 mk = box_masks<TS, PPT>(bb, g);
-          if (RAYFLAG && r3.w < ALPHA_CLAMP && ray_available(r0, g) && screen_far<TS>(r1, r2, r3.w)) mk.y |= RAYBIT;
+          if (RAYFLAG && r3.w < ALPHA_CLAMP && ray_available(r0, g)) {
+            mk.y |= RAYBIT;
+            if (screen_far<TS>(r1, r2, r3.w)) mk.y |= FARBIT;
+          }
           s_msk[slot] = mk;
           s_j[slot] = j;
         }
@@ -571,7 +575,7 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
             constexpr int PS = PPT >= 2 ? 2 : 1;  // pixels per hit evaluation
             // the pixel walk, with or without the per-pixel ray test
             auto walk = [&](auto ray_tag) {
-            constexpr int FAST = decltype(ray_tag)::value ? HIT_RAY_FAR : HIT_FULL;
+            constexpr int FAST = decltype(ray_tag)::value;
 #pragma unroll
             for (int pp = 0; pp < PPT; pp += PS) {
             bool need_q[PS];
@@ -654,8 +658,9 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR
             }
             }
             };
-            if (RAYFLAG && (mk.y & RAYBIT)) walk(std::true_type{});
-            else walk(std::false_type{});
+            if (RAYFLAG && (mk.y & FARBIT)) walk(std::integral_constant<int, HIT_RAY_FAR>{});
+            else if (RAYFLAG && (mk.y & RAYBIT)) walk(std::integral_constant<int, HIT_RAY_OK>{});
+            else walk(std::integral_constant<int, HIT_FULL>{});
             tdone = dm == PMASK;
           }
           if (GM && gm_on && (k & 31) == 31) flush_row_groups<PPT, GPL, GM ? GW : 1>(gcur, s_gw, g0, k >> 5);
@@ -784,9 +789,8 @@ __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 32 && !MASK
   constexpr bool SYS = LEAN && GS_BWD_SY_SMEM;
   __shared__ uint32_t s_nc[LEAN ? TP : 1];
   __shared__ float s_sy[SYS ? TS : 1];
-  // Bit 31 of a staged column mask (tiles of up to 16 pixels): the entry's
-  // ray branch is available at every pixel of the tile (ray_available) and
-  // its opacity is below the α clamp (α = o·ĝ with ĝ ≤ 1 is never clamped).
+  // Bits 31 and 30 of a staged column mask, as in the forward: RAYBIT for
+  // the HIT_RAY_OK form, with FARBIT for the HIT_RAY_FAR form.
   constexpr bool RAYFLAG = TS <= 16;
   constexpr uint32_t RAYBIT = 0x80000000u;
   constexpr uint32_t FARBIT = 0x40000000u;  // with RAYBIT: the HIT_RAY_FAR form (screen_far)
