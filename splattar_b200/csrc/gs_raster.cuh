@@ -415,11 +415,14 @@ __device__ __forceinline__ void cut_tile_end(const RasterArgs& a, int tile, uint
 // loss reads nothing else); depth and normal are neither accumulated nor
 // written.
 // Resident two-warp colour-only forward CTAs per SM that the register
-// allocation must allow (1: the compiler's choice). 14 caps the registers at 72 (7 warps per
-// SM sub-partition): on 1M surfels × 8 × 1080p the colour-only (64, 4)
-// forward ran 3.32 ms at 72 registers against 4.21 ms at the compiler's 99.
+// allocation must allow (1: the compiler's choice). 16 caps the registers at
+// 64 (8 warps per SM sub-partition, 40 B of spills): on 1M surfels × 8 ×
+// 1080p the colour-only (64, 4) forward ran 2.74 ms against 2.82 ms at 14
+// CTAs (72 registers) and 3.32 → 4.21 ms earlier between 72 registers and
+// the compiler's 99. With the per-entry hit forms the walk needs fewer live
+// values; before them 64 registers ran slower than 72.
 #ifndef GS_FWD_2WARP_CTAS
-#define GS_FWD_2WARP_CTAS 14
+#define GS_FWD_2WARP_CTAS 16
 #endif
 template <int TS, int BATCH, int PREC, bool DET, bool PERSIST, int PPT, bool COLOR = false, bool MASK = false>
 __global__ void __launch_bounds__(TS * TS / PPT, ((TS * TS / PPT) == 64 && COLOR && !MASK) ? GS_FWD_2WARP_CTAS : 1)
